@@ -1,0 +1,308 @@
+#!/usr/bin/env python
+"""Benchmark: query cells/s annotated on B200 (SingleR first + final labels).
+
+Workload (default): the mid-size exact-correlation configuration, 20,000 reference cells x 25,000
+genes, 100,000 query cells, ~6 % nonzero float32 CSR of log2(1+x), 30 labels; seeded synthetic
+data (no public dataset here).  One step = one full annotation (score step + fine-tune) of the
+100,000-cell query batch; the reference preparation (marker training, reference ranks) is done once
+before timing and reported as ref_prep_s.
+
+  value : cells/s with the query CSR already resident in HBM (device pointers into the C ABI)
+  e2e   : cells/s through the same C ABI call from pinned host buffers (H2D inside the timed region)
+
+`--impl reference` times the CPU restatement of the reference's path (oracle/, the reference's own
+code has no CPU path for its kernels) on every host core, on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): weak scaling, each rank annotates its own query batch with the reference
+replicated; no collective in the data path, the max over ranks of the device time is reported.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from cusingler_b200 import synth  # noqa: E402
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
+
+
+def peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, FALLBACK_BF16_TFLOPS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def make_data(args, rank: int):
+    wl = synth.WORKLOADS[args.workload]
+    world = synth.make_world(wl, 0)
+    n_ref = args.n_ref or wl.n_ref
+    n_qry = args.n_qry or wl.n_qry
+    ref = synth.generate(world, n_ref, 0)
+    qry = synth.generate(world, n_qry, 1 + 1000 * rank)
+    return wl, ref, qry
+
+
+def cpu_reference(args, wl, ref, qry, steps, warmup, sample):
+    """The CPU restatement of the reference path (oracle), all host threads, on `sample` query
+    cells per step.  Returns (cells/s, cores, seconds per step)."""
+    from oracle import oracle as O
+
+    cores = os.cpu_count() or 1
+    L = wl.n_labels
+    names = synth.names("CT", L)
+    genes = synth.names("G", ref.n_cols)
+    times = []
+    for s in range(warmup + steps):
+        a = (s * sample) % max(1, qry.n_rows - sample)
+        sub = qry.rows(a, a + sample)
+        orc = O.Oracle(O.Problem(ref, sub, names, ref.labels, genes, genes), cores)
+        orc.train()
+        t0 = time.perf_counter()
+        orc.score(mode=O.MODE_FP32REF)
+        orc.finetune(mode=O.MODE_FP32REF)
+        dt = time.perf_counter() - t0
+        if s >= warmup:
+            times.append(dt)
+    per_step = sum(times) / len(times)
+    return sample / per_step, cores, per_step
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wl, ref, qry = make_data(args, 0)
+    value, cores, per_step = cpu_reference(args, wl, ref, qry, args.steps, args.warmup, args.cpu_sample)
+    line = {
+        "metric": "query cells/s annotated (first + final label)", "value": value, "unit": "cells/s",
+        "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_step * 1000, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {wl.n_ref} ref x {wl.n_qry} query x {wl.n_genes} genes, "
+                               f"{wl.n_labels} labels", "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.cpu_sample} query cells per step, full reference"},
+        "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mid", choices=list(synth.WORKLOADS))
+    ap.add_argument("--n-ref", type=int, default=0)
+    ap.add_argument("--n-qry", type=int, default=0)
+    ap.add_argument("--mode", default="exact", choices=["exact", "fp32ref"])
+    ap.add_argument("--cpu-sample", type=int, default=96)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world_size > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from cusingler_b200 import abi
+
+    wl, ref, qry = make_data(args, rank)
+    L = wl.n_labels
+    names = synth.names("CT", L)
+    genes = synth.names("G", ref.n_cols)
+    mode = abi.MODE_EXACT if args.mode == "exact" else abi.MODE_FP32REF
+    ann = abi.Annotator(gpuid=local, mode=mode)
+    t0 = time.perf_counter()
+    ann.train(ref, ref.labels, names, genes, genes)
+    ref_prep_s = time.perf_counter() - t0
+    stream = torch.cuda.current_stream()
+    ann.set_stream(stream.cuda_stream)
+
+    dev = torch.device("cuda", local)
+    d_data = torch.from_numpy(qry.data).to(dev)
+    d_idx = torch.from_numpy(qry.indices).to(dev)
+    d_ptr = torch.from_numpy(qry.indptr.astype(np.int32)).to(dev)
+    csr_dev = abi.device_csr(qry.n_rows, qry.n_cols, d_data.data_ptr(), d_idx.data_ptr(), d_ptr.data_ptr())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        first, final = ann.annotate(csr_dev)
+    barrier()
+    ann.reset_timings()
+    ann.set_profiling(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            first, final = ann.annotate(csr_dev)
+        ev1.record(stream)
+        barrier()
+    ann.set_profiling(False)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    tm = ann.timings()
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world_size * qry.n_rows / (ms / 1000.0)
+
+    # e2e: host (pinned) inputs through the same call, upload inside the timed region
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    h_data, h_idx, h_ptr = pin(qry.data), pin(qry.indices), pin(qry.indptr.astype(np.int32))
+    csr_host = abi.SgrCsr(qry.n_rows, qry.n_cols, h_data.data_ptr(), h_idx.data_ptr(), h_ptr.data_ptr(), 0)
+    e2e_steps = max(1, min(args.steps, 3))
+    ann.annotate(csr_host)
+    barrier()
+    ev0.record(stream)
+    for _ in range(e2e_steps):
+        first_h, final_h = ann.annotate(csr_host)
+    ev1.record(stream)
+    barrier()
+    e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = qry.data.nbytes + qry.indices.nbytes + 4 * (qry.n_rows + 1)
+    d2h = 2 * 4 * qry.n_rows
+
+    hbm, bf16, src = peaks()
+    steps = args.steps
+    stages = {k: tm[k] / steps for k in ("rank_ms", "corr_ms", "select_ms", "finetune_ms")}
+    corr_launch_ms = tm["corr_ms"] / max(1, tm["corr_launches"])
+    corr_ops_launch = tm["corr_ops"] / max(1, tm["corr_launches"])
+    rank_launch_ms = tm["rank_ms"] / max(1, tm["rank_launches"])
+    rank_bytes_launch = tm["rank_bytes"] / max(1, tm["rank_launches"])
+    int8_peak = 2 * bf16  # dense int8 = 2x dense bf16 on B200; no int8 figure is measured
+    roof_corr = {"kernel": "score-step correlation", "bound": "tensor",
+                 "achieved": corr_ops_launch / (corr_launch_ms / 1000) / 1e12, "peak": int8_peak,
+                 "unit": "TFLOP/s", "traffic": None,
+                 "peak_note": f"int8 dense = 2 x {src} bf16 cuBLAS ({bf16} TFLOP/s)"}
+    roof_corr["frac"] = roof_corr["achieved"] / roof_corr["peak"]
+    roof_rank = {"kernel": "gather + rank", "bound": "hbm",
+                 "achieved": rank_bytes_launch / (rank_launch_ms / 1000) / 1e9, "peak": hbm, "unit": "GB/s",
+                 "traffic": None, "peak_note": f"{src} copy bandwidth"}
+    roof_rank["frac"] = roof_rank["achieved"] / roof_rank["peak"]
+    dominant = roof_corr if stages["corr_ms"] >= stages["rank_ms"] else roof_rank
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        v, cores, per = cpu_reference(args, wl, ref, qry, 1, 0, args.cpu_sample)
+        cpu = {"value": v, "unit": "cells/s", "cores": cores, "kind": "port",
+               "sample": f"{args.cpu_sample} query cells of the same batch, full reference, {per:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": "query cells/s annotated (first + final label)", "value": value, "unit": "cells/s",
+            "n_gpus": world_size, "steps": steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int8" if mode == abi.MODE_EXACT else "f32", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {ref.n_rows} ref x {qry.n_rows} query x {ref.n_cols} genes, "
+                                   f"{L} labels, {qry.nnz / (qry.n_rows * qry.n_cols):.3f} density",
+                       "form": f"plain ({args.mode})", "l2": "inputs larger than L2 (query CSR "
+                                                             f"{h2d / 1e9:.2f} GB)",
+                       "parallelism": f"query sharding x{world_size}"},
+            "e2e": {"value": world_size * qry.n_rows / (e2e_ms / 1000.0), "unit": "cells/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(tm["launches"] / steps * steps),
+            "roofline": dominant, "roofline_other": roof_rank if dominant is roof_corr else roof_corr,
+            "stages_ms": stages, "ref_prep_s": ref_prep_s,
+            "ft_rounds_per_cell": tm["ft_cell_rounds"] / max(1, tm["cells"]),
+            "clocks": clk.summary(), "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ann.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

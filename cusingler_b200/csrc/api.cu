@@ -1,0 +1,952 @@
+// C ABI (include/sgr.h) and the host orchestration of the SingleR path on one GPU.
+//
+// Reference flow restated (STOmics/cusingler): Pipeline::train / score / finetune
+// (src/pipeline.cpp:128-156, 47-111), get_label (src/cusingler.cu:986-1136), cufinetune and
+// finetune_round (src/cusingler.cu:1138-1333).  The reference keeps every stage's state in
+// file-scope globals and exits on errors; here the state lives in sgr_ctx and errors come back as
+// sgr_status.
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <map>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "sgr_internal.h"
+#include "stl_order.h"
+
+using namespace sgr;
+
+namespace {
+
+enum Stage { ST_H2D = 0, ST_RANK, ST_CORR, ST_SELECT, ST_FT, ST_COUNT };
+
+// CUDA-event spans on the context's stream; resolved after the call's final synchronisation.
+struct Profiler {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    struct Span {
+        int stage;
+        cudaEvent_t a, b;
+    };
+    std::vector<Span> spans;
+    sgr_timings acc{};
+
+    cudaEvent_t take() {
+        if (used == pool.size()) {
+            cudaEvent_t e;
+            SGR_CUDA(cudaEventCreate(&e));
+            pool.push_back(e);
+        }
+        return pool[used++];
+    }
+    int begin(int stage, cudaStream_t s) {
+        if (!on) return -1;
+        Span sp{stage, take(), take()};
+        SGR_CUDA(cudaEventRecord(sp.a, s));
+        spans.push_back(sp);
+        return (int)spans.size() - 1;
+    }
+    void end(int id, cudaStream_t s) {
+        if (id >= 0) SGR_CUDA(cudaEventRecord(spans[id].b, s));
+    }
+    // after the stream is synchronised
+    void collect() {
+        if (!on || spans.empty()) {
+            spans.clear();
+            used = 0;
+            return;
+        }
+        double* slot[ST_COUNT] = {&acc.h2d_ms, &acc.rank_ms, &acc.corr_ms, &acc.select_ms, &acc.finetune_ms};
+        float first_last = 0.f;
+        for (auto& sp : spans) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, sp.a, sp.b) == cudaSuccess) *slot[sp.stage] += ms;
+        }
+        if (cudaEventElapsedTime(&first_last, spans.front().a, spans.back().b) == cudaSuccess)
+            acc.total_ms += first_last;
+        cudaGetLastError();
+        spans.clear();
+        used = 0;
+    }
+    ~Profiler() {
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+}  // namespace
+
+struct sgr_ctx {
+    int device = 0;
+    int cores = 1;
+    cudaStream_t stream = nullptr;      // the stream work runs on
+    cudaStream_t own_stream = nullptr;  // created with the context
+    Profiler prof;
+    sgr_mode mode = SGR_MODE_EXACT;
+    std::string err;
+    bool trained = false;        // reference resident on the device
+    bool markers_ready = false;  // host marker training done
+
+    Markers mk;
+    uint32_t R = 0;      // reference rows
+    uint32_t ref_cols = 0;
+    int G = 0, Kp = 0;   // score-step genes and padded row length
+    uint32_t Wt = 0;     // fine-tune gene pool
+
+    // device reference: regrouped CSR (original columns), score-step ranks, thre-filtered CSR
+    DevBuf<float> ref_data;
+    DevBuf<int32_t> ref_indices, ref_indptr;
+    DevBuf<int32_t> ref_map_common, qry_map_common, ref_map_thre, qry_map_thre;
+    DevBuf<int8_t> ref_limbs;
+    DevBuf<int64_t> ref_n2;
+    DevBuf<double> ref_rinv;
+    DevBuf<float> ref_f32;
+    std::vector<int64_t> h_ref_n2;
+    DevBuf<float> reff_data;
+    DevBuf<int32_t> reff_indices, reff_indptr;
+
+    // per-call query buffers
+    DevBuf<float> q_data;
+    DevBuf<int32_t> q_indices, q_indptr;
+    DevBuf<int8_t> q_limbs;
+    DevBuf<int64_t> q_n2;
+    DevBuf<double> q_rinv;
+    DevBuf<float> q_f32;
+    DevBuf<float> scores;
+    DevBuf<LabelQ> lq;
+    DevBuf<float> label_scores;
+    DevBuf<int32_t> first;
+    DevBuf<uint8_t> flags;
+    DevBuf<float> sel_scratch;
+    DevBuf<RankGroup> rank_groups;
+    DevBuf<int> status;
+    DevBuf<int32_t> counts, offsets;
+    DevBuf<float> qf_data;
+    DevBuf<int32_t> qf_indices, qf_indptr;
+
+    // fine-tune round buffers
+    DevBuf<int32_t> ft_maps;
+    DevBuf<RankGroup> ft_rgroups_q, ft_rgroups_r;
+    DevBuf<RankItem> ft_items_q, ft_items_r;
+    DevBuf<int16_t> ft_qd, ft_rd;
+    DevBuf<int64_t> ft_qn, ft_rn;
+    DevBuf<double> ft_qr, ft_rr;
+    DevBuf<float> ft_qf, ft_rf;
+    DevBuf<FtGroup> ft_groups;
+    DevBuf<FtCorrItem> ft_corr_items;
+    DevBuf<FtSelItem> ft_sel_items;
+    DevBuf<LabelQ> ft_lq;
+    DevBuf<float> ft_scores, ft_label_scores;
+};
+
+namespace {
+
+constexpr int kScoreChunkBytes = 1 << 30;  // score-step correlation block (queries x reference)
+
+int pow2_at_least(int v) {
+    int n = 1;
+    while (n < v) n <<= 1;
+    return n;
+}
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+template <class F>
+sgr_status guarded(sgr_ctx* ctx, F&& f) {
+    if (!ctx) return SGR_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    try {
+        if (ctx->device >= 0) SGR_CUDA(cudaSetDevice(ctx->device));
+        const uint64_t l0 = launch_count();
+        f();
+        if (ctx->stream) {
+            SGR_CUDA(cudaStreamSynchronize(ctx->stream));
+            ctx->prof.collect();
+        }
+        ctx->prof.acc.launches += launch_count() - l0;
+        return SGR_OK;
+    } catch (const Error& e) {
+        ctx->err = e.what();
+        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+        cudaGetLastError();
+        ctx->prof.spans.clear();
+        ctx->prof.used = 0;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        ctx->err = "host allocation failed";
+        return SGR_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        ctx->err = e.what();
+        return SGR_ERR_INVALID_ARGUMENT;
+    }
+}
+
+void check_csr_shape(const sgr_csr* m, const char* what) {
+    if (!m) fail(SGR_ERR_INVALID_ARGUMENT, std::string(what) + ": null matrix");
+    if (m->n_rows && (!m->indptr)) fail(SGR_ERR_INVALID_ARGUMENT, std::string(what) + ": null indptr");
+}
+
+// Host-side validation of a host CSR (offsets monotone, columns in range).
+void validate_host_csr(const sgr_csr* m, const char* what) {
+    check_csr_shape(m, what);
+    if (m->indptr[0] != 0) fail(SGR_ERR_INVALID_ARGUMENT, std::string(what) + ": indptr[0] != 0");
+    for (uint32_t r = 0; r < m->n_rows; ++r)
+        if (m->indptr[r + 1] < m->indptr[r])
+            fail(SGR_ERR_INVALID_ARGUMENT, std::string(what) + ": indptr decreases at row " + std::to_string(r));
+}
+
+// LabelQ of a score list of `len` values at `start` for quantile p: the reference's float index
+// grid i * step with step = 1/(len-1), lower_bound of p (src/cusingler.cu:947-978).
+LabelQ make_lq(int start, int len, float p) {
+    LabelQ q{};
+    q.start = start;
+    q.len = len;
+    if (len <= 1) {
+        q.kind = 0;
+        return q;
+    }
+    const float step = 1.0 / (len - 1);
+    q.step = step;
+    const float first = 0 * step, last = (len - 1) * step;
+    if (p <= first) {
+        q.kind = 1;
+        return q;
+    }
+    if (last <= p) {
+        q.kind = 2;
+        return q;
+    }
+    int lo = 0, hi = len;
+    while (lo < hi) {
+        int mid = (lo + hi) / 2;
+        if (mid * step < p) lo = mid + 1;
+        else hi = mid;
+    }
+    q.kind = 3;
+    q.k = lo;
+    q.prev_index = (lo - 1) * step;
+    return q;
+}
+
+void check_status(sgr_ctx* ctx) {
+    int st = 0;
+    SGR_CUDA(cudaMemcpyAsync(&st, ctx->status.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    SGR_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (st & 1) fail(SGR_ERR_INVALID_ARGUMENT, "a CSR column index is out of range");
+    if (st & 2) fail(SGR_ERR_INVALID_ARGUMENT, "a CSR value is NaN");
+    if (st & 8) fail(SGR_ERR_STATE, "NaN-bearing score list without sort scratch");
+    // bit 4: libstdc++ would have read outside a NaN-bearing list; the result is the bounded one
+}
+
+void reset_status(sgr_ctx* ctx) {
+    ctx->status.ensure(1);
+    SGR_CUDA(cudaMemsetAsync(ctx->status.p, 0, sizeof(int), ctx->stream));
+}
+
+// Makes the query CSR device-resident (borrowed when it already is).
+struct DevCsr {
+    const float* data;
+    const int32_t* indices;
+    const int32_t* indptr;
+    uint32_t n_rows, n_cols;
+    int64_t nnz;  // -1 when unknown (device input)
+};
+
+DevCsr query_on_device(sgr_ctx* ctx, const sgr_csr* q) {
+    check_csr_shape(q, "query");
+    if (q->on_device) {
+        int32_t nnz = 0;
+        if (q->n_rows) {
+            SGR_CUDA(cudaMemcpyAsync(&nnz, q->indptr + q->n_rows, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+            SGR_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+        return {q->data, q->indices, q->indptr, q->n_rows, q->n_cols, nnz};
+    }
+    validate_host_csr(q, "query");
+    const size_t nnz = (size_t)q->indptr[q->n_rows];
+    int sp = ctx->prof.begin(ST_H2D, ctx->stream);
+    ctx->q_data.upload(q->data, nnz, ctx->stream);
+    ctx->q_indices.upload(q->indices, nnz, ctx->stream);
+    ctx->q_indptr.upload(q->indptr, (size_t)q->n_rows + 1, ctx->stream);
+    ctx->prof.end(sp, ctx->stream);
+    return {ctx->q_data.p, ctx->q_indices.p, ctx->q_indptr.p, q->n_rows, q->n_cols, (int64_t)nnz};
+}
+
+int sort_cap(int G) { return std::min(pow2_at_least(std::max(G, 32)), 4096); }
+
+// Gather + rank of rows [0, n) of a device CSR over one gene subset.
+void rank_rows(sgr_ctx* ctx, const DevCsr& m, const RankGroup& grp, int out_mode, int norm_mode) {
+    ctx->rank_groups.upload(&grp, 1, ctx->stream);
+    RankLaunch a{};
+    a.data = m.data;
+    a.indices = m.indices;
+    a.indptr = m.indptr;
+    a.n_cols = m.n_cols;
+    a.items = nullptr;
+    a.row0 = 0;
+    a.n_items = m.n_rows;
+    a.groups = ctx->rank_groups.p;
+    a.out_mode = out_mode;
+    a.norm_mode = norm_mode;
+    a.max_Kp = grp.Kp;
+    a.cap = sort_cap(grp.G);
+    a.status = ctx->status.p;
+    launch_rank(a, ctx->stream);
+}
+
+// Compacts a device CSR to the columns with map >= 0 into (data, indices, indptr) buffers.
+void filter_csr(sgr_ctx* ctx, const DevCsr& m, const int32_t* map, DevBuf<float>& od, DevBuf<int32_t>& oi,
+                DevBuf<int32_t>& op) {
+    ctx->counts.ensure(m.n_rows + 1);
+    op.ensure((size_t)m.n_rows + 1);
+    launch_filter_count(m.indptr, m.indices, m.n_rows, m.n_cols, map, ctx->counts.p, ctx->stream);
+    launch_exclusive_scan(ctx->counts.p, op.p, m.n_rows, nullptr, ctx->stream);
+    int32_t total = 0;
+    SGR_CUDA(cudaMemcpyAsync(&total, op.p + m.n_rows, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    SGR_CUDA(cudaStreamSynchronize(ctx->stream));
+    od.ensure(std::max<int32_t>(total, 1));
+    oi.ensure(std::max<int32_t>(total, 1));
+    launch_filter_fill(m.data, m.indptr, m.indices, m.n_rows, m.n_cols, map, op.p, od.p, oi.p, ctx->stream);
+}
+
+std::vector<int32_t> position_map(const std::vector<int32_t>& colmap, const std::vector<uint32_t>& genes,
+                                  uint32_t W) {
+    std::vector<int32_t> pos(W, -1);
+    for (size_t i = 0; i < genes.size(); ++i) pos[genes[i]] = (int32_t)i;
+    std::vector<int32_t> out(colmap.size(), -1);
+    for (size_t c = 0; c < colmap.size(); ++c)
+        if (colmap[c] >= 0 && (uint32_t)colmap[c] < W) out[c] = pos[colmap[c]];
+    return out;
+}
+
+void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const char* const* label_names,
+           uint32_t n_labels, const char* const* ref_genes, const char* const* qry_genes, uint32_t n_qry) {
+    if (!ref || ref->on_device) fail(SGR_ERR_INVALID_ARGUMENT, "reference must be a host CSR");
+    if (!celltypes || !label_names || !ref_genes || !qry_genes) fail(SGR_ERR_INVALID_ARGUMENT, "null argument");
+    validate_host_csr(ref, "reference");
+    for (uint32_t r = 0; r < ref->n_rows; ++r)
+        for (int32_t i = ref->indptr[r]; i < ref->indptr[r + 1]; ++i)
+            if ((uint32_t)ref->indices[i] >= ref->n_cols)
+                fail(SGR_ERR_INVALID_ARGUMENT, "reference column index out of range");
+    ctx->trained = false;
+    ctx->markers_ready = false;
+    HostCsr h{ref->n_rows, ref->n_cols, ref->data, ref->indices, ref->indptr};
+    train_markers(h, celltypes, n_labels, ref_genes, qry_genes, n_qry, ctx->cores, ctx->mk);
+    Markers& mk = ctx->mk;
+    ctx->R = ref->n_rows;
+    ctx->ref_cols = ref->n_cols;
+    ctx->G = (int)mk.common.size();
+    ctx->Kp = round_up(std::max(ctx->G, 1), 128);
+    ctx->Wt = (uint32_t)mk.thre.size();
+    ctx->markers_ready = true;
+    if (ctx->device < 0) return;  // host-only context: marker training only
+    if (ctx->G > 8128) fail(SGR_ERR_UNSUPPORTED, "more than 8128 score-step marker genes");
+
+    // regrouped reference CSR
+    std::vector<int32_t> indptr(ctx->R + 1, 0);
+    for (uint32_t j = 0; j < ctx->R; ++j) {
+        uint32_t r = mk.ref_order[j];
+        indptr[j + 1] = indptr[j] + (ref->indptr[r + 1] - ref->indptr[r]);
+    }
+    std::vector<float> data(indptr[ctx->R]);
+    std::vector<int32_t> indices(indptr[ctx->R]);
+    for (uint32_t j = 0; j < ctx->R; ++j) {
+        uint32_t r = mk.ref_order[j];
+        std::copy(ref->data + ref->indptr[r], ref->data + ref->indptr[r + 1], data.begin() + indptr[j]);
+        std::copy(ref->indices + ref->indptr[r], ref->indices + ref->indptr[r + 1], indices.begin() + indptr[j]);
+    }
+    cudaStream_t s = ctx->stream;
+    ctx->ref_data.upload(data, s);
+    ctx->ref_indices.upload(indices, s);
+    ctx->ref_indptr.upload(indptr, s);
+    ctx->ref_map_common.upload(position_map(mk.ref_colmap, mk.common, mk.W), s);
+    ctx->qry_map_common.upload(position_map(mk.qry_colmap, mk.common, mk.W), s);
+    ctx->ref_map_thre.upload(position_map(mk.ref_colmap, mk.thre, mk.W), s);
+    ctx->qry_map_thre.upload(position_map(mk.qry_colmap, mk.thre, mk.W), s);
+
+    // score-step reference ranks (int8 limb planes), resident for every query batch
+    reset_status(ctx);
+    ctx->ref_limbs.ensure((size_t)ctx->R * 3 * ctx->Kp);
+    ctx->ref_n2.ensure(ctx->R);
+    ctx->ref_rinv.ensure(ctx->R);
+    ctx->ref_f32.ensure(ctx->R);
+    DevCsr rm{ctx->ref_data.p, ctx->ref_indices.p, ctx->ref_indptr.p, ctx->R, ctx->ref_cols, (int64_t)indptr[ctx->R]};
+    RankGroup g{ctx->ref_map_common.p, ctx->G, ctx->Kp, ctx->ref_limbs.p, ctx->ref_n2.p, ctx->ref_rinv.p,
+                ctx->ref_f32.p};
+    rank_rows(ctx, rm, g, RANK_LIMBS, NORM_SEQ);
+    ctx->h_ref_n2.resize(ctx->R);
+    SGR_CUDA(cudaMemcpyAsync(ctx->h_ref_n2.data(), ctx->ref_n2.p, ctx->R * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    // fine-tune: reference compacted to the thre pool
+    filter_csr(ctx, rm, ctx->ref_map_thre.p, ctx->reff_data, ctx->reff_indices, ctx->reff_indptr);
+    check_status(ctx);
+    ctx->trained = true;
+}
+
+// Score-step device pass over the first nq rows of `q` (already device resident).
+void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
+    cudaStream_t s = ctx->stream;
+    const uint32_t Q = q.n_rows, R = ctx->R, L = ctx->mk.n_labels;
+    const bool fp32 = ctx->mode == SGR_MODE_FP32REF;
+    ctx->q_limbs.ensure((size_t)Q * 3 * ctx->Kp);
+    ctx->q_n2.ensure(Q);
+    ctx->q_rinv.ensure(Q);
+    ctx->q_f32.ensure(Q);
+    RankGroup g{ctx->qry_map_common.p, ctx->G, ctx->Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p};
+    DevCsr qq = q;
+    const uint64_t l0 = launch_count();
+    int sp = ctx->prof.begin(ST_RANK, s);
+    rank_rows(ctx, qq, g, RANK_LIMBS, fp32 ? NORM_SEQ : NORM_NONE);
+    ctx->prof.end(sp, s);
+    ctx->prof.acc.rank_launches += launch_count() - l0;
+
+    std::vector<LabelQ> lq(L);
+    bool any_nan_ref = false;
+    for (uint32_t l = 0; l < L; ++l) {
+        lq[l] = make_lq((int)ctx->mk.ctidx[2 * l], (int)ctx->mk.ctidx[2 * l + 1], p);
+        for (uint32_t r = ctx->mk.ctidx[2 * l]; r < ctx->mk.ctidx[2 * l] + ctx->mk.ctidx[2 * l + 1]; ++r)
+            if (ctx->h_ref_n2[r] == 0) lq[l].has_nan = 1, any_nan_ref = true;
+    }
+    ctx->lq.upload(lq, s);
+    uint32_t max_len = 1;
+    for (uint32_t l = 0; l < L; ++l) max_len = std::max(max_len, ctx->mk.ctidx[2 * l + 1]);
+    float* scratch = nullptr;
+    if (any_nan_ref) {
+        scratch = ctx->sel_scratch.ensure((size_t)select_blocks_with_scratch() * 8 * max_len);
+    }
+    ctx->label_scores.ensure((size_t)Q * L);
+    ctx->first.ensure(Q);
+    ctx->flags.ensure((size_t)Q * L);
+    const uint32_t chunk = (uint32_t)std::max<size_t>(1, std::min<size_t>(Q, kScoreChunkBytes / (4 * (size_t)R)));
+    ctx->scores.ensure((size_t)chunk * R);
+    for (uint32_t q0 = 0; q0 < Q; q0 += chunk) {
+        const int nq = (int)std::min(chunk, Q - q0);
+        const uint64_t c0 = launch_count();
+        sp = ctx->prof.begin(ST_CORR, s);
+        launch_corr_simt(fp32, ctx->q_limbs.p + (size_t)q0 * 3 * ctx->Kp, ctx->ref_limbs.p, nq, (int)R, ctx->G,
+                         ctx->Kp, ctx->q_f32.p + q0, ctx->ref_f32.p, ctx->q_rinv.p + q0, ctx->ref_rinv.p,
+                         ctx->q_n2.p + q0, ctx->ref_n2.p, ctx->scores.p, R, s);
+        ctx->prof.end(sp, s);
+        ctx->prof.acc.corr_launches += launch_count() - c0;
+        sp = ctx->prof.begin(ST_SELECT, s);
+        launch_select_first(ctx->scores.p, R, nq, (int)L, ctx->lq.p, p, thre, ctx->q_n2.p + q0,
+                            ctx->label_scores.p + (size_t)q0 * L, ctx->first.p + q0, ctx->flags.p + (size_t)q0 * L,
+                            scratch, max_len, ctx->status.p, s);
+        ctx->prof.end(sp, s);
+    }
+    ctx->prof.acc.cells += Q;
+    ctx->prof.acc.corr_ops += 2ull * Q * R * (uint64_t)ctx->G;
+    ctx->prof.acc.rank_bytes += 8ull * (uint64_t)(q.nnz) + 4ull * (Q + 1) + 3ull * Q * (uint64_t)ctx->Kp;
+}
+
+// ---- fine-tune ---------------------------------------------------------------------------------
+
+struct CellState {
+    std::vector<uint8_t> top;  // candidate labels in the reference's list order
+    int times = 0;
+    int rounds = 0;
+};
+
+// Genes of one candidate set: union over ordered pairs of the first min(len, gene_thre) entries of
+// the pair's fine-tune list, ascending thre ids (src/cusingler.cu:1141-1161).
+std::vector<uint32_t> round_genes(const Markers& mk, const std::vector<uint8_t>& labels) {
+    const uint32_t L = mk.n_labels;
+    const int gene_thre = marker_count(labels.size());
+    std::vector<uint32_t> genes;
+    for (uint8_t i : labels)
+        for (uint8_t j : labels) {
+            if (i == j) continue;
+            uint32_t pos = mk.ft_idx[(i * L + j) * 2];
+            int len = (int)mk.ft_idx[(i * L + j) * 2 + 1];
+            if (len > gene_thre) len = gene_thre;
+            genes.insert(genes.end(), mk.ft_genes.begin() + pos, mk.ft_genes.begin() + pos + len);
+        }
+    std::sort(genes.begin(), genes.end());
+    genes.erase(std::unique(genes.begin(), genes.end()), genes.end());
+    return genes;
+}
+
+// One reference fine-tune decision from the candidate scores in list order
+// (src/cusingler.cu:1270-1295).
+std::vector<uint8_t> decide(const std::vector<uint8_t>& top, const std::vector<float>& sc, float thre) {
+    int mn, mx;
+    stl::minmax(sc.data(), (int)sc.size(), &mn, &mx);
+    const float lo = sc[mn], hi = sc[mx];
+    const float t = hi - thre;
+    if (std::isnan(hi)) return {top.front()};
+    std::vector<uint8_t> res;
+    for (size_t i = 0; i < sc.size(); ++i) {
+        if (sc[i] <= lo || sc[i] < t) continue;
+        if (sc[i] == hi) res.insert(res.begin(), top[i]);
+        else res.push_back(top[i]);
+    }
+    if (res.empty()) res.push_back(top.front());
+    return res;
+}
+
+struct Group {
+    std::vector<uint8_t> labels;  // ascending
+    std::vector<uint32_t> genes;  // thre ids, ascending
+    std::vector<uint32_t> cells;
+};
+
+void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float p, float thre, int times,
+                     int32_t* final_labels, int32_t* rounds_out) {
+    cudaStream_t s = ctx->stream;
+    const Markers& mk = ctx->mk;
+    const uint32_t Q = q.n_rows, L = mk.n_labels, Wt = ctx->Wt;
+    const bool fp32 = ctx->mode == SGR_MODE_FP32REF;
+    const int sp_ft = ctx->prof.begin(ST_FT, s);
+    struct EndSpan {
+        sgr_ctx* c;
+        int id;
+        ~EndSpan() {
+            if (id >= 0) cudaEventRecord(c->prof.spans[id].b, c->stream);
+        }
+    } end_ft{ctx, sp_ft};
+
+    // query compacted to the thre pool (once per call)
+    filter_csr(ctx, q, ctx->qry_map_thre.p, ctx->qf_data, ctx->qf_indices, ctx->qf_indptr);
+    DevCsr qf{ctx->qf_data.p, ctx->qf_indices.p, ctx->qf_indptr.p, Q, std::max<uint32_t>(Wt, 1), -1};
+    DevCsr rf{ctx->reff_data.p, ctx->reff_indices.p, ctx->reff_indptr.p, ctx->R, std::max<uint32_t>(Wt, 1), -1};
+
+    std::vector<CellState> st(Q);
+    for (uint32_t i = 0; i < Q; ++i)
+        for (uint32_t l = 0; l < L; ++l)
+            if (flags[(size_t)i * L + l]) st[i].top.push_back((uint8_t)l);
+
+    uint32_t max_label = 1;
+    for (uint32_t l = 0; l < L; ++l) max_label = std::max(max_label, mk.ctidx[2 * l + 1]);
+
+    for (;;) {
+        // active cells grouped by candidate set
+        std::map<std::vector<uint8_t>, uint32_t> gid;
+        std::vector<Group> groups;
+        for (uint32_t i = 0; i < Q; ++i) {
+            CellState& c = st[i];
+            if (!(c.top.size() > 1 && (times == 0 || c.times++ < times))) continue;
+            std::vector<uint8_t> key = c.top;
+            std::sort(key.begin(), key.end());
+            auto it = gid.find(key);
+            if (it == gid.end()) {
+                it = gid.emplace(key, (uint32_t)groups.size()).first;
+                groups.push_back(Group{key, round_genes(mk, key), {}});
+            }
+            groups[it->second].cells.push_back(i);
+        }
+        if (groups.empty()) break;
+        // sets with fewer than 20 genes keep their first candidate (src/cusingler.cu:1158-1159)
+        std::vector<uint32_t> work;
+        for (uint32_t gi = 0; gi < groups.size(); ++gi) {
+            if (groups[gi].genes.size() < 20) {
+                for (uint32_t c : groups[gi].cells) {
+                    st[c].top = {st[c].top.front()};
+                    st[c].rounds++;
+                }
+            } else {
+                work.push_back(gi);
+            }
+        }
+        // process the remaining groups in batches bounded by device memory
+        size_t wi = 0;
+        while (wi < work.size()) {
+            std::vector<uint32_t> batch;
+            size_t bytes = 0;
+            const size_t budget = (size_t)4 << 30;
+            while (wi < work.size()) {
+                const Group& g = groups[work[wi]];
+                size_t nref = 0;
+                for (uint8_t l : g.labels) nref += mk.ctidx[2 * l + 1];
+                const size_t Kp = round_up((int)g.genes.size(), 32);
+                const size_t b = (nref + g.cells.size()) * Kp * 2 + g.cells.size() * nref * 4 + (size_t)Wt * 4;
+                if (!batch.empty() && bytes + b > budget) break;
+                batch.push_back(work[wi++]);
+                bytes += b;
+            }
+            // tables
+            const uint32_t nb = (uint32_t)batch.size();
+            std::vector<int32_t> maps((size_t)nb * Wt, -1);
+            std::vector<FtGroup> fg(nb);
+            std::vector<RankGroup> rgq(nb), rgr(nb);
+            std::vector<RankItem> iq, ir;
+            std::vector<FtCorrItem> ci;
+            std::vector<FtSelItem> si;
+            std::vector<LabelQ> lqs;
+            int64_t q_rows = 0, r_rows = 0, sc_off = 0, out_off = 0, q_elems = 0, r_elems = 0;
+            int maxKp = 32;
+            for (uint32_t b = 0; b < nb; ++b) {
+                const Group& g = groups[batch[b]];
+                const int G = (int)g.genes.size();
+                const int Kp = round_up(G, 32);
+                maxKp = std::max(maxKp, Kp);
+                for (int i = 0; i < G; ++i) maps[(size_t)b * Wt + g.genes[i]] = i;
+                FtGroup& f = fg[b];
+                f.G = G;
+                f.Kp = Kp;
+                f.n_cells = (int32_t)g.cells.size();
+                f.q_el = q_elems;
+                f.r_el = r_elems;
+                f.q_row = q_rows;
+                f.r_row = r_rows;
+                f.s_off = sc_off;
+                f.n_labels = (int32_t)g.labels.size();
+                f.lq_off = (int32_t)lqs.size();
+                f.out_off = out_off;
+                int32_t nref = 0;
+                for (uint8_t l : g.labels) {
+                    const uint32_t st0 = mk.ctidx[2 * l], len = mk.ctidx[2 * l + 1];
+                    lqs.push_back(make_lq(nref, (int)len, p));
+                    for (uint32_t r = st0; r < st0 + len; ++r) ir.push_back(RankItem{r, b, (uint32_t)nref++, 0});
+                }
+                f.n_ref = nref;
+                for (uint32_t c = 0; c < g.cells.size(); ++c) {
+                    iq.push_back(RankItem{g.cells[c], b, c, 0});
+                    si.push_back(FtSelItem{b, c});
+                }
+                const uint32_t qb = 16;
+                for (int32_t r = 0; r < nref; ++r)
+                    for (uint32_t c0 = 0; c0 < g.cells.size(); c0 += qb)
+                        ci.push_back(FtCorrItem{b, (uint32_t)r, c0, std::min<uint32_t>(c0 + qb, g.cells.size())});
+                q_elems += (int64_t)g.cells.size() * Kp;
+                r_elems += (int64_t)nref * Kp;
+                q_rows += g.cells.size();
+                r_rows += nref;
+                sc_off += (int64_t)g.cells.size() * nref;
+                out_off += (int64_t)g.cells.size() * g.labels.size();
+            }
+            ctx->ft_maps.upload(maps, s);
+            ctx->ft_qd.ensure(std::max<int64_t>(q_elems, 1));
+            ctx->ft_rd.ensure(std::max<int64_t>(r_elems, 1));
+            ctx->ft_qn.ensure(q_rows);
+            ctx->ft_rn.ensure(r_rows);
+            ctx->ft_qr.ensure(q_rows);
+            ctx->ft_rr.ensure(r_rows);
+            ctx->ft_qf.ensure(q_rows);
+            ctx->ft_rf.ensure(r_rows);
+            for (uint32_t b = 0; b < nb; ++b) {
+                const FtGroup& f = fg[b];
+                const int32_t* map = ctx->ft_maps.p + (size_t)b * Wt;
+                rgq[b] = RankGroup{map, f.G, f.Kp, ctx->ft_qd.p + f.q_el, ctx->ft_qn.p + f.q_row,
+                                   ctx->ft_qr.p + f.q_row, ctx->ft_qf.p + f.q_row};
+                rgr[b] = RankGroup{map, f.G, f.Kp, ctx->ft_rd.p + f.r_el, ctx->ft_rn.p + f.r_row,
+                                   ctx->ft_rr.p + f.r_row, ctx->ft_rf.p + f.r_row};
+            }
+            ctx->ft_rgroups_q.upload(rgq, s);
+            ctx->ft_rgroups_r.upload(rgr, s);
+            ctx->ft_items_q.upload(iq, s);
+            ctx->ft_items_r.upload(ir, s);
+            RankLaunch a{};
+            a.out_mode = RANK_D16;
+            a.norm_mode = fp32 ? NORM_TREE128 : NORM_NONE;
+            a.max_Kp = maxKp;
+            a.cap = std::min(pow2_at_least(maxKp), 4096);
+            a.status = ctx->status.p;
+            a.data = qf.data;
+            a.indices = qf.indices;
+            a.indptr = qf.indptr;
+            a.n_cols = qf.n_cols;
+            a.items = ctx->ft_items_q.p;
+            a.n_items = (uint32_t)iq.size();
+            a.groups = ctx->ft_rgroups_q.p;
+            launch_rank(a, s);
+            a.data = rf.data;
+            a.indices = rf.indices;
+            a.indptr = rf.indptr;
+            a.n_cols = rf.n_cols;
+            a.items = ctx->ft_items_r.p;
+            a.n_items = (uint32_t)ir.size();
+            a.groups = ctx->ft_rgroups_r.p;
+            launch_rank(a, s);
+
+            ctx->ft_groups.upload(fg, s);
+            ctx->ft_corr_items.upload(ci, s);
+            ctx->ft_sel_items.upload(si, s);
+            ctx->ft_lq.upload(lqs, s);
+            ctx->ft_scores.ensure(std::max<int64_t>(sc_off, 1));
+            ctx->ft_label_scores.ensure(std::max<int64_t>(out_off, 1));
+            launch_ft_corr(fp32, ctx->ft_groups.p, ctx->ft_corr_items.p, (uint32_t)ci.size(), ctx->ft_qd.p,
+                           ctx->ft_rd.p, ctx->ft_qf.p, ctx->ft_rf.p, ctx->ft_qr.p, ctx->ft_rr.p, ctx->ft_qn.p,
+                           ctx->ft_rn.p, ctx->ft_scores.p, s);
+            float* scratch = ctx->sel_scratch.ensure((size_t)select_blocks_with_scratch() * 8 * max_label);
+            launch_ft_select(ctx->ft_groups.p, ctx->ft_sel_items.p, (uint32_t)si.size(), ctx->ft_lq.p, p,
+                             ctx->ft_scores.p, ctx->ft_label_scores.p, scratch, max_label, ctx->status.p, s);
+            std::vector<float> ls(out_off);
+            SGR_CUDA(cudaMemcpyAsync(ls.data(), ctx->ft_label_scores.p, out_off * sizeof(float),
+                                     cudaMemcpyDeviceToHost, s));
+            check_status(ctx);
+            // decisions, in each cell's own list order
+            for (uint32_t b = 0; b < nb; ++b) {
+                const Group& g = groups[batch[b]];
+                const FtGroup& f = fg[b];
+                for (uint32_t c = 0; c < g.cells.size(); ++c) {
+                    CellState& cs = st[g.cells[c]];
+                    std::vector<float> sc(cs.top.size());
+                    for (size_t i = 0; i < cs.top.size(); ++i) {
+                        const size_t j = std::lower_bound(g.labels.begin(), g.labels.end(), cs.top[i]) - g.labels.begin();
+                        sc[i] = ls[f.out_off + (int64_t)c * f.n_labels + j];
+                    }
+                    cs.top = decide(cs.top, sc, thre);
+                    cs.rounds++;
+                }
+            }
+        }
+    }
+    for (uint32_t i = 0; i < Q; ++i) {
+        final_labels[i] = st[i].top.empty() ? 0 : st[i].top.front();
+        if (rounds_out) rounds_out[i] = st[i].rounds;
+        ctx->prof.acc.ft_cell_rounds += st[i].rounds;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+sgr_status sgr_create(int gpuid, int cores, sgr_ctx** out) {
+    if (!out) return SGR_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (gpuid == -1) {  // host-only context: marker training and introspection, no device work
+        auto* ctx = new sgr_ctx();
+        ctx->device = -1;
+        ctx->cores = cores > 0 ? cores : 1;
+        *out = ctx;
+        return SGR_OK;
+    }
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || gpuid < 0 || gpuid >= n) {
+        cudaGetLastError();
+        return SGR_ERR_CUDA;
+    }
+    auto* ctx = new sgr_ctx();
+    ctx->device = gpuid;
+    ctx->cores = cores > 0 ? cores : 1;
+    if (cudaSetDevice(gpuid) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return SGR_ERR_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    *out = ctx;
+    return SGR_OK;
+}
+
+sgr_status sgr_destroy(sgr_ctx* ctx) {
+    if (!ctx) return SGR_OK;
+    if (ctx->device < 0) {
+        delete ctx;
+        return SGR_OK;
+    }
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaStream_t s = ctx->own_stream;
+    delete ctx;  // DevBuf destructors free device memory
+    if (s) cudaStreamDestroy(s);
+    return SGR_OK;
+}
+
+sgr_status sgr_set_stream(sgr_ctx* ctx, void* stream) {
+    if (!ctx || ctx->device < 0) return SGR_ERR_INVALID_ARGUMENT;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return SGR_OK;
+}
+
+sgr_status sgr_set_profiling(sgr_ctx* ctx, int on) {
+    if (!ctx) return SGR_ERR_INVALID_ARGUMENT;
+    ctx->prof.on = on != 0;
+    return SGR_OK;
+}
+
+sgr_status sgr_reset_timings(sgr_ctx* ctx) {
+    if (!ctx) return SGR_ERR_INVALID_ARGUMENT;
+    ctx->prof.acc = sgr_timings{};
+    return SGR_OK;
+}
+
+sgr_status sgr_get_timings(const sgr_ctx* ctx, sgr_timings* out) {
+    if (!ctx || !out) return SGR_ERR_INVALID_ARGUMENT;
+    *out = ctx->prof.acc;
+    return SGR_OK;
+}
+
+const char* sgr_last_error(const sgr_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+sgr_status sgr_set_mode(sgr_ctx* ctx, sgr_mode mode) {
+    if (!ctx) return SGR_ERR_INVALID_ARGUMENT;
+    if (mode != SGR_MODE_EXACT && mode != SGR_MODE_FP32REF) return SGR_ERR_INVALID_ARGUMENT;
+    ctx->mode = mode;
+    return SGR_OK;
+}
+
+sgr_status sgr_train_ref(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const char* const* label_names,
+                         uint32_t n_labels, const char* const* ref_genes, const char* const* qry_genes,
+                         uint32_t n_qry_genes) {
+    return guarded(ctx, [&] { train(ctx, ref, celltypes, label_names, n_labels, ref_genes, qry_genes, n_qry_genes); });
+}
+
+sgr_status sgr_score_first(sgr_ctx* ctx, const sgr_csr* qry, float quantile, float finetune_thre,
+                           int32_t* first_labels, float* label_scores, uint8_t* flags) {
+    return guarded(ctx, [&] {
+        if (!ctx->trained) fail(SGR_ERR_STATE, "score before train");
+        if (!first_labels) fail(SGR_ERR_INVALID_ARGUMENT, "null first_labels");
+        reset_status(ctx);
+        DevCsr q = query_on_device(ctx, qry);
+        if (q.n_rows == 0) return;
+        score_device(ctx, q, quantile, finetune_thre);
+        const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
+        cudaStream_t s = ctx->stream;
+        SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        if (label_scores)
+            SGR_CUDA(cudaMemcpyAsync(label_scores, ctx->label_scores.p, (size_t)Q * L * sizeof(float),
+                                     cudaMemcpyDeviceToHost, s));
+        if (flags)
+            SGR_CUDA(cudaMemcpyAsync(flags, ctx->flags.p, (size_t)Q * L, cudaMemcpyDeviceToHost, s));
+        check_status(ctx);
+    });
+}
+
+sgr_status sgr_finetune(sgr_ctx* ctx, const sgr_csr* qry, const uint8_t* flags, float quantile, float finetune_thre,
+                        int32_t finetune_times, int32_t* final_labels, int32_t* rounds) {
+    return guarded(ctx, [&] {
+        if (!ctx->trained) fail(SGR_ERR_STATE, "finetune before train");
+        if (!flags || !final_labels) fail(SGR_ERR_INVALID_ARGUMENT, "null flags or final_labels");
+        reset_status(ctx);
+        DevCsr q = query_on_device(ctx, qry);
+        if (q.n_rows == 0) return;
+        finetune_device(ctx, q, flags, quantile, finetune_thre, finetune_times, final_labels, rounds);
+    });
+}
+
+sgr_status sgr_annotate(sgr_ctx* ctx, const sgr_csr* qry, float quantile, float finetune_thre, int32_t finetune_times,
+                        int32_t* first_labels, int32_t* final_labels, float* label_scores) {
+    return guarded(ctx, [&] {
+        if (!ctx->trained) fail(SGR_ERR_STATE, "annotate before train");
+        if (!first_labels || !final_labels) fail(SGR_ERR_INVALID_ARGUMENT, "null output");
+        reset_status(ctx);
+        DevCsr q = query_on_device(ctx, qry);
+        if (q.n_rows == 0) return;
+        score_device(ctx, q, quantile, finetune_thre);
+        const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
+        cudaStream_t s = ctx->stream;
+        std::vector<uint8_t> fl((size_t)Q * L);
+        SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        SGR_CUDA(cudaMemcpyAsync(fl.data(), ctx->flags.p, fl.size(), cudaMemcpyDeviceToHost, s));
+        if (label_scores)
+            SGR_CUDA(cudaMemcpyAsync(label_scores, ctx->label_scores.p, (size_t)Q * L * sizeof(float),
+                                     cudaMemcpyDeviceToHost, s));
+        check_status(ctx);
+        finetune_device(ctx, q, fl.data(), quantile, finetune_thre, finetune_times, final_labels, nullptr);
+    });
+}
+
+sgr_status sgr_get_info(const sgr_ctx* ctx, sgr_info* out) {
+    if (!ctx || !out) return SGR_ERR_INVALID_ARGUMENT;
+    if (!ctx->markers_ready) return SGR_ERR_STATE;
+    out->n_labels = ctx->mk.n_labels;
+    out->n_genes = ctx->mk.W;
+    out->n_common = (uint32_t)ctx->mk.common.size();
+    out->n_thre = (uint32_t)ctx->mk.thre.size();
+    out->filter_genes = ctx->mk.filter_genes ? 1 : 0;
+    out->ref_rows = (uint32_t)ctx->mk.ref_order.size();
+    out->n_pair_genes = ctx->mk.pair_genes.size();
+    return SGR_OK;
+}
+
+sgr_status sgr_get_u32(const sgr_ctx* ctx, int what, uint32_t* out, uint64_t cap) {
+    if (!ctx || !out) return SGR_ERR_INVALID_ARGUMENT;
+    if (!ctx->markers_ready) return SGR_ERR_STATE;
+    const Markers& m = ctx->mk;
+    const std::vector<uint32_t>* v = nullptr;
+    switch (what) {
+        case 0: v = &m.common; break;
+        case 1: v = &m.thre; break;
+        case 2: v = &m.pair_genes; break;
+        case 3: v = &m.pair_idx; break;
+        case 4: v = &m.ft_genes; break;
+        case 5: v = &m.ft_idx; break;
+        case 6: v = &m.ctidx; break;
+        case 7: v = &m.ref_order; break;
+        default: return SGR_ERR_INVALID_ARGUMENT;
+    }
+    if (v->size() > cap) return SGR_ERR_INVALID_ARGUMENT;
+    std::copy(v->begin(), v->end(), out);
+    return SGR_OK;
+}
+
+sgr_status sgr_debug_ranks(sgr_ctx* ctx, const sgr_csr* rows, int which, int32_t* d_out) {
+    return guarded(ctx, [&] {
+        if (!ctx->trained) fail(SGR_ERR_STATE, "not trained");
+        cudaStream_t s = ctx->stream;
+        const int G = ctx->G, Kp = ctx->Kp;
+        uint32_t n;
+        std::vector<int8_t> limbs;
+        if (which == 1) {
+            n = ctx->R;
+            limbs.resize((size_t)n * 3 * Kp);
+            SGR_CUDA(cudaMemcpyAsync(limbs.data(), ctx->ref_limbs.p, limbs.size(), cudaMemcpyDeviceToHost, s));
+        } else {
+            reset_status(ctx);
+            DevCsr q = query_on_device(ctx, rows);
+            n = q.n_rows;
+            ctx->q_limbs.ensure((size_t)n * 3 * Kp);
+            ctx->q_n2.ensure(n);
+            ctx->q_rinv.ensure(n);
+            ctx->q_f32.ensure(n);
+            RankGroup g{ctx->qry_map_common.p, G, Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p};
+            rank_rows(ctx, q, g, RANK_LIMBS, NORM_NONE);
+            limbs.resize((size_t)n * 3 * Kp);
+            SGR_CUDA(cudaMemcpyAsync(limbs.data(), ctx->q_limbs.p, limbs.size(), cudaMemcpyDeviceToHost, s));
+            check_status(ctx);
+        }
+        SGR_CUDA(cudaStreamSynchronize(s));
+        for (uint32_t r = 0; r < n; ++r) {
+            const int8_t* row = limbs.data() + (size_t)r * 3 * Kp;
+            for (int i = 0; i < G; ++i) {
+                const int h = row[i], l = row[Kp + i], sm = row[2 * Kp + i];
+                if (sm != h + l) fail(SGR_ERR_STATE, "limb planes disagree");
+                d_out[(size_t)r * G + i] = 128 * h + l;
+            }
+        }
+    });
+}
+
+sgr_status sgr_debug_scores(sgr_ctx* ctx, const sgr_csr* qry, float* out) {
+    return guarded(ctx, [&] {
+        if (!ctx->trained) fail(SGR_ERR_STATE, "not trained");
+        reset_status(ctx);
+        DevCsr q = query_on_device(ctx, qry);
+        const uint32_t Q = q.n_rows, R = ctx->R;
+        const bool fp32 = ctx->mode == SGR_MODE_FP32REF;
+        cudaStream_t s = ctx->stream;
+        ctx->q_limbs.ensure((size_t)Q * 3 * ctx->Kp);
+        ctx->q_n2.ensure(Q);
+        ctx->q_rinv.ensure(Q);
+        ctx->q_f32.ensure(Q);
+        RankGroup g{ctx->qry_map_common.p, ctx->G, ctx->Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p};
+        rank_rows(ctx, q, g, RANK_LIMBS, fp32 ? NORM_SEQ : NORM_NONE);
+        DevBuf<float> sc;
+        sc.ensure((size_t)Q * R);
+        launch_corr_simt(fp32, ctx->q_limbs.p, ctx->ref_limbs.p, (int)Q, (int)R, ctx->G, ctx->Kp, ctx->q_f32.p,
+                         ctx->ref_f32.p, ctx->q_rinv.p, ctx->ref_rinv.p, ctx->q_n2.p, ctx->ref_n2.p, sc.p, R, s);
+        SGR_CUDA(cudaMemcpyAsync(out, sc.p, (size_t)Q * R * sizeof(float), cudaMemcpyDeviceToHost, s));
+        check_status(ctx);
+    });
+}
+
+void sgr_debug_stl_sort(float* v, int32_t n) {
+    int oob = 0;
+    stl::sort(v, n, &oob);
+}
+
+void sgr_debug_stl_minmax(const float* v, int32_t n, int32_t* mn, int32_t* mx) {
+    int a = 0, b = 0;
+    stl::minmax(v, n, &a, &b);
+    *mn = a;
+    *mx = b;
+}
+
+}  // extern "C"

@@ -1,0 +1,772 @@
+// Device kernels of the SingleR path (gather + rank, CSR compaction, SIMT correlation, per-label
+// quantile selection, fine-tune correlation and selection) for sm_100a.
+//
+// Reference kernels restated here (STOmics/cusingler src/cusingler.cu):
+//   csr2dense (204-281) + get_device_ref_lines (566-577) + csrFilter codes (src/io.cpp:470-523)
+//       -> rank_kernel: one warp per cell row gathers the row's marker entries straight from the
+//          CSR, sorts them in shared memory and writes tie-averaged doubled centred ranks.
+//   rankdata_bin3 / rankdata_batch / rankdata (745-801, 601-625, 158-179)
+//       -> the same half-integer ranks 1 + #less + (#equal - 1)/2, as d = 2*rank - (G+1).
+//   spearman (918-945)        -> corr_simt_kernel (fp32ref: fma chain over genes in order).
+//   spearman_reduce (803-856) -> ft_corr_kernel (fp32ref: 128 contiguous chunks + pairwise tree).
+//   percentile + get_label's argmax and flags (947-978, 1080-1133)
+//       -> select_first_kernel (radix selection of the two order statistics per label, libstdc++
+//          std::sort restated for NaN-bearing lists, std::minmax_element order for the argmax).
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <type_traits>
+
+#include "kernels.cuh"
+#include "sgr_internal.h"
+#include "stl_order.h"
+
+namespace sgr {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t ord_key(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ __forceinline__ float key_float(uint32_t k) {
+    uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    return __uint_as_float(u);
+}
+
+// -0 and +0 are one value (the reference keys its per-row value codes with std::set<float>).
+__device__ __forceinline__ float canon_zero(float v) {
+    uint32_t u = __float_as_uint(v);
+    return (u << 1) == 0 ? 0.0f : v;
+}
+
+// d = 128*h + l with l in [-64, 63]; s = h + l (the Karatsuba limb).
+__device__ __forceinline__ void split_limbs(int d, int& h, int& l, int& s) {
+    l = ((d + 64) & 127) - 64;
+    h = (d - l) >> 7;
+    s = h + l;
+}
+
+__device__ __forceinline__ int64_t warp_sum_i64(int64_t v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int lower_hi(const uint64_t* keys, int n, uint32_t hv) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if ((uint32_t)(keys[mid] >> 32) < hv) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int upper_hi(const uint64_t* keys, int n, uint32_t hv) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if ((uint32_t)(keys[mid] >> 32) <= hv) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Ascending bitonic sort of n (power of two) keys in shared memory by one warp.
+__device__ void warp_bitonic(uint64_t* keys, int n, int lane) {
+    for (int size = 2; size <= n; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = lane; t < (n >> 1); t += 32) {
+                int i = 2 * t - (t & (stride - 1));
+                int j = i + stride;
+                uint64_t a = keys[i], b = keys[j];
+                bool up = (i & size) == 0;
+                if ((a > b) == up) {
+                    keys[i] = b;
+                    keys[j] = a;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+__device__ __forceinline__ int stage_d(const unsigned char* stage, int mode, int Kp, int p) {
+    if (mode == RANK_LIMBS) {
+        const int8_t* s = reinterpret_cast<const int8_t*>(stage);
+        return 128 * (int)s[p] + (int)s[Kp + p];
+    }
+    return reinterpret_cast<const int16_t*>(stage)[p];
+}
+
+__device__ __forceinline__ void stage_put(unsigned char* stage, int mode, int Kp, int p, int d) {
+    if (mode == RANK_LIMBS) {
+        int h, l, s;
+        split_limbs(d, h, l, s);
+        int8_t* st = reinterpret_cast<int8_t*>(stage);
+        st[p] = (int8_t)h;
+        st[Kp + p] = (int8_t)l;
+        st[2 * Kp + p] = (int8_t)s;
+    } else {
+        reinterpret_cast<int16_t*>(stage)[p] = (int16_t)d;
+    }
+}
+
+__global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    uint64_t* keys = reinterpret_cast<uint64_t*>(smem + (size_t)warp * warp_bytes);
+    unsigned char* stage = reinterpret_cast<unsigned char*>(keys + a.cap);
+    for (uint32_t item = blockIdx.x * wpb + warp; item < a.n_items; item += gridDim.x * wpb) {
+        RankItem it;
+        if (a.items) {
+            it = a.items[item];
+        } else {
+            it.row = a.row0 + item;
+            it.group = 0;
+            it.slot = item;
+        }
+        const RankGroup g = a.groups[it.group];
+        const int G = g.G, Kp = g.Kp;
+        const int beg = a.indptr[it.row], end = a.indptr[it.row + 1];
+
+        // 1) compact the row's entries in the gene subset into (value key, position) sort keys
+        int k = 0, bad = 0;
+        for (int base = beg; base < end; base += 32) {
+            const int i = base + lane;
+            bool hit = false;
+            uint64_t key = 0;
+            if (i < end) {
+                const int c = __ldg(a.indices + i);
+                if ((unsigned)c >= a.n_cols) {
+                    bad |= 1;
+                } else {
+                    const int pos = __ldg(g.colmap + c);
+                    if (pos >= 0) {
+                        float v = __ldg(a.data + i);
+                        if (v != v) bad |= 2;
+                        v = canon_zero(v);
+                        hit = true;
+                        key = ((uint64_t)ord_key(v) << 32) | (uint32_t)pos;
+                    }
+                }
+            }
+            const unsigned m = __ballot_sync(FULL, hit);
+            if (hit) {
+                const int idx = k + __popc(m & ((1u << lane) - 1u));
+                if (idx < a.cap) keys[idx] = key;
+            }
+            k += __popc(m);
+        }
+        bad = __reduce_or_sync(FULL, bad);
+        if (bad && lane == 0) atomicOr(a.status, bad);
+        __syncwarp();
+        const bool fits = k <= a.cap;
+        if (fits && k > 1) {
+            int n = 1;
+            while (n < k) n <<= 1;
+            for (int i = k + lane; i < n; i += 32) keys[i] = ~0ull;
+            __syncwarp();
+            warp_bitonic(keys, n, lane);
+        }
+
+        // 2) every position of the subset starts as an implicit zero: rank (G-k+1)/2, d = -k;
+        //    the padding [G, Kp) is 0 so that it adds nothing to a dot product
+        const int d0 = -k;
+        if (a.out_mode == RANK_LIMBS) {
+            int h0, l0, s0;
+            split_limbs(d0, h0, l0, s0);
+            uint32_t* st = reinterpret_cast<uint32_t*>(stage);
+            for (int w = lane; w < 3 * Kp / 4; w += 32) {
+                const int plane = (4 * w) / Kp, pos = (4 * w) % Kp;
+                const uint32_t fb = (uint8_t)(int8_t)(plane == 0 ? h0 : plane == 1 ? l0 : s0);
+                uint32_t word = 0;
+                for (int b = 0; b < 4; ++b)
+                    if (pos + b < G) word |= fb << (8 * b);
+                st[w] = word;
+            }
+        } else {
+            int16_t* st = reinterpret_cast<int16_t*>(stage);
+            for (int p = lane; p < Kp; p += 32) st[p] = p < G ? (int16_t)d0 : (int16_t)0;
+        }
+        __syncwarp();
+
+        // 3) stored entries: d = 2 * (G - k + #less + (#equal + 1)/2) - (G + 1)
+        int64_t sq = 0;
+        if (fits) {
+            for (int j = lane; j < k; j += 32) {
+                const uint64_t key = keys[j];
+                const uint32_t hv = (uint32_t)(key >> 32);
+                const int lo = lower_hi(keys, k, hv), hi = upper_hi(keys, k, hv);
+                const int d = G - 2 * k + 2 * lo + (hi - lo);
+                stage_put(stage, a.out_mode, Kp, (int)(uint32_t)key, d);
+                sq += (int64_t)d * d;
+            }
+        } else {
+            // more entries than the sort buffer holds: count directly over the row
+            for (int i = beg + lane; i < end; i += 32) {
+                const int c = a.indices[i];
+                if ((unsigned)c >= a.n_cols) continue;
+                const int pos = g.colmap[c];
+                if (pos < 0) continue;
+                const float v = canon_zero(a.data[i]);
+                int less = 0, eq = 0;
+                for (int j = beg; j < end; ++j) {
+                    const int c2 = a.indices[j];
+                    if ((unsigned)c2 >= a.n_cols || g.colmap[c2] < 0) continue;
+                    const float w = canon_zero(a.data[j]);
+                    less += w < v;
+                    eq += w == v;
+                }
+                const int d = G - 2 * k + 2 * less + eq;
+                stage_put(stage, a.out_mode, Kp, pos, d);
+                sq += (int64_t)d * d;
+            }
+        }
+        sq = warp_sum_i64(sq);
+        __syncwarp();
+        const int64_t n2 = sq + (int64_t)(G - k) * k * k;
+        if (lane == 0) {
+            g.n2[it.slot] = n2;
+            g.rinv[it.slot] = n2 > 0 ? 1.0 / sqrt((double)n2) : 0.0;
+        }
+
+        // 4) FP32 self-norm in the reference's order (fp32ref mode only)
+        if (a.norm_mode == NORM_SEQ) {
+            if (lane == 0) {
+                float acc = 0.f;
+                for (int p = 0; p < G; ++p) {
+                    const float x = stage_d(stage, a.out_mode, Kp, p) * 0.5f;
+                    acc = fmaf(x, x, acc);
+                }
+                g.f32norm[it.slot] = acc;
+            }
+        } else if (a.norm_mode == NORM_TREE128) {
+            const int step = (G + 127) / 128;
+            float c[4];
+            for (int t = 0; t < 4; ++t) {
+                const int ch = 4 * lane + t;
+                float acc = 0.f;
+                for (int p = ch * step; p < (ch + 1) * step && p < G; ++p) {
+                    const float x = stage_d(stage, a.out_mode, Kp, p) * 0.5f;
+                    acc = fmaf(x, x, acc);
+                }
+                c[t] = acc;
+            }
+            float v = __fadd_rn(__fadd_rn(c[0], c[1]), __fadd_rn(c[2], c[3]));
+            for (int o = 1; o < 32; o <<= 1) {
+                const float w = __shfl_down_sync(FULL, v, o);
+                if ((lane & (2 * o - 1)) == 0) v = __fadd_rn(v, w);
+            }
+            if (lane == 0) g.f32norm[it.slot] = v;
+        }
+
+        // 5) coalesced write of the staged row
+        const int row_bytes = a.out_mode == RANK_LIMBS ? 3 * Kp : 2 * Kp;
+        uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(g.out) + (size_t)it.slot * row_bytes);
+        const uint4* src = reinterpret_cast<const uint4*>(stage);
+        for (int w = lane; w < row_bytes / 16; w += 32) dst[w] = src[w];
+        __syncwarp();
+    }
+}
+
+// ---- CSR compaction --------------------------------------------------------------------------
+
+__global__ void filter_count_kernel(const int32_t* indptr, const int32_t* indices, uint32_t n_rows, uint32_t n_cols,
+                                    const int32_t* map, int32_t* counts) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n_rows;
+         row += (gridDim.x * blockDim.x) >> 5) {
+        int cnt = 0;
+        for (int i = indptr[row] + lane; i < indptr[row + 1]; i += 32) {
+            const int c = indices[i];
+            cnt += ((unsigned)c < n_cols && map[c] >= 0);
+        }
+        cnt = __reduce_add_sync(FULL, cnt);
+        if (lane == 0) counts[row] = cnt;
+    }
+}
+
+__global__ void filter_fill_kernel(const float* data, const int32_t* indptr, const int32_t* indices, uint32_t n_rows,
+                                   uint32_t n_cols, const int32_t* map, const int32_t* out_ptr, float* out_data,
+                                   int32_t* out_indices) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n_rows;
+         row += (gridDim.x * blockDim.x) >> 5) {
+        int base = out_ptr[row];
+        const int beg = indptr[row], end = indptr[row + 1];
+        for (int i0 = beg; i0 < end; i0 += 32) {
+            const int i = i0 + lane;
+            int nc = -1;
+            if (i < end) {
+                const int c = indices[i];
+                if ((unsigned)c < n_cols) nc = map[c];
+            }
+            const unsigned m = __ballot_sync(FULL, nc >= 0);
+            if (nc >= 0) {
+                const int o = base + __popc(m & ((1u << lane) - 1u));
+                out_data[o] = data[i];
+                out_indices[o] = nc;
+            }
+            base += __popc(m);
+        }
+    }
+}
+
+// Exclusive scan of n values into out[0..n] (out[n] = total) by one block of 1024 threads.
+__global__ void __launch_bounds__(1024) scan_kernel(const int32_t* in, int32_t* out, uint32_t n) {
+    __shared__ int32_t warp_tot[32];
+    __shared__ int32_t carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < n; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const int32_t v = i < n ? in[i] : 0;
+        int32_t x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(FULL, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int32_t t = warp_tot[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t y = __shfl_up_sync(FULL, t, o);
+                if (lane >= o) t += y;
+            }
+            warp_tot[lane] = t;
+        }
+        __syncthreads();
+        const int32_t excl = carry + (warp ? warp_tot[warp - 1] : 0) + x - v;
+        if (i < n) out[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[n] = carry;
+}
+
+// ---- score-step correlation on CUDA cores -----------------------------------------------------
+//
+// 128 x 128 output tile per block, 8 x 8 per thread, genes in ascending order (BK = 8), so each
+// output is one fused multiply-add chain over genes 0..G-1 exactly as the reference's spearman
+// kernel accumulates it.  Padding genes hold d = 0 and leave the chain unchanged.
+template <bool FP32>
+__global__ void __launch_bounds__(256) corr_simt_kernel(const int8_t* A, const int8_t* B, int nq, int R, int G,
+                                                        int Kp, const float* fa, const float* fb, const double* ra,
+                                                        const double* rb, const int64_t* na, const int64_t* nb,
+                                                        float* out, int64_t ld) {
+    using T = typename std::conditional<FP32, float, double>::type;
+    __shared__ T As[8][132];
+    __shared__ T Bs[8][132];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int m0 = blockIdx.y * 128, n0 = blockIdx.x * 128;
+    const int lr = threadIdx.x >> 1, lk = (threadIdx.x & 1) * 4;
+    T acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = T(0);
+    const int Kend = (G + 7) & ~7;
+    for (int k0 = 0; k0 < Kend; k0 += 8) {
+        {
+            const int q = m0 + lr;
+            uint32_t h4 = 0, l4 = 0;
+            if (q < nq) {
+                const int8_t* row = A + (size_t)q * 3 * Kp;
+                h4 = *reinterpret_cast<const uint32_t*>(row + k0 + lk);
+                l4 = *reinterpret_cast<const uint32_t*>(row + Kp + k0 + lk);
+            }
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int d = 128 * (int)(int8_t)(h4 >> (8 * b)) + (int)(int8_t)(l4 >> (8 * b));
+                As[lk + b][lr] = FP32 ? T(d * 0.5f) : T(d);
+            }
+        }
+        {
+            const int r = n0 + lr;
+            uint32_t h4 = 0, l4 = 0;
+            if (r < R) {
+                const int8_t* row = B + (size_t)r * 3 * Kp;
+                h4 = *reinterpret_cast<const uint32_t*>(row + k0 + lk);
+                l4 = *reinterpret_cast<const uint32_t*>(row + Kp + k0 + lk);
+            }
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int d = 128 * (int)(int8_t)(h4 >> (8 * b)) + (int)(int8_t)(l4 >> (8 * b));
+                Bs[lk + b][lr] = FP32 ? T(d * 0.5f) : T(d);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+            T av[8], bv[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) av[i] = As[kk][ty * 8 + i];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) bv[j] = Bs[kk][tx * 8 + j];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int q = m0 + ty * 8 + i;
+        if (q >= nq) continue;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int r = n0 + tx * 8 + j;
+            if (r >= R) continue;
+            float s;
+            if (FP32) {
+                const float div = sqrtf(fa[q] * fb[r]);
+                s = div != 0.f ? (float)acc[i][j] / div : __int_as_float(0x7fffffff);
+            } else {
+                s = (na[q] == 0 || nb[r] == 0) ? __int_as_float(0x7fffffff)
+                                               : (float)(((double)acc[i][j] * ra[q]) * rb[r]);
+            }
+            out[(size_t)q * ld + r] = s;
+        }
+    }
+}
+
+// ---- per-label quantile ------------------------------------------------------------------------
+
+__device__ __forceinline__ float interp(float p, float prev_index, float step, float a, float b) {
+    // (p - prev_index) * (b - a) / step + a, each operation rounded once (src/cusingler.cu:975)
+    return __fadd_rn(__fdiv_rn(__fmul_rn(__fsub_rn(p, prev_index), __fsub_rn(b, a)), step), a);
+}
+
+__device__ __forceinline__ int warp_incl_scan(int x, int lane) {
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// Key of the j-th smallest (0-based) of v[0..n) by 4 passes of an 8-bit radix histogram.
+__device__ uint32_t warp_select(const float* v, int n, int j, int* hist, int lane) {
+    uint32_t prefix = 0, mask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int b = lane; b < 256; b += 32) hist[b] = 0;
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            const uint32_t u = ord_key(v[i]);
+            if ((u & mask) == prefix) atomicAdd(&hist[(u >> shift) & 255], 1);
+        }
+        __syncwarp();
+        int c[8], s = 0;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            c[t] = hist[8 * lane + t];
+            s += c[t];
+        }
+        const int incl = warp_incl_scan(s, lane), excl = incl - s;
+        const unsigned own = __ballot_sync(FULL, excl <= j && j < incl);
+        const int src = __ffs(own) - 1;
+        int bin = 0, before = 0;
+        if (lane == src) {
+            int acc = excl;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                if (j < acc + c[t]) {
+                    bin = 8 * lane + t;
+                    before = acc;
+                    break;
+                }
+                acc += c[t];
+            }
+        }
+        bin = __shfl_sync(FULL, bin, src);
+        before = __shfl_sync(FULL, before, src);
+        j -= before;
+        prefix |= (uint32_t)bin << shift;
+        mask |= 0xffu << shift;
+        __syncwarp();
+    }
+    return prefix;
+}
+
+__device__ __forceinline__ uint32_t warp_min_u32(uint32_t x) { return __reduce_min_sync(FULL, x); }
+__device__ __forceinline__ uint32_t warp_max_u32(uint32_t x) { return __reduce_max_sync(FULL, x); }
+
+// The reference's percentile(v, n, p) (src/cusingler.cu:947-978) for one score list, by one warp.
+// Lists holding NaN are sorted exactly as libstdc++ would, in `scratch` (n floats), by lane 0.
+__device__ float quantile_warp(const float* v, const LabelQ& lq, float p, int* hist, float* scratch, int lane,
+                               int* status) {
+    const int n = lq.len;
+    if (lq.kind == 0) return v[0];
+    bool nan = false;
+    for (int i = lane; i < n; i += 32) nan |= (v[i] != v[i]);
+    nan = __any_sync(FULL, nan);
+    if (nan) {
+        float r = 0.f;
+        if (scratch == nullptr) {
+            if (lane == 0) atomicOr(status, 8);
+            return __int_as_float(0x7fffffff);
+        }
+        for (int i = lane; i < n; i += 32) scratch[i] = v[i];
+        __syncwarp();
+        if (lane == 0) {
+            int oob = 0;
+            stl::sort(scratch, n, &oob);
+            if (oob) atomicOr(status, 4);
+            if (lq.kind == 1) r = scratch[0];
+            else if (lq.kind == 2) r = scratch[n - 1];
+            else r = interp(p, lq.prev_index, lq.step, scratch[lq.k - 1], scratch[lq.k]);
+        }
+        __syncwarp();
+        return __shfl_sync(FULL, r, 0);
+    }
+    if (lq.kind == 1 || lq.kind == 2) {
+        uint32_t m = lq.kind == 1 ? 0xffffffffu : 0u;
+        for (int i = lane; i < n; i += 32) {
+            const uint32_t u = ord_key(v[i]);
+            m = lq.kind == 1 ? min(m, u) : max(m, u);
+        }
+        m = lq.kind == 1 ? warp_min_u32(m) : warp_max_u32(m);
+        return key_float(m);
+    }
+    const uint32_t ka = warp_select(v, n, lq.k - 1, hist, lane);
+    int le = 0;
+    uint32_t nxt = 0xffffffffu;
+    for (int i = lane; i < n; i += 32) {
+        const uint32_t u = ord_key(v[i]);
+        le += u <= ka;
+        if (u > ka) nxt = min(nxt, u);
+    }
+    le = __reduce_add_sync(FULL, le);
+    nxt = warp_min_u32(nxt);
+    const uint32_t kb = le > lq.k ? ka : nxt;
+    return interp(p, lq.prev_index, lq.step, key_float(ka), key_float(kb));
+}
+
+__global__ void __launch_bounds__(256) select_first_kernel(const float* scores, int64_t ld, int nq, int L,
+                                                           const LabelQ* lq, float p, float thre, const int64_t* qn2,
+                                                           float* label_scores, int32_t* first, uint8_t* flags,
+                                                           float* scratch, int64_t spw, int* status) {
+    __shared__ float ls[256];
+    __shared__ int hist[8][256];
+    __shared__ int s_mx;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* my_scratch = scratch ? scratch + (size_t)(blockIdx.x * 8 + warp) * spw : nullptr;
+    for (int q = blockIdx.x; q < nq; q += gridDim.x) {
+        const float* row = scores + (size_t)q * ld;
+        const bool qnan = qn2[q] == 0;
+        for (int l = warp; l < L; l += 8) {
+            const LabelQ d = lq[l];
+            float r;
+            if (qnan) r = __int_as_float(0x7fffffff);
+            else r = quantile_warp(row + d.start, d, p, hist[warp], my_scratch, lane, status);
+            if (lane == 0) ls[l] = r;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int mn, mx;
+            stl::minmax(ls, L, &mn, &mx);
+            s_mx = mx;
+            first[q] = mx;
+        }
+        __syncthreads();
+        const float t = __fsub_rn(ls[s_mx], thre);
+        for (int l = threadIdx.x; l < L; l += blockDim.x) {
+            label_scores[(size_t)q * L + l] = ls[l];
+            if (flags) flags[(size_t)q * L + l] = ls[l] >= t ? 1 : 0;
+        }
+        __syncthreads();
+    }
+}
+
+// ---- fine-tune correlation and selection ------------------------------------------------------
+
+template <bool FP32>
+__global__ void __launch_bounds__(256) ft_corr_kernel(const FtGroup* groups, const FtCorrItem* items, uint32_t n_items,
+                                                      const int16_t* qd, const int16_t* rd, const float* qf,
+                                                      const float* rf, const double* qr, const double* rr,
+                                                      const int64_t* qn, const int64_t* rn, float* scores) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t wpb = blockDim.x >> 5;
+    for (uint32_t w = blockIdx.x * wpb + (threadIdx.x >> 5); w < n_items; w += gridDim.x * wpb) {
+        const FtCorrItem it = items[w];
+        const FtGroup g = groups[it.group];
+        const int G = g.G, Kp = g.Kp;
+        const int step = (G + 127) / 128;
+        const int64_t rrow = g.r_row + it.ref;
+        const int16_t* y = rd + g.r_el + (int64_t)it.ref * Kp;
+        for (uint32_t q = it.q_begin; q < it.q_end; ++q) {
+            const int64_t qrow = g.q_row + q;
+            const int16_t* x = qd + g.q_el + (int64_t)q * Kp;
+            float s;
+            if (FP32) {
+                float c[4];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const int ch = 4 * lane + t;
+                    float acc = 0.f;
+                    for (int i = ch * step; i < (ch + 1) * step && i < G; ++i)
+                        acc = fmaf(x[i] * 0.5f, y[i] * 0.5f, acc);
+                    c[t] = acc;
+                }
+                float v = __fadd_rn(__fadd_rn(c[0], c[1]), __fadd_rn(c[2], c[3]));
+                for (int o = 1; o < 32; o <<= 1) {
+                    const float u = __shfl_down_sync(FULL, v, o);
+                    if ((lane & (2 * o - 1)) == 0) v = __fadd_rn(v, u);
+                }
+                const float div = sqrtf(qf[qrow] * rf[rrow]);
+                s = div != 0.f ? v / div : __int_as_float(0x7fffffff);
+            } else {
+                int64_t acc = 0;
+                for (int i = lane; i < G; i += 32) acc += (int32_t)x[i] * (int32_t)y[i];
+                acc = warp_sum_i64(acc);
+                s = (qn[qrow] == 0 || rn[rrow] == 0) ? __int_as_float(0x7fffffff)
+                                                     : (float)(((double)acc * qr[qrow]) * rr[rrow]);
+            }
+            if (lane == 0) scores[g.s_off + (int64_t)q * g.n_ref + it.ref] = s;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) ft_select_kernel(const FtGroup* groups, const FtSelItem* items, uint32_t n_items,
+                                                        const LabelQ* lq, float p, const float* scores,
+                                                        float* label_scores, float* scratch, int64_t spw,
+                                                        int* status) {
+    __shared__ int hist[8][256];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* my_scratch = scratch ? scratch + (size_t)(blockIdx.x * 8 + warp) * spw : nullptr;
+    for (uint32_t w = blockIdx.x * 8 + warp; w < n_items; w += gridDim.x * 8) {
+        const FtSelItem it = items[w];
+        const FtGroup g = groups[it.group];
+        const float* row = scores + g.s_off + (int64_t)it.cell * g.n_ref;
+        for (int j = 0; j < g.n_labels; ++j) {
+            const LabelQ d = lq[g.lq_off + j];
+            const float r = quantile_warp(row + d.start, d, p, hist[warp], my_scratch, lane, status);
+            if (lane == 0) label_scores[g.out_off + (int64_t)it.cell * g.n_labels + j] = r;
+        }
+    }
+}
+
+std::atomic<uint64_t> g_launches{0};
+
+}  // namespace
+
+uint64_t launch_count() { return g_launches.load(); }
+void count_launch(uint64_t n) { g_launches += n; }
+
+int device_sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+namespace {
+int sm_count() { return device_sm_count(); }
+}  // namespace
+
+void launch_rank(const RankLaunch& a, cudaStream_t s) {
+    if (a.n_items == 0) return;
+    const int stage_bytes = a.out_mode == RANK_LIMBS ? 3 * a.max_Kp : 2 * a.max_Kp;
+    const int warp_bytes = ((a.cap * 8 + stage_bytes) + 15) & ~15;
+    const int budget = 200 * 1024;
+    int wpb = budget / warp_bytes;
+    if (wpb > 8) wpb = 8;
+    if (wpb < 1) fail(SGR_ERR_UNSUPPORTED, "gene subset too wide for the rank kernel's shared memory");
+    const int smem = wpb * warp_bytes;
+    SGR_CUDA(cudaFuncSetAttribute(rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int per_sm = std::max(1, std::min(8, (228 * 1024) / (smem + 1024)));
+    long blocks = ((long)a.n_items + wpb - 1) / wpb;
+    blocks = std::min<long>(blocks, (long)sm_count() * per_sm * 4);
+    rank_kernel<<<(unsigned)blocks, 32 * wpb, smem, s>>>(a, warp_bytes);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+void launch_filter_count(const int32_t* indptr, const int32_t* indices, uint32_t n_rows, uint32_t n_cols,
+                         const int32_t* map, int32_t* counts, cudaStream_t s) {
+    if (!n_rows) return;
+    const unsigned blocks = std::min<unsigned>((n_rows + 7) / 8, sm_count() * 16);
+    filter_count_kernel<<<blocks, 256, 0, s>>>(indptr, indices, n_rows, n_cols, map, counts);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+void launch_exclusive_scan(const int32_t* in, int32_t* out, uint32_t n, int32_t*, cudaStream_t s) {
+    scan_kernel<<<1, 1024, 0, s>>>(in, out, n);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+void launch_filter_fill(const float* data, const int32_t* indptr, const int32_t* indices, uint32_t n_rows,
+                        uint32_t n_cols, const int32_t* map, const int32_t* out_ptr, float* out_data,
+                        int32_t* out_indices, cudaStream_t s) {
+    if (!n_rows) return;
+    const unsigned blocks = std::min<unsigned>((n_rows + 7) / 8, sm_count() * 16);
+    filter_fill_kernel<<<blocks, 256, 0, s>>>(data, indptr, indices, n_rows, n_cols, map, out_ptr, out_data,
+                                              out_indices);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+void launch_corr_simt(bool fp32ref, const int8_t* A, const int8_t* B, int nq, int R, int G, int Kp, const float* fa,
+                      const float* fb, const double* ra, const double* rb, const int64_t* na, const int64_t* nb,
+                      float* scores, int64_t ld, cudaStream_t s) {
+    if (nq <= 0 || R <= 0) return;
+    dim3 grid((R + 127) / 128, (nq + 127) / 128);
+    if (fp32ref)
+        corr_simt_kernel<true><<<grid, 256, 0, s>>>(A, B, nq, R, G, Kp, fa, fb, ra, rb, na, nb, scores, ld);
+    else
+        corr_simt_kernel<false><<<grid, 256, 0, s>>>(A, B, nq, R, G, Kp, fa, fb, ra, rb, na, nb, scores, ld);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+void launch_select_first(const float* scores, int64_t ld, int nq, int L, const LabelQ* lq, float p, float thre,
+                         const int64_t* qn2, float* label_scores, int32_t* first, uint8_t* flags, float* scratch,
+                         int64_t spw, int* status, cudaStream_t s) {
+    if (nq <= 0) return;
+    const unsigned blocks = scratch ? (unsigned)std::min<long>(nq, sm_count() * 2)
+                                    : (unsigned)std::min<long>(nq, sm_count() * 8);
+    select_first_kernel<<<blocks, 256, 0, s>>>(scores, ld, nq, L, lq, p, thre, qn2, label_scores, first, flags,
+                                               scratch, spw, status);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+void launch_ft_corr(bool fp32ref, const FtGroup* groups, const FtCorrItem* items, uint32_t n_items, const int16_t* qd,
+                    const int16_t* rd, const float* qf, const float* rf, const double* qr, const double* rr,
+                    const int64_t* qn, const int64_t* rn, float* scores, cudaStream_t s) {
+    if (!n_items) return;
+    const unsigned blocks = std::min<unsigned>((n_items + 7) / 8, sm_count() * 16);
+    if (fp32ref)
+        ft_corr_kernel<true><<<blocks, 256, 0, s>>>(groups, items, n_items, qd, rd, qf, rf, qr, rr, qn, rn, scores);
+    else
+        ft_corr_kernel<false><<<blocks, 256, 0, s>>>(groups, items, n_items, qd, rd, qf, rf, qr, rr, qn, rn, scores);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+void launch_ft_select(const FtGroup* groups, const FtSelItem* items, uint32_t n_items, const LabelQ* lq, float p,
+                      const float* scores, float* label_scores, float* scratch, int64_t spw, int* status,
+                      cudaStream_t s) {
+    if (!n_items) return;
+    const unsigned blocks = scratch ? (unsigned)std::min<long>((n_items + 7) / 8, sm_count() * 2)
+                                    : (unsigned)std::min<long>((n_items + 7) / 8, sm_count() * 8);
+    ft_select_kernel<<<blocks, 256, 0, s>>>(groups, items, n_items, lq, p, scores, label_scores, scratch, spw, status);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+}  // namespace sgr

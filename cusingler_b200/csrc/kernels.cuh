@@ -1,0 +1,130 @@
+// Device kernels of the SingleR path and their launch helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace sgr {
+
+int device_sm_count();
+
+// Kernels launched by this process's library (read before and after a call to count its launches).
+uint64_t launch_count();
+void count_launch(uint64_t n = 1);
+
+// Grid caps of the selection kernels; their scratch (NaN-bearing lists) is sized per warp of the
+// capped grid.
+inline int select_blocks_with_scratch() { return device_sm_count() * 2; }
+
+// ---- gather + rank ----------------------------------------------------------------------------
+//
+// A "rank group" is one gene subset: a column map from input column to position in [0, G) (or -1),
+// its width G, the padded width Kp (multiple of 128) and where its rows go.
+struct RankGroup {
+    const int32_t* colmap;  // input column -> position, -1 if not in the subset
+    int32_t G;
+    int32_t Kp;
+    void* out;              // LIMBS: int8 [rows][3*Kp] planes H|L|S; D16: int16 [rows][Kp]
+    int64_t* n2;            // per row: sum of d^2 (exact)
+    double* rinv;           // per row: 1/sqrt(n2), 0 when n2 == 0
+    float* f32norm;         // per row, fp32 reference-order sum of x^2 (x = d/2), or nullptr
+};
+
+struct RankItem {
+    uint32_t row;    // input CSR row
+    uint32_t group;  // index into the group table
+    uint32_t slot;   // output row within the group
+    uint32_t pad;
+};
+
+enum RankOut { RANK_LIMBS = 0, RANK_D16 = 1 };
+enum F32Norm { NORM_NONE = 0, NORM_SEQ = 1, NORM_TREE128 = 2 };
+
+struct RankLaunch {
+    const float* data;
+    const int32_t* indices;
+    const int32_t* indptr;
+    uint32_t n_cols;            // input column count (bounds check)
+    const RankItem* items;      // nullptr: item i is row row0 + i of group 0, slot i
+    uint32_t row0;
+    uint32_t n_items;
+    const RankGroup* groups;    // device array
+    int out_mode;               // RankOut
+    int norm_mode;              // F32Norm
+    int max_Kp;                 // largest Kp over the groups (smem sizing)
+    int cap;                    // sort capacity per warp (power of two)
+    int* status;                // device flags: bit0 column out of range, bit1 NaN value
+};
+
+void launch_rank(const RankLaunch& a, cudaStream_t s);
+
+// Compact a CSR to the columns with map[c] >= 0 (new column = map[c]); two passes.
+void launch_filter_count(const int32_t* indptr, const int32_t* indices, uint32_t n_rows, uint32_t n_cols,
+                         const int32_t* map, int32_t* counts, cudaStream_t s);
+void launch_exclusive_scan(const int32_t* in, int32_t* out, uint32_t n, int32_t* scratch, cudaStream_t s);
+void launch_filter_fill(const float* data, const int32_t* indptr, const int32_t* indices, uint32_t n_rows,
+                        uint32_t n_cols, const int32_t* map, const int32_t* out_ptr, float* out_data,
+                        int32_t* out_indices, cudaStream_t s);
+
+// ---- score-step correlation on CUDA cores -------------------------------------------------------
+//
+// scores[q - q0][r] for q in [q0, q0 + nq), r in [0, R): A/B are LIMBS rows (3*Kp bytes).
+// fp32ref: fused multiply-add chain over genes in order (the reference's spearman kernel order).
+// exact:   FP64 accumulation of the integer products (exact), FP64 normalisation.
+void launch_corr_simt(bool fp32ref, const int8_t* A, const int8_t* B, int nq, int R, int G, int Kp,
+                      const float* fa, const float* fb, const double* ra, const double* rb,
+                      const int64_t* na, const int64_t* nb, float* scores, int64_t ld, cudaStream_t s);
+
+// ---- per-label quantile, argmax, candidate flags ------------------------------------------------
+struct LabelQ {
+    int32_t start;       // first column of the label's scores in a score row
+    int32_t len;
+    int32_t kind;        // 0 single value, 1 minimum, 2 maximum, 3 interpolate between k-1 and k
+    int32_t k;
+    float prev_index;    // index[k-1] of the reference's float index grid
+    float step;          // the grid step 1/(len-1) as float
+    int32_t has_nan;     // some reference row of the label has zero variance
+    int32_t pad;
+};
+
+void launch_select_first(const float* scores, int64_t ld, int nq, int L, const LabelQ* lq, float p,
+                         float thre, const int64_t* qn2, float* label_scores, int32_t* first, uint8_t* flags,
+                         float* scratch, int64_t scratch_per_warp, int* status, cudaStream_t s);
+
+// ---- fine-tune ----------------------------------------------------------------------------------
+struct FtGroup {
+    int32_t G;             // genes of the round's subset
+    int32_t Kp;            // padded row length of d16 rows
+    int32_t n_cells;       // query cells in the group
+    int32_t n_ref;         // reference rows of the candidate labels
+    int64_t q_el;          // first element of the group's d16 query rows
+    int64_t r_el;          // first element of the group's d16 reference rows
+    int64_t q_row;         // first per-row norm index of the group's query rows
+    int64_t r_row;         // first per-row norm index of the group's reference rows
+    int64_t s_off;         // first score (floats) of the group's n_cells x n_ref block
+    int32_t n_labels;      // candidate labels of the group
+    int32_t lq_off;        // first LabelQ of the group (label segments inside a score row)
+    int64_t out_off;       // first label score of the group's n_cells x n_labels block
+};
+
+struct FtCorrItem {
+    uint32_t group;
+    uint32_t ref;          // reference row within the group
+    uint32_t q_begin, q_end;
+};
+
+void launch_ft_corr(bool fp32ref, const FtGroup* groups, const FtCorrItem* items, uint32_t n_items,
+                    const int16_t* qd, const int16_t* rd, const float* qf, const float* rf, const double* qr,
+                    const double* rr, const int64_t* qn, const int64_t* rn, float* scores, cudaStream_t s);
+
+struct FtSelItem {
+    uint32_t group;
+    uint32_t cell;         // query cell within the group
+};
+
+void launch_ft_select(const FtGroup* groups, const FtSelItem* items, uint32_t n_items, const LabelQ* lq,
+                      float p, const float* scores, float* label_scores, float* scratch,
+                      int64_t scratch_per_warp, int* status, cudaStream_t s);
+
+}  // namespace sgr

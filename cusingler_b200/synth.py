@@ -10,7 +10,7 @@ There is no public dataset in this environment, so every workload is generated:
   cells, which is what gives per-label medians (and so marker genes) their signal;
 * stored value ``log2(1 + x)`` as float32, CSR rows with ascending column indices and no explicit
   zeros;
-* label proportions ``~ Dirichlet(1)``; each label has a marker block of genes whose mean is
+* label proportions ``~ Dirichlet(1)`` floored at ``1/(4L)``; each label has a marker block of genes whose mean is
   multiplied by a factor.  Family configurations give every label of a family a shared block plus a
   few label-specific genes with a small factor, so labels inside a family are near-identical.
 
@@ -94,7 +94,11 @@ def make_world(wl: Workload, seed: int = 0) -> World:
     rng = np.random.default_rng([seed, 7919])
     W, L = wl.n_genes, wl.n_labels
     mu = np.exp(rng.uniform(np.log(0.5), np.log(20.0), size=W))
+    # Dirichlet(1) proportions, floored at 1/(4L) so that every label has reference cells (the
+    # reference cannot handle a label without any)
     props = rng.dirichlet(np.ones(L))
+    props = np.maximum(props, 0.25 / L)
+    props = props / props.sum()
     factor = np.ones((L, W), dtype=np.float32)
     perm = rng.permutation(W)
     pos = 0

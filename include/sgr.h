@@ -1,0 +1,169 @@
+/* sgr.h -- C ABI of the B200 SingleR annotation path (library: cusingler_b200/_lib/libsgr.so).
+ *
+ * The reference keeps its device path behind seven C++ free functions over file-scope globals
+ * (src/cusingler.cuh:13-23 of STOmics/cusingler): initGPU, copyin_score, get_label, destroy_score,
+ * copyin, cufinetune, destroy; the host stages live in DataParser (src/io.h:16-107).  This header
+ * replaces that seam with an opaque context, plain pointers and sizes, and status codes instead
+ * of exit().  Each entry point names the reference interface it replaces.
+ *
+ * Threading: one context is used by one host thread at a time.  Contexts are independent.
+ * Memory: unless a sgr_csr says on_device = 1, every pointer is host memory; the library copies
+ * what it needs and never keeps a caller pointer past the call.
+ */
+#ifndef SGR_H_
+#define SGR_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum sgr_status {
+    SGR_OK = 0,
+    SGR_ERR_INVALID_ARGUMENT = 1, /* malformed CSR, out-of-range code, bad size            */
+    SGR_ERR_CUDA = 2,             /* a CUDA runtime call failed (message in last_error)    */
+    SGR_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed                              */
+    SGR_ERR_NO_INTERSECTION = 4,  /* reference and query share no gene name                */
+    SGR_ERR_EMPTY_LABEL = 5,      /* a label name has no reference cell                    */
+    SGR_ERR_UNSUPPORTED = 6,      /* a size beyond what this build supports                */
+    SGR_ERR_STATE = 7,            /* call order violated (e.g. score before train)         */
+    SGR_ERR_TIMEOUT = 8           /* a bounded device wait ran out                          */
+} sgr_status;
+
+/* Arithmetic of the rank correlation.
+ *  SGR_MODE_EXACT   integer numerator on the INT8 tensor cores (doubled centred ranks split in two
+ *                   int8 limbs, int32 accumulation, int64 recombination), FP64 normalisation,
+ *                   rounded once to float.  Default.
+ *  SGR_MODE_FP32REF the reference's own FP32 operation order, reproduced bit for bit (CUDA cores).
+ */
+typedef enum sgr_mode { SGR_MODE_EXACT = 0, SGR_MODE_FP32REF = 1 } sgr_mode;
+
+/* A CSR matrix (rows = cells, columns = genes), the h5ad /X layout the reference reads
+ * (test/test_basic.py:7-15).  Column indices of a row must be distinct; they need not be sorted. */
+typedef struct sgr_csr {
+    uint32_t n_rows;
+    uint32_t n_cols;
+    const float* data;      /* indptr[n_rows] values                                    */
+    const int32_t* indices; /* indptr[n_rows] column ids                                */
+    const int32_t* indptr;  /* n_rows + 1 offsets, indptr[0] == 0                       */
+    int32_t on_device;      /* 0: host memory; 1: device memory of the context's GPU    */
+} sgr_csr;
+
+typedef struct sgr_ctx sgr_ctx;
+
+/* Replaces initGPU (src/cusingler.cu:74-90): selects `gpuid`, creates a stream and the context.
+ * `cores` is the host thread count for marker training (DataParser(thread_num), src/io.h:19).
+ * gpuid == -1 makes a host-only context: sgr_train_ref then runs the marker training alone (for
+ * inspection through sgr_get_info / sgr_get_u32) and the device stages return SGR_ERR_STATE. */
+sgr_status sgr_create(int gpuid, int cores, sgr_ctx** out);
+
+/* Replaces destroy / destroy_score (src/cusingler.cu:92-130): frees everything the context owns. */
+sgr_status sgr_destroy(sgr_ctx* ctx);
+
+/* Message of the last failed call on this context ("" if none).  Valid until the next call. */
+const char* sgr_last_error(const sgr_ctx* ctx);
+
+sgr_status sgr_set_mode(sgr_ctx* ctx, sgr_mode mode);
+
+/* Replaces PyDataParser::prepareData + findIntersectionGenes + loadRefData + trainData
+ * (src/io.cpp:792-821, 306-349, 351-370, 141-262) and the reference half of copyin_score /
+ * copyin (src/cusingler.cu:283-521): intersects gene names, regroups reference rows by label,
+ * trains the per-label-pair marker lists on the host, and leaves the ranked reference resident on
+ * the device.  `celltypes[i]` is the label code of reference row i, narrowed to 8 bits as
+ * src/io.cpp:813 does; `label_names` has n_labels entries.  The query gene names are needed here
+ * because the gene intersection decides the reference's columns. */
+sgr_status sgr_train_ref(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes,
+                         const char* const* label_names, uint32_t n_labels,
+                         const char* const* ref_genes, const char* const* qry_genes,
+                         uint32_t n_qry_genes);
+
+/* Replaces copyin_score + get_label (src/cusingler.cu:283-413, 986-1136): per query cell, the
+ * per-label `quantile` (a fraction, e.g. 0.8f) of its correlations with that label's reference
+ * cells, the first label (last index of the maximum, as std::minmax_element gives) and the
+ * candidate flags (score >= max - finetune_thre).  Outputs are host arrays:
+ * first_labels[n_rows]; label_scores[n_rows * n_labels] and flags[n_rows * n_labels] may be NULL. */
+sgr_status sgr_score_first(sgr_ctx* ctx, const sgr_csr* qry, float quantile, float finetune_thre,
+                           int32_t* first_labels, float* label_scores, uint8_t* flags);
+
+/* Replaces copyin + cufinetune (src/cusingler.cu:415-521, 1297-1333): starting from the candidate
+ * flags (n_rows * n_labels, nonzero = candidate), repeats the fine-tune round until one label is
+ * left (or finetune_times rounds when it is > 0) and writes final_labels[n_rows] (0 when a cell has
+ * no candidate, as the reference does).  rounds (n_rows, may be NULL) receives the round count. */
+sgr_status sgr_finetune(sgr_ctx* ctx, const sgr_csr* qry, const uint8_t* flags, float quantile,
+                        float finetune_thre, int32_t finetune_times, int32_t* final_labels,
+                        int32_t* rounds);
+
+/* Both steps in one call (Pipeline::score + Pipeline::finetune, src/pipeline.cpp:47-111).
+ * label_scores may be NULL. */
+sgr_status sgr_annotate(sgr_ctx* ctx, const sgr_csr* qry, float quantile, float finetune_thre,
+                        int32_t finetune_times, int32_t* first_labels, int32_t* final_labels,
+                        float* label_scores);
+
+/* Runs the context's work on `stream` (a cudaStream_t of the context's device; NULL restores the
+ * context's own stream).  Calls stay synchronous: they return after their results are on the host. */
+sgr_status sgr_set_stream(sgr_ctx* ctx, void* stream);
+
+/* ---- Measurement --------------------------------------------------------------------------- */
+
+/* Per-stage device times of the calls since the last sgr_reset_timings, measured with CUDA events
+ * on the context's stream while profiling is on (sgr_set_profiling(ctx, 1)). */
+typedef struct sgr_timings {
+    double h2d_ms;          /* query upload (host inputs only)                                 */
+    double rank_ms;         /* score-step gather + rank of the query                            */
+    double corr_ms;         /* score-step correlation                                            */
+    double select_ms;       /* score-step quantile / argmax / flags                              */
+    double finetune_ms;     /* whole fine-tune (device time of its stages plus host decisions)   */
+    double total_ms;        /* first to last event of the calls                                  */
+    uint64_t launches;      /* kernels launched                                                  */
+    uint64_t corr_launches;
+    uint64_t rank_launches;
+    uint64_t rank_bytes;    /* algorithmic bytes of the score-step gather + rank                 */
+    uint64_t corr_ops;      /* algorithmic ops 2*Q*R*G of the score-step correlation             */
+    uint64_t cells;         /* query cells annotated                                             */
+    uint64_t ft_cell_rounds;/* fine-tune (cell, round) pairs                                     */
+} sgr_timings;
+
+sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
+sgr_status sgr_reset_timings(sgr_ctx* ctx);
+sgr_status sgr_get_timings(const sgr_ctx* ctx, sgr_timings* out);
+
+/* ---- Introspection (tests and tools) ------------------------------------------------------- */
+
+typedef struct sgr_info {
+    uint32_t n_labels;
+    uint32_t n_genes;        /* gene space of the trained reference (its column count)        */
+    uint32_t n_common;       /* marker genes of the score step (G)                             */
+    uint32_t n_thre;         /* marker genes the fine-tune lists draw from                     */
+    uint32_t filter_genes;   /* 1 when the gene names differed and were intersected             */
+    uint32_t ref_rows;
+    uint64_t n_pair_genes;   /* length of the concatenated per-pair marker lists               */
+} sgr_info;
+
+sgr_status sgr_get_info(const sgr_ctx* ctx, sgr_info* out);
+
+/* what: 0 common genes (ascending), 1 thre genes (ascending), 2 per-pair positive marker lists
+ * (concatenated, gene ids), 3 their (start, len) per ordered label pair (2 * L * L),
+ * 4 fine-tune pair lists (thre-compact ids), 5 their (start, len) (2 * L * L), 6 (start, len) of
+ * each label in the regrouped reference (2 * L), 7 original row of each regrouped reference row.
+ * `cap` is the capacity of `out` in elements. */
+sgr_status sgr_get_u32(const sgr_ctx* ctx, int what, uint32_t* out, uint64_t cap);
+
+/* Doubled centred ranks d = 2 * rank - (G + 1) over the common genes, computed on the device by
+ * the score-step gather kernel, for every row of `rows` (host copy, n_rows * n_common int32).
+ * which: 0 the query rows given, 1 the trained reference (rows ignored). */
+sgr_status sgr_debug_ranks(sgr_ctx* ctx, const sgr_csr* rows, int which, int32_t* d_out);
+
+/* Raw score-step correlations (n_rows x ref_rows, float, host) of the query rows. */
+sgr_status sgr_debug_scores(sgr_ctx* ctx, const sgr_csr* qry, float* out);
+
+/* The device routines that restate libstdc++'s std::sort and std::minmax_element orders (used by
+ * the quantile and argmax kernels for NaN-bearing score lists), run on the host for testing. */
+void sgr_debug_stl_sort(float* v, int32_t n);
+void sgr_debug_stl_minmax(const float* v, int32_t n, int32_t* min_idx, int32_t* max_idx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SGR_H_ */

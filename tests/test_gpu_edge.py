@@ -1,0 +1,125 @@
+"""Edge cases on the GPU: empty query, constant rows (NaN scores), one-cell labels, unsorted CSR
+columns, gene-name intersection, malformed inputs, and the drop-in module."""
+
+import numpy as np
+import pytest
+
+from cusingler_b200 import abi, synth
+from oracle import oracle as O
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def _csr_from_rows(rows, n_cols):
+    data, idx, ptr = [], [], [0]
+    for r in rows:
+        for c, v in r:
+            idx.append(c)
+            data.append(v)
+        ptr.append(len(idx))
+    return synth.CSR(len(rows), n_cols, np.array(data, np.float32), np.array(idx, np.int32),
+                     np.array(ptr, np.int32), np.zeros(len(rows), np.int32))
+
+
+def _run_both(prob, mode):
+    a = abi.Annotator(gpuid=0, mode=mode)
+    a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
+    first, scores, flags = a.score_first(prob.qry)
+    final, rounds = a.finetune(prob.qry, flags)
+    orc = O.Oracle(prob)
+    orc.train()
+    of, os_, ofl, _ = orc.score(mode=0 if mode == abi.MODE_FP32REF else 1)
+    ofin, orounds = orc.finetune(mode=0 if mode == abi.MODE_FP32REF else 1)
+    assert H.ulp_diff(scores, os_).max() == 0
+    assert np.array_equal(first, of)
+    assert np.array_equal(flags, ofl.astype(np.uint8))
+    assert np.array_equal(final, ofin)
+    assert np.array_equal(rounds, orounds)
+    return first, final
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_FP32REF, abi.MODE_EXACT])
+def test_constant_and_empty_rows(mode):
+    """Constant query rows give all-NaN scores (first label = last label, no flags, final 0);
+    constant reference rows make NaN-bearing score lists sorted in libstdc++'s order."""
+    ref, qry, L = H.dataset("tiny")
+    rows_q = [list(zip(qry.indices[qry.indptr[i]:qry.indptr[i + 1]], qry.data[qry.indptr[i]:qry.indptr[i + 1]]))
+              for i in range(40)]
+    rows_q[3] = []                       # all implicit zeros
+    rows_q[5] = [(c, 1.0) for c in range(qry.n_cols)]  # every gene equal
+    rows_r = [list(zip(ref.indices[ref.indptr[i]:ref.indptr[i + 1]], ref.data[ref.indptr[i]:ref.indptr[i + 1]]))
+              for i in range(ref.n_rows)]
+    for i in (0, 1, 50, 51, 52):
+        rows_r[i] = []
+    q = _csr_from_rows(rows_q, qry.n_cols)
+    r = _csr_from_rows(rows_r, ref.n_cols)
+    prob = O.Problem(r, q, synth.names("CT", L), ref.labels, synth.names("G", ref.n_cols),
+                     synth.names("G", qry.n_cols))
+    first, final = _run_both(prob, mode)
+    assert first[3] == L - 1 and final[3] == 0
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_FP32REF, abi.MODE_EXACT])
+def test_single_cell_labels_and_unsorted_columns(mode):
+    ref, qry, L = H.dataset("tiny")
+    codes = ref.labels.copy()
+    codes[0] = L          # two extra labels with one reference cell each
+    codes[1] = L + 1
+    rng = np.random.default_rng(0)
+    qd, qi = qry.data.copy(), qry.indices.copy()
+    for i in range(qry.n_rows):   # shuffle column order within each query row
+        a, b = qry.indptr[i], qry.indptr[i + 1]
+        p = rng.permutation(b - a)
+        qd[a:b], qi[a:b] = qd[a:b][p], qi[a:b][p]
+    q = synth.CSR(qry.n_rows, qry.n_cols, qd, qi, qry.indptr, qry.labels)
+    prob = O.Problem(ref, q, synth.names("CT", L + 2), codes, synth.names("G", ref.n_cols),
+                     synth.names("G", qry.n_cols))
+    _run_both(prob, mode)
+
+
+def test_gene_intersection():
+    ref, qry, L = H.dataset("tiny")
+    rg = synth.names("G", ref.n_cols)
+    qg = synth.names("G", qry.n_cols)
+    for i in range(0, len(qg), 9):
+        qg[i] = f"Q{i}"
+    prob = O.Problem(ref, qry, synth.names("CT", L), ref.labels, rg, qg)
+    _run_both(prob, abi.MODE_FP32REF)
+
+
+def test_empty_query_and_errors():
+    ref, qry, L = H.dataset("tiny")
+    a = abi.Annotator(gpuid=0)
+    a.train(ref, ref.labels, synth.names("CT", L), synth.names("G", ref.n_cols), synth.names("G", qry.n_cols))
+    empty = synth.CSR(0, qry.n_cols, np.zeros(0, np.float32), np.zeros(0, np.int32), np.zeros(1, np.int32),
+                      np.zeros(0, np.int32))
+    first, scores, flags = a.score_first(empty)
+    assert first.shape == (0,)
+    bad = synth.CSR(2, qry.n_cols, np.ones(2, np.float32), np.array([1, qry.n_cols + 5], np.int32),
+                    np.array([0, 1, 2], np.int32), np.zeros(2, np.int32))
+    with pytest.raises(abi.SgrError) as e:
+        a.score_first(bad)
+    assert e.value.status == 1
+    nanq = synth.CSR(1, qry.n_cols, np.array([np.nan], np.float32), np.array([int(a.u32(0)[0])], np.int32),
+                     np.array([0, 1], np.int32), np.zeros(1, np.int32))
+    with pytest.raises(abi.SgrError):
+        a.score_first(nanq)
+    # the context stays usable after an error
+    first, _, _ = a.score_first(qry)
+    assert first.shape == (qry.n_rows,)
+
+
+def test_dropin_run_matches_oracle():
+    from cusingler import cusingler
+    prob = H.problem("tiny")
+    ref, qry = prob.ref, prob.qry
+    cells = [f"cell{i}" for i in range(qry.n_rows)]
+    res = cusingler.run(8, 0, ref.n_rows, ref.n_cols, ref.data, ref.indices, ref.indptr,
+                        qry.n_rows, qry.n_cols, qry.data, qry.indices, qry.indptr,
+                        prob.label_names, prob.celltypes, cells, prob.ref_genes, prob.qry_genes,
+                        quantile=80, finetune_thre=0.05, finetune_times=0)
+    o = H.oracle_run("tiny", 1)
+    assert [r[0] for r in res] == cells
+    assert [r[1] for r in res] == [prob.label_names[i] for i in o["first"]]
+    assert [r[2] for r in res] == [prob.label_names[i] for i in o["final"]]

@@ -1,0 +1,97 @@
+"""GPU parity through the C ABI against the oracle.
+
+Bars: ranks and gene indices bit-exact; fp32ref mode scores bit-exact with the oracle's restatement
+of the reference's FP32 order (so labels are identical); exact mode scores bit-exact with the
+oracle's exact formula, within 1e-5 absolute of the FP32 reference order, and labels identical
+except at documented near-ties.
+"""
+
+import numpy as np
+import pytest
+
+from cusingler_b200 import abi
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+KINDS = ["tiny", "families", "small"]
+
+
+def annotator(kind, mode):
+    prob = H.problem(kind)
+    a = abi.Annotator(gpuid=0, cores=8, mode=mode)
+    a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
+    return a, prob
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_ranks_bit_exact(kind):
+    a, prob = annotator(kind, abi.MODE_EXACT)
+    res = H.oracle_run(kind, 1)
+    orc = res["oracle"]
+    d_ref = a.debug_ranks()
+    d_qry = a.debug_ranks(prob.qry)
+    for r in range(0, prob.ref.n_rows, max(1, prob.ref.n_rows // 200)):
+        assert np.array_equal(d_ref[r], orc.rank_row(0, r)), r
+    for q in range(prob.qry.n_rows):
+        assert np.array_equal(d_qry[q], orc.rank_row(1, q)), q
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_scores_fp32ref_bit_exact(kind):
+    a, prob = annotator(kind, abi.MODE_FP32REF)
+    raw = a.debug_scores(prob.qry)
+    ref = H.oracle_run(kind, 0)["raw"]
+    assert H.ulp_diff(raw, ref).max() == 0
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_scores_exact(kind):
+    a, prob = annotator(kind, abi.MODE_EXACT)
+    raw = a.debug_scores(prob.qry)
+    exact = H.oracle_run(kind, 1)["raw"]
+    fp32 = H.oracle_run(kind, 0)["raw"]
+    assert H.ulp_diff(raw, exact).max() == 0
+    assert np.nanmax(np.abs(raw - fp32)) < 1e-5
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("mode", [abi.MODE_FP32REF, abi.MODE_EXACT])
+def test_first_labels_and_flags(kind, mode):
+    a, prob = annotator(kind, mode)
+    first, scores, flags = a.score_first(prob.qry)
+    res = H.oracle_run(kind, 0 if mode == abi.MODE_FP32REF else 1)
+    assert H.ulp_diff(scores, res["scores"]).max() == 0
+    assert np.array_equal(first, res["first"])
+    assert np.array_equal(flags, res["flags"].astype(np.uint8))
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("mode", [abi.MODE_FP32REF, abi.MODE_EXACT])
+def test_final_labels(kind, mode):
+    a, prob = annotator(kind, mode)
+    res = H.oracle_run(kind, 0 if mode == abi.MODE_FP32REF else 1)
+    final, rounds = a.finetune(prob.qry, res["flags"].astype(np.uint8))
+    assert np.array_equal(final, res["final"])
+    assert np.array_equal(rounds, res["rounds"])
+
+
+@pytest.mark.parametrize("times", [1, 2])
+def test_finetune_times(times):
+    a, prob = annotator("tiny", abi.MODE_FP32REF)
+    res = H.oracle_run("tiny", 0, times)
+    final, rounds = a.finetune(prob.qry, res["flags"].astype(np.uint8), times=times)
+    assert np.array_equal(final, res["final"])
+    assert rounds.max() <= times
+
+
+def test_annotate_matches_steps():
+    a, prob = annotator("small", abi.MODE_EXACT)
+    first, final, scores = a.annotate(prob.qry, with_scores=True)
+    res = H.oracle_run("small", 1)
+    assert np.array_equal(first, res["first"]) and np.array_equal(final, res["final"])
+    fp = H.oracle_run("small", 0)
+    # exact vs the reference's FP32 order: scores within 1e-5, labels equal unless at a near-tie
+    assert np.nanmax(np.abs(scores - fp["scores"])) < 1e-5
+    assert (first != fp["first"]).sum() == 0
+    assert (final != fp["final"]).sum() <= 1
