@@ -8,6 +8,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <map>
 #include <set>
@@ -154,6 +156,35 @@ int pow2_at_least(int v) {
 }
 
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// SGR_TRACE=1 prints per-round fine-tune statistics and phase times to stderr (diagnostics only:
+// it synchronises after each phase, so traced runs are slower).
+bool trace_on() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("SGR_TRACE");
+        on = (e && *e && *e != '0') ? 1 : 0;
+    }
+    return on == 1;
+}
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct PhaseClock {
+    cudaStream_t s;
+    bool on;
+    double t;
+    PhaseClock(cudaStream_t s_) : s(s_), on(trace_on()), t(now_ms()) {}
+    double lap() {
+        if (!on) return 0;
+        cudaStreamSynchronize(s);
+        double n = now_ms(), d = n - t;
+        t = n;
+        return d;
+    }
+};
 
 template <class F>
 sgr_status guarded(sgr_ctx* ctx, F&& f) {
@@ -538,6 +569,11 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
             groups[it->second].cells.push_back(i);
         }
         if (groups.empty()) break;
+        if (trace_on()) {
+            size_t cells = 0;
+            for (auto& g : groups) cells += g.cells.size();
+            fprintf(stderr, "[sgr ft] round: %zu active cells in %zu candidate sets\n", cells, groups.size());
+        }
         // sets with fewer than 20 genes keep their first candidate (src/cusingler.cu:1158-1159)
         std::vector<uint32_t> work;
         for (uint32_t gi = 0; gi < groups.size(); ++gi) {
@@ -567,6 +603,7 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
                 bytes += b;
             }
             // tables
+            PhaseClock pc(s);
             const uint32_t nb = (uint32_t)batch.size();
             std::vector<int32_t> maps((size_t)nb * Wt, -1);
             std::vector<FtGroup> fg(nb);
@@ -634,6 +671,7 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
                 rgr[b] = RankGroup{map, f.G, f.Kp, ctx->ft_rd.p + f.r_el, ctx->ft_rn.p + f.r_row,
                                    ctx->ft_rr.p + f.r_row, ctx->ft_rf.p + f.r_row};
             }
+            const double t_host = pc.lap();
             ctx->ft_rgroups_q.upload(rgq, s);
             ctx->ft_rgroups_r.upload(rgr, s);
             ctx->ft_items_q.upload(iq, s);
@@ -652,6 +690,7 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
             a.n_items = (uint32_t)iq.size();
             a.groups = ctx->ft_rgroups_q.p;
             launch_rank(a, s);
+            const double t_rank_q = pc.lap();
             a.data = rf.data;
             a.indices = rf.indices;
             a.indptr = rf.indptr;
@@ -660,6 +699,7 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
             a.n_items = (uint32_t)ir.size();
             a.groups = ctx->ft_rgroups_r.p;
             launch_rank(a, s);
+            const double t_rank_r = pc.lap();
 
             ctx->ft_groups.upload(fg, s);
             ctx->ft_corr_items.upload(ci, s);
@@ -670,6 +710,7 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
             launch_ft_corr(fp32, ctx->ft_groups.p, ctx->ft_corr_items.p, (uint32_t)ci.size(), ctx->ft_qd.p,
                            ctx->ft_rd.p, ctx->ft_qf.p, ctx->ft_rf.p, ctx->ft_qr.p, ctx->ft_rr.p, ctx->ft_qn.p,
                            ctx->ft_rn.p, ctx->ft_scores.p, s);
+            const double t_corr = pc.lap();
             float* scratch = ctx->sel_scratch.ensure((size_t)select_blocks_with_scratch() * 8 * max_label);
             launch_ft_select(ctx->ft_groups.p, ctx->ft_sel_items.p, (uint32_t)si.size(), ctx->ft_lq.p, p,
                              ctx->ft_scores.p, ctx->ft_label_scores.p, scratch, max_label, ctx->status.p, s);
@@ -677,6 +718,7 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
             SGR_CUDA(cudaMemcpyAsync(ls.data(), ctx->ft_label_scores.p, out_off * sizeof(float),
                                      cudaMemcpyDeviceToHost, s));
             check_status(ctx);
+            const double t_sel = pc.lap();
             // decisions, in each cell's own list order
             for (uint32_t b = 0; b < nb; ++b) {
                 const Group& g = groups[batch[b]];
@@ -692,6 +734,12 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
                     cs.rounds++;
                 }
             }
+            if (trace_on())
+                fprintf(stderr,
+                        "[sgr ft] batch groups=%u cells=%zu ref_rows=%zu corr_items=%zu maxKp=%d | host %.2f "
+                        "rank_q %.2f rank_r %.2f corr %.2f select %.2f decide %.2f ms\n",
+                        nb, iq.size(), ir.size(), ci.size(), maxKp, t_host, t_rank_q, t_rank_r, t_corr, t_sel,
+                        pc.lap());
         }
     }
     for (uint32_t i = 0; i < Q; ++i) {
