@@ -110,6 +110,13 @@ struct sgr_ctx {
     std::vector<int64_t> h_ref_n2;
     DevBuf<float> reff_data;
     DevBuf<int32_t> reff_indices, reff_indptr;
+    DevBuf<uint32_t> ref_sorted;       // thre-pool entries of each reference row, by value
+    DevBuf<uint32_t> d_ctidx, d_ft_genes, d_ft_idx;
+    DevBuf<int32_t> d_gene_thre;
+    DevBuf<LabelQ> d_lq_label;
+    DevBuf<int> next_cell;
+    DevBuf<int32_t> d_final, d_rounds;
+    DevBuf<float> ft_scratch;
 
     // per-call query buffers
     DevBuf<float> q_data;
@@ -376,6 +383,7 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     ctx->markers_ready = true;
     if (ctx->device < 0) return;  // host-only context: marker training only
     if (ctx->G > 8128) fail(SGR_ERR_UNSUPPORTED, "more than 8128 score-step marker genes");
+    if (ctx->Wt > 40000) fail(SGR_ERR_UNSUPPORTED, "fine-tune gene pool above 40000 genes");
 
     // regrouped reference CSR
     std::vector<int32_t> indptr(ctx->R + 1, 0);
@@ -411,8 +419,20 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     rank_rows(ctx, rm, g, RANK_LIMBS, NORM_SEQ);
     ctx->h_ref_n2.resize(ctx->R);
     SGR_CUDA(cudaMemcpyAsync(ctx->h_ref_n2.data(), ctx->ref_n2.p, ctx->R * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    // fine-tune: reference compacted to the thre pool
+    // fine-tune: reference compacted to the thre pool, each row's entries sorted by value
     filter_csr(ctx, rm, ctx->ref_map_thre.p, ctx->reff_data, ctx->reff_indices, ctx->reff_indptr);
+    int32_t reff_nnz = 0;
+    SGR_CUDA(cudaMemcpyAsync(&reff_nnz, ctx->reff_indptr.p + ctx->R, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SGR_CUDA(cudaStreamSynchronize(s));
+    ctx->ref_sorted.ensure(std::max<int32_t>(reff_nnz, 1));
+    launch_ref_presort(ctx->reff_data.p, ctx->reff_indices.p, ctx->reff_indptr.p, ctx->R,
+                       std::min(pow2_at_least(std::max<int>(ctx->Wt, 32)), 8192), ctx->ref_sorted.p, s);
+    ctx->d_ctidx.upload(mk.ctidx, s);
+    ctx->d_ft_genes.upload(mk.ft_genes.empty() ? std::vector<uint32_t>{0} : mk.ft_genes, s);
+    ctx->d_ft_idx.upload(mk.ft_idx, s);
+    std::vector<int32_t> gt(mk.n_labels + 1, 0);
+    for (uint32_t n = 1; n <= mk.n_labels; ++n) gt[n] = marker_count(n);
+    ctx->d_gene_thre.upload(gt, s);
     check_status(ctx);
     ctx->trained = true;
 }
@@ -749,6 +769,71 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
     }
 }
 
+// Exact-mode fine-tune: the persistent kernel over a device work queue.  `flags_dev` is the
+// Q x L candidate-flag matrix in device memory.
+void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev, float p, float thre, int times,
+                         int32_t* final_labels, int32_t* rounds_out) {
+    cudaStream_t s = ctx->stream;
+    const Markers& mk = ctx->mk;
+    const uint32_t Q = q.n_rows, L = mk.n_labels, Wt = ctx->Wt;
+    const int sp_ft = ctx->prof.begin(ST_FT, s);
+    filter_csr(ctx, q, ctx->qry_map_thre.p, ctx->qf_data, ctx->qf_indices, ctx->qf_indptr);
+    uint32_t max_label = 1;
+    std::vector<LabelQ> lq(L);
+    for (uint32_t l = 0; l < L; ++l) {
+        max_label = std::max(max_label, mk.ctidx[2 * l + 1]);
+        lq[l] = make_lq(0, (int)mk.ctidx[2 * l + 1], p);
+    }
+    ctx->d_lq_label.upload(lq, s);
+    const int capq = std::min(pow2_at_least(std::max<int>(Wt, 32)), 8192);
+    const size_t smem = ft_persistent_smem((int)std::max<uint32_t>(Wt, 1), capq);
+    if (smem > 220 * 1024) fail(SGR_ERR_UNSUPPORTED, "fine-tune gene pool too wide for shared memory");
+    const int grid = ft_persistent_grid(smem);
+    const int64_t per_cta = (int64_t)ctx->R + 8 * (int64_t)max_label;
+    ctx->ft_scratch.ensure((size_t)grid * per_cta);
+    ctx->next_cell.ensure(1);
+    SGR_CUDA(cudaMemsetAsync(ctx->next_cell.p, 0, sizeof(int), s));
+    ctx->d_final.ensure(Q);
+    ctx->d_rounds.ensure(Q);
+    FtPersistentArgs a{};
+    a.ref_sorted = ctx->ref_sorted.p;
+    a.ref_ptr = ctx->reff_indptr.p;
+    a.ctidx = ctx->d_ctidx.p;
+    a.ft_genes = ctx->d_ft_genes.p;
+    a.ft_idx = ctx->d_ft_idx.p;
+    a.gene_thre = ctx->d_gene_thre.p;
+    a.lq_label = ctx->d_lq_label.p;
+    a.L = (int)L;
+    a.Wt = (int)std::max<uint32_t>(Wt, 1);
+    a.qf_data = ctx->qf_data.p;
+    a.qf_idx = ctx->qf_indices.p;
+    a.qf_ptr = ctx->qf_indptr.p;
+    a.Q = (int)Q;
+    a.flags = flags_dev;
+    a.p = p;
+    a.thre = thre;
+    a.times = times;
+    a.next_cell = ctx->next_cell.p;
+    a.final_labels = ctx->d_final.p;
+    a.rounds = ctx->d_rounds.p;
+    a.scratch = ctx->ft_scratch.p;
+    a.scratch_per_cta = per_cta;
+    a.max_rcand = (int)ctx->R;
+    a.max_label = (int)max_label;
+    a.capq = capq;
+    a.status = ctx->status.p;
+    launch_ft_persistent(a, grid, smem, s);
+    ctx->prof.end(sp_ft, s);
+    SGR_CUDA(cudaMemcpyAsync(final_labels, ctx->d_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    std::vector<int32_t> rounds(Q);
+    SGR_CUDA(cudaMemcpyAsync(rounds.data(), ctx->d_rounds.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    check_status(ctx);
+    for (uint32_t i = 0; i < Q; ++i) {
+        if (rounds_out) rounds_out[i] = rounds[i];
+        ctx->prof.acc.ft_cell_rounds += rounds[i];
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -865,7 +950,12 @@ sgr_status sgr_finetune(sgr_ctx* ctx, const sgr_csr* qry, const uint8_t* flags, 
         reset_status(ctx);
         DevCsr q = query_on_device(ctx, qry);
         if (q.n_rows == 0) return;
-        finetune_device(ctx, q, flags, quantile, finetune_thre, finetune_times, final_labels, rounds);
+        if (ctx->mode == SGR_MODE_EXACT) {
+            ctx->flags.upload(flags, (size_t)q.n_rows * ctx->mk.n_labels, ctx->stream);
+            finetune_persistent(ctx, q, ctx->flags.p, quantile, finetune_thre, finetune_times, final_labels, rounds);
+        } else {
+            finetune_device(ctx, q, flags, quantile, finetune_thre, finetune_times, final_labels, rounds);
+        }
     });
 }
 
@@ -880,14 +970,18 @@ sgr_status sgr_annotate(sgr_ctx* ctx, const sgr_csr* qry, float quantile, float 
         score_device(ctx, q, quantile, finetune_thre);
         const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
         cudaStream_t s = ctx->stream;
-        std::vector<uint8_t> fl((size_t)Q * L);
         SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        SGR_CUDA(cudaMemcpyAsync(fl.data(), ctx->flags.p, fl.size(), cudaMemcpyDeviceToHost, s));
         if (label_scores)
             SGR_CUDA(cudaMemcpyAsync(label_scores, ctx->label_scores.p, (size_t)Q * L * sizeof(float),
                                      cudaMemcpyDeviceToHost, s));
-        check_status(ctx);
-        finetune_device(ctx, q, fl.data(), quantile, finetune_thre, finetune_times, final_labels, nullptr);
+        if (ctx->mode == SGR_MODE_EXACT) {
+            finetune_persistent(ctx, q, ctx->flags.p, quantile, finetune_thre, finetune_times, final_labels, nullptr);
+        } else {
+            std::vector<uint8_t> fl((size_t)Q * L);
+            SGR_CUDA(cudaMemcpyAsync(fl.data(), ctx->flags.p, fl.size(), cudaMemcpyDeviceToHost, s));
+            check_status(ctx);
+            finetune_device(ctx, q, fl.data(), quantile, finetune_thre, finetune_times, final_labels, nullptr);
+        }
     });
 }
 

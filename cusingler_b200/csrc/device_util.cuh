@@ -1,0 +1,195 @@
+// Device helpers shared by the kernels: ordered float keys, warp sorts and searches, and the
+// per-label quantile of the reference's percentile() (src/cusingler.cu:947-978 of
+// STOmics/cusingler) by radix selection, with libstdc++'s sort order for NaN-bearing lists.
+#pragma once
+
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "stl_order.h"
+
+namespace sgr {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t ord_key(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ __forceinline__ float key_float(uint32_t k) {
+    uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    return __uint_as_float(u);
+}
+
+// -0 and +0 are one value (the reference keys its per-row value codes with std::set<float>).
+__device__ __forceinline__ float canon_zero(float v) {
+    uint32_t u = __float_as_uint(v);
+    return (u << 1) == 0 ? 0.0f : v;
+}
+
+// d = 128*h + l with l in [-64, 63]; s = h + l (the Karatsuba limb).
+__device__ __forceinline__ void split_limbs(int d, int& h, int& l, int& s) {
+    l = ((d + 64) & 127) - 64;
+    h = (d - l) >> 7;
+    s = h + l;
+}
+
+__device__ __forceinline__ int64_t warp_sum_i64(int64_t v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int lower_hi(const uint64_t* keys, int n, uint32_t hv) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if ((uint32_t)(keys[mid] >> 32) < hv) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int upper_hi(const uint64_t* keys, int n, uint32_t hv) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if ((uint32_t)(keys[mid] >> 32) <= hv) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Ascending bitonic sort of n (power of two) keys in shared memory by one warp.
+__device__ void warp_bitonic(uint64_t* keys, int n, int lane) {
+    for (int size = 2; size <= n; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = lane; t < (n >> 1); t += 32) {
+                int i = 2 * t - (t & (stride - 1));
+                int j = i + stride;
+                uint64_t a = keys[i], b = keys[j];
+                bool up = (i & size) == 0;
+                if ((a > b) == up) {
+                    keys[i] = b;
+                    keys[j] = a;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+__device__ __forceinline__ float interp(float p, float prev_index, float step, float a, float b) {
+    // (p - prev_index) * (b - a) / step + a, each operation rounded once (src/cusingler.cu:975)
+    return __fadd_rn(__fdiv_rn(__fmul_rn(__fsub_rn(p, prev_index), __fsub_rn(b, a)), step), a);
+}
+
+__device__ __forceinline__ int warp_incl_scan(int x, int lane) {
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// Key of the j-th smallest (0-based) of v[0..n) by 4 passes of an 8-bit radix histogram.
+__device__ uint32_t warp_select(const float* v, int n, int j, int* hist, int lane) {
+    uint32_t prefix = 0, mask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int b = lane; b < 256; b += 32) hist[b] = 0;
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            const uint32_t u = ord_key(v[i]);
+            if ((u & mask) == prefix) atomicAdd(&hist[(u >> shift) & 255], 1);
+        }
+        __syncwarp();
+        int c[8], s = 0;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            c[t] = hist[8 * lane + t];
+            s += c[t];
+        }
+        const int incl = warp_incl_scan(s, lane), excl = incl - s;
+        const unsigned own = __ballot_sync(FULL, excl <= j && j < incl);
+        const int src = __ffs(own) - 1;
+        int bin = 0, before = 0;
+        if (lane == src) {
+            int acc = excl;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                if (j < acc + c[t]) {
+                    bin = 8 * lane + t;
+                    before = acc;
+                    break;
+                }
+                acc += c[t];
+            }
+        }
+        bin = __shfl_sync(FULL, bin, src);
+        before = __shfl_sync(FULL, before, src);
+        j -= before;
+        prefix |= (uint32_t)bin << shift;
+        mask |= 0xffu << shift;
+        __syncwarp();
+    }
+    return prefix;
+}
+
+__device__ __forceinline__ uint32_t warp_min_u32(uint32_t x) { return __reduce_min_sync(FULL, x); }
+__device__ __forceinline__ uint32_t warp_max_u32(uint32_t x) { return __reduce_max_sync(FULL, x); }
+
+// The reference's percentile(v, n, p) (src/cusingler.cu:947-978) for one score list, by one warp.
+// Lists holding NaN are sorted exactly as libstdc++ would, in `scratch` (n floats), by lane 0.
+__device__ float quantile_warp(const float* v, const LabelQ& lq, float p, int* hist, float* scratch, int lane,
+                               int* status) {
+    const int n = lq.len;
+    if (lq.kind == 0) return v[0];
+    bool nan = false;
+    for (int i = lane; i < n; i += 32) nan |= (v[i] != v[i]);
+    nan = __any_sync(FULL, nan);
+    if (nan) {
+        float r = 0.f;
+        if (scratch == nullptr) {
+            if (lane == 0) atomicOr(status, 8);
+            return __int_as_float(0x7fffffff);
+        }
+        for (int i = lane; i < n; i += 32) scratch[i] = v[i];
+        __syncwarp();
+        if (lane == 0) {
+            int oob = 0;
+            stl::sort(scratch, n, &oob);
+            if (oob) atomicOr(status, 4);
+            if (lq.kind == 1) r = scratch[0];
+            else if (lq.kind == 2) r = scratch[n - 1];
+            else r = interp(p, lq.prev_index, lq.step, scratch[lq.k - 1], scratch[lq.k]);
+        }
+        __syncwarp();
+        return __shfl_sync(FULL, r, 0);
+    }
+    if (lq.kind == 1 || lq.kind == 2) {
+        uint32_t m = lq.kind == 1 ? 0xffffffffu : 0u;
+        for (int i = lane; i < n; i += 32) {
+            const uint32_t u = ord_key(v[i]);
+            m = lq.kind == 1 ? min(m, u) : max(m, u);
+        }
+        m = lq.kind == 1 ? warp_min_u32(m) : warp_max_u32(m);
+        return key_float(m);
+    }
+    const uint32_t ka = warp_select(v, n, lq.k - 1, hist, lane);
+    int le = 0;
+    uint32_t nxt = 0xffffffffu;
+    for (int i = lane; i < n; i += 32) {
+        const uint32_t u = ord_key(v[i]);
+        le += u <= ka;
+        if (u > ka) nxt = min(nxt, u);
+    }
+    le = __reduce_add_sync(FULL, le);
+    nxt = warp_min_u32(nxt);
+    const uint32_t kb = le > lq.k ? ka : nxt;
+    return interp(p, lq.prev_index, lq.step, key_float(ka), key_float(kb));
+}
+
+
+}  // namespace
+}  // namespace sgr

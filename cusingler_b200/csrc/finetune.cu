@@ -1,0 +1,392 @@
+// Persistent fine-tune kernel (exact arithmetic) and the reference pre-sort it reads.
+//
+// Restates the reference's per-cell fine-tune loop (src/cusingler.cu:1138-1333 of
+// STOmics/cusingler: finetune_round + cufinetune) as one persistent kernel.  Each CTA takes the
+// next query cell from a device work queue and runs all of that cell's rounds on the device:
+//   1. gene set S = union over ordered candidate pairs of the first min(len, gene_thre(n)) genes of
+//      the pair's fine-tune list; fewer than 20 genes keeps the first candidate;
+//   2. the query's ranks over S (its thre-pool entries, sorted in shared memory);
+//   3. for every reference cell of every candidate label, the rank correlation over S;
+//   4. per label the quantile of those correlations, then the reference's keep/drop rule.
+//
+// Step 3 never builds a dense rank row.  With d = 2*rank - (|S|+1) and e = d + k (k = stored
+// entries of the row inside S), e is 0 at every implicit zero, so
+//     sum_g d_q d_r = sum_{g stored in both} e_q e_r - |S| k_q k_r.
+// Each reference row's thre-pool entries are sorted by value once (ref_presort_kernel), so for any
+// S one pass over the row, keeping the entries inside S, yields every kept entry's rank: runs of
+// equal values give (#less, #equal) directly.  The pass accumulates, per run of b kept entries with
+// a kept entries before it (z = 2a + b):  X = sum z * s, Y = s, Z1 = sum b z, Z2 = sum b z^2, where s
+// is the sum of the query's e over the run's genes, and then
+//     N   = X + (|S| - k_r) Y - |S| k_q k_r
+//     n_r = Z2 + 2 c Z1 + k_r c^2 + (|S| - k_r) k_r^2,   c = |S| - 2 k_r
+// exactly in int64.  The score is float((N * (1/sqrt(n_q))) * (1/sqrt(n_r))) in FP64, the same
+// formula as the score step's exact mode.
+
+#include <algorithm>
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "sgr_internal.h"
+#include "stl_order.h"
+#include "device_util.cuh"
+
+namespace sgr {
+
+namespace {
+
+constexpr int SENT = INT32_MIN;  // "gene not in S"
+
+// One warp per reference row: its thre-pool entries sorted by (value, gene), packed as
+// (value code << 16) | gene, where the code numbers the row's distinct values from 1 upward.
+__global__ void __launch_bounds__(256) ref_presort_kernel(const float* data, const int32_t* idx, const int32_t* ptr,
+                                                          uint32_t n_rows, int cap, uint32_t* out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    uint64_t* keys = reinterpret_cast<uint64_t*>(smem) + (size_t)warp * cap;
+    for (uint32_t row = blockIdx.x * wpb + warp; row < n_rows; row += gridDim.x * wpb) {
+        const int beg = ptr[row], k = ptr[row + 1] - beg;
+        if (k <= cap) {
+            int n = 1;
+            while (n < k) n <<= 1;
+            for (int i = lane; i < n; i += 32)
+                keys[i] = i < k ? ((uint64_t)ord_key(canon_zero(data[beg + i])) << 32) | (uint32_t)idx[beg + i]
+                                : ~0ull;
+            __syncwarp();
+            if (k > 1) warp_bitonic(keys, n, lane);
+            int carry = 0;
+            for (int base = 0; base < k; base += 32) {
+                const int j = base + lane;
+                bool nr = false;
+                if (j < k) nr = j == 0 || (uint32_t)(keys[j] >> 32) != (uint32_t)(keys[j - 1] >> 32);
+                const unsigned m = __ballot_sync(FULL, nr);
+                const int code = carry + __popc(m & (0xffffffffu >> (31 - lane)));
+                if (j < k) out[beg + j] = ((uint32_t)code << 16) | (uint32_t)(keys[j] & 0xffffu);
+                carry += __popc(m);
+            }
+            __syncwarp();
+        } else {
+            // rows longer than the sort buffer: positions and codes by counting
+            for (int i = lane; i < k; i += 32) {
+                const float v = canon_zero(data[beg + i]);
+                const int g = idx[beg + i];
+                int pos = 0, code = 1;
+                for (int j = 0; j < k; ++j) {
+                    const float w = canon_zero(data[beg + j]);
+                    const int h = idx[beg + j];
+                    pos += (w < v) || (w == v && h < g);
+                    if (w < v) {
+                        // count w once: only at its smallest gene id
+                        bool first = true;
+                        for (int t = 0; t < k && first; ++t)
+                            if (canon_zero(data[beg + t]) == w && idx[beg + t] < h) first = false;
+                        code += first;
+                    }
+                }
+                out[beg + pos] = ((uint32_t)code << 16) | (uint32_t)g;
+            }
+        }
+    }
+}
+
+struct FtShared {
+    int cell, ntop, nS, kq, rounds, done;
+    int64_t nq;
+    double rq;
+};
+
+__global__ void __launch_bounds__(256) ft_persistent_kernel(FtPersistentArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int Wt = a.Wt, L = a.L;
+    const int nwords = (Wt + 31) / 32;
+    int* eqv = reinterpret_cast<int*>(smem);                                     // Wt
+    uint32_t* bits = reinterpret_cast<uint32_t*>(eqv + ((Wt + 3) & ~3));         // nwords
+    uint64_t* qkeys = reinterpret_cast<uint64_t*>(bits + ((nwords + 3) & ~3));   // capq (8-byte aligned)
+    int* hist = reinterpret_cast<int*>(qkeys + a.capq);                          // 8 * 256
+    float* lsc = reinterpret_cast<float*>(hist + 8 * 256);                       // 256
+    int* off = reinterpret_cast<int*>(lsc + 256);                                // 257
+    int* red = off + 257;                                                        // 8 (+pad)
+    uint8_t* top = reinterpret_cast<uint8_t*>(red + 16);                         // 256
+    uint8_t* ntopv = top + 256;                                                  // 256
+    __shared__ FtShared sh;
+
+    float* scores = a.scratch + (size_t)blockIdx.x * a.scratch_per_cta;
+    float* nan_scratch = scores + a.max_rcand;
+
+    for (;;) {
+        if (tid == 0) sh.cell = atomicAdd(a.next_cell, 1);
+        __syncthreads();
+        const int cell = sh.cell;
+        if (cell >= a.Q) break;
+
+        // candidates: flagged labels in ascending order (src/cusingler.cu:1305-1312)
+        if (warp == 0) {
+            int n = 0;
+            for (int base = 0; base < L; base += 32) {
+                const int l = base + lane;
+                const bool f = l < L && a.flags[(size_t)cell * L + l] != 0;
+                const unsigned m = __ballot_sync(FULL, f);
+                if (f) top[n + __popc(m & ((1u << lane) - 1u))] = (uint8_t)l;
+                n += __popc(m);
+            }
+            if (lane == 0) {
+                sh.ntop = n;
+                sh.rounds = 0;
+                sh.done = 0;
+            }
+        }
+        __syncthreads();
+        int times_used = 0;
+        for (;;) {
+            const int ntop = sh.ntop;
+            if (!(ntop > 1 && (a.times == 0 || times_used++ < a.times))) break;
+            // 1) gene set S over the thre pool
+            for (int w = tid; w < nwords; w += blockDim.x) bits[w] = 0u;
+            __syncthreads();
+            const int gthre = a.gene_thre[ntop];
+            for (int pr = warp; pr < ntop * ntop; pr += 8) {
+                const int i = pr / ntop, j = pr % ntop;
+                if (i == j) continue;
+                const int li = top[i], lj = top[j];
+                const uint32_t pos = a.ft_idx[2 * ((size_t)li * L + lj)];
+                int len = (int)a.ft_idx[2 * ((size_t)li * L + lj) + 1];
+                if (len > gthre) len = gthre;
+                for (int e = lane; e < len; e += 32) {
+                    const uint32_t g = a.ft_genes[pos + e];
+                    atomicOr(&bits[g >> 5], 1u << (g & 31));
+                }
+            }
+            __syncthreads();
+            int cnt = 0;
+            for (int w = tid; w < nwords; w += blockDim.x) cnt += __popc(bits[w]);
+            cnt = __reduce_add_sync(FULL, cnt);
+            if (lane == 0) red[warp] = cnt;
+            __syncthreads();
+            if (tid == 0) {
+                int t = 0;
+                for (int w = 0; w < 8; ++w) t += red[w];
+                sh.nS = t;
+                sh.rounds++;
+            }
+            __syncthreads();
+            const int nS = sh.nS;
+            if (nS < 20) {  // keep the first candidate (src/cusingler.cu:1158-1159)
+                if (tid == 0) sh.ntop = 1;
+                __syncthreads();
+                continue;
+            }
+            // 2) query ranks over S: e = |S| - k + 2 #less + #equal at stored genes, 0 elsewhere in S
+            for (int g = tid; g < Wt; g += blockDim.x) eqv[g] = (bits[g >> 5] >> (g & 31)) & 1u ? 0 : SENT;
+            __syncthreads();
+            if (warp == 0) {
+                const int beg = a.qf_ptr[cell], end = a.qf_ptr[cell + 1];
+                int k = 0;
+                for (int base = beg; base < end; base += 32) {
+                    const int i = base + lane;
+                    bool hit = false;
+                    uint64_t key = 0;
+                    if (i < end) {
+                        const int g = a.qf_idx[i];
+                        if ((bits[g >> 5] >> (g & 31)) & 1u) {
+                            hit = true;
+                            key = ((uint64_t)ord_key(canon_zero(a.qf_data[i])) << 32) | (uint32_t)g;
+                        }
+                    }
+                    const unsigned m = __ballot_sync(FULL, hit);
+                    if (hit) {
+                        const int o = k + __popc(m & ((1u << lane) - 1u));
+                        if (o < a.capq) qkeys[o] = key;
+                    }
+                    k += __popc(m);
+                }
+                __syncwarp();
+                int64_t sq = 0;
+                if (k <= a.capq) {
+                    int n = 1;
+                    while (n < k) n <<= 1;
+                    for (int i = k + lane; i < n; i += 32) qkeys[i] = ~0ull;
+                    __syncwarp();
+                    if (k > 1) warp_bitonic(qkeys, n, lane);
+                    for (int j = lane; j < k; j += 32) {
+                        const uint64_t key = qkeys[j];
+                        const uint32_t hv = (uint32_t)(key >> 32);
+                        const int lo = lower_hi(qkeys, k, hv), hi = upper_hi(qkeys, k, hv);
+                        const int e = nS - k + 2 * lo + (hi - lo);
+                        eqv[(int)(uint32_t)key] = e;
+                        sq += (int64_t)(e - k) * (e - k);
+                    }
+                } else {
+                    for (int i = beg + lane; i < end; i += 32) {
+                        const int g = a.qf_idx[i];
+                        if (!((bits[g >> 5] >> (g & 31)) & 1u)) continue;
+                        const float v = canon_zero(a.qf_data[i]);
+                        int less = 0, eq = 0;
+                        for (int j = beg; j < end; ++j) {
+                            const int h = a.qf_idx[j];
+                            if (!((bits[h >> 5] >> (h & 31)) & 1u)) continue;
+                            const float w = canon_zero(a.qf_data[j]);
+                            less += w < v;
+                            eq += w == v;
+                        }
+                        const int e = nS - k + 2 * less + eq;
+                        eqv[g] = e;
+                        sq += (int64_t)(e - k) * (e - k);
+                    }
+                }
+                for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(FULL, sq, o);
+                if (lane == 0) {
+                    const int64_t nq = sq + (int64_t)(nS - k) * k * k;
+                    sh.kq = k;
+                    sh.nq = nq;
+                    sh.rq = nq > 0 ? 1.0 / sqrt((double)nq) : 0.0;
+                }
+            }
+            if (tid == 0) {
+                int o = 0;
+                for (int i = 0; i < ntop; ++i) {
+                    off[i] = o;
+                    o += (int)a.ctidx[2 * top[i] + 1];
+                }
+                off[ntop] = o;
+            }
+            __syncthreads();
+            // 3) correlation with every reference cell of every candidate label
+            const int total = off[ntop];
+            const int kq = sh.kq;
+            const int64_t nq = sh.nq;
+            const double rq = sh.rq;
+            for (int f = tid; f < total; f += blockDim.x) {
+                int lo = 0, hi = ntop - 1;  // label slot: off[lo] <= f < off[lo+1]
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (off[mid] <= f) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int r = (int)a.ctidx[2 * top[lo]] + (f - off[lo]);
+                const int beg = a.ref_ptr[r], end = a.ref_ptr[r + 1];
+                int64_t X = 0, Y = 0, Z1 = 0, Z2 = 0;
+                int ka = 0, b = 0, s = 0;
+                uint32_t cur = 0xffffffffu;
+                for (int j = beg; j < end; ++j) {
+                    const uint32_t ent = __ldg(a.ref_sorted + j);
+                    const int v = eqv[ent & 0xffffu];
+                    if (v == SENT) continue;
+                    const uint32_t code = ent >> 16;
+                    if (code != cur) {
+                        if (b) {
+                            const int64_t z = 2 * ka + b;
+                            X += z * s;
+                            Y += s;
+                            Z1 += b * z;
+                            Z2 += b * z * z;
+                            ka += b;
+                        }
+                        b = 0;
+                        s = 0;
+                        cur = code;
+                    }
+                    ++b;
+                    s += v;
+                }
+                if (b) {
+                    const int64_t z = 2 * ka + b;
+                    X += z * s;
+                    Y += s;
+                    Z1 += b * z;
+                    Z2 += b * z * z;
+                    ka += b;
+                }
+                const int64_t kr = ka;
+                const int64_t N = X + ((int64_t)nS - kr) * Y - (int64_t)nS * kq * kr;
+                const int64_t c = (int64_t)nS - 2 * kr;
+                const int64_t nr = Z2 + 2 * c * Z1 + kr * c * c + ((int64_t)nS - kr) * kr * kr;
+                float sc;
+                if (nq == 0 || nr == 0) sc = __int_as_float(0x7fffffff);
+                else sc = (float)(((double)N * rq) * (1.0 / sqrt((double)nr)));
+                scores[f] = sc;
+            }
+            __syncthreads();
+            // 4) per-label quantile, then keep / drop (src/cusingler.cu:1256-1295)
+            for (int i = warp; i < ntop; i += 8) {
+                LabelQ q = a.lq_label[top[i]];
+                const float v = quantile_warp(scores + off[i], q, a.p, hist + 256 * warp,
+                                                  nan_scratch + (size_t)warp * a.max_label, lane, a.status);
+                if (lane == 0) lsc[i] = v;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                int mn, mx;
+                stl::minmax(lsc, ntop, &mn, &mx);
+                const float lo = lsc[mn], hi = lsc[mx];
+                const float t = __fsub_rn(hi, a.thre);
+                int n = 0;
+                if (!(hi != hi)) {
+                    for (int i = 0; i < ntop; ++i) {
+                        const float s = lsc[i];
+                        if (s <= lo || s < t) continue;
+                        if (s == hi) {
+                            for (int j = n; j > 0; --j) ntopv[j] = ntopv[j - 1];
+                            ntopv[0] = top[i];
+                        } else {
+                            ntopv[n] = top[i];
+                        }
+                        ++n;
+                    }
+                }
+                if (n == 0) {
+                    ntopv[0] = top[0];
+                    n = 1;
+                }
+                for (int i = 0; i < n; ++i) top[i] = ntopv[i];
+                sh.ntop = n;
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            a.final_labels[cell] = sh.ntop > 0 ? (int32_t)top[0] : 0;
+            if (a.rounds) a.rounds[cell] = sh.rounds;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+size_t ft_persistent_smem(int Wt, int capq) {
+    const int nwords = (Wt + 31) / 32;
+    size_t b = 0;
+    b += sizeof(int) * ((Wt + 3) & ~3);
+    b += sizeof(uint32_t) * ((nwords + 3) & ~3);
+    b += sizeof(uint64_t) * capq;
+    b += sizeof(int) * 8 * 256 + sizeof(float) * 256 + sizeof(int) * (257 + 16) + 512;
+    return (b + 15) & ~size_t(15);
+}
+
+void launch_ref_presort(const float* data, const int32_t* idx, const int32_t* ptr, uint32_t n_rows, int cap,
+                        uint32_t* out, cudaStream_t s) {
+    if (!n_rows) return;
+    int wpb = std::max(1, std::min(8, (200 * 1024) / (cap * 8)));
+    const size_t smem = (size_t)wpb * cap * 8;
+    SGR_CUDA(cudaFuncSetAttribute(ref_presort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const unsigned blocks = std::min<unsigned>((n_rows + wpb - 1) / wpb, device_sm_count() * 8);
+    ref_presort_kernel<<<blocks, 32 * wpb, smem, s>>>(data, idx, ptr, n_rows, cap, out);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+int ft_persistent_grid(size_t smem) {
+    SGR_CUDA(cudaFuncSetAttribute(ft_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ft_persistent_kernel, 256, smem);
+    if (per_sm < 1) per_sm = 1;
+    return device_sm_count() * per_sm;
+}
+
+void launch_ft_persistent(const FtPersistentArgs& a, int grid, size_t smem, cudaStream_t s) {
+    SGR_CUDA(cudaFuncSetAttribute(ft_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ft_persistent_kernel<<<grid, 256, smem, s>>>(a);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+}  // namespace sgr

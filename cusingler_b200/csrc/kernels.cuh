@@ -127,4 +127,36 @@ void launch_ft_select(const FtGroup* groups, const FtSelItem* items, uint32_t n_
                       float p, const float* scores, float* label_scores, float* scratch,
                       int64_t scratch_per_warp, int* status, cudaStream_t s);
 
+// Persistent exact fine-tune (finetune.cu).
+struct FtPersistentArgs {
+    const uint32_t* ref_sorted;   // per reference row: thre-pool entries by value, (code << 16) | gene
+    const int32_t* ref_ptr;       // row offsets into ref_sorted
+    const uint32_t* ctidx;        // (start, len) per label
+    const uint32_t* ft_genes;     // fine-tune pair lists (thre ids)
+    const uint32_t* ft_idx;       // (start, len) per ordered label pair
+    const int32_t* gene_thre;     // marker count per candidate count n
+    const LabelQ* lq_label;       // quantile grid per label (start 0)
+    int L, Wt;
+    const float* qf_data;         // query compacted to the thre pool
+    const int32_t* qf_idx;
+    const int32_t* qf_ptr;
+    int Q;
+    const uint8_t* flags;         // Q x L first-round candidate flags
+    float p, thre;
+    int times;
+    int* next_cell;               // work-queue counter (zeroed before launch)
+    int32_t* final_labels;
+    int32_t* rounds;
+    float* scratch;               // per CTA: max_rcand scores + 8 * max_label sort space
+    int64_t scratch_per_cta;
+    int max_rcand, max_label, capq;
+    int* status;
+};
+
+size_t ft_persistent_smem(int Wt, int capq);
+int ft_persistent_grid(size_t smem);
+void launch_ft_persistent(const FtPersistentArgs& a, int grid, size_t smem, cudaStream_t s);
+void launch_ref_presort(const float* data, const int32_t* idx, const int32_t* ptr, uint32_t n_rows, int cap,
+                        uint32_t* out, cudaStream_t s);
+
 }  // namespace sgr
