@@ -277,6 +277,7 @@ void check_status(sgr_ctx* ctx) {
     if (st & 1) fail(SGR_ERR_INVALID_ARGUMENT, "a CSR column index is out of range");
     if (st & 2) fail(SGR_ERR_INVALID_ARGUMENT, "a CSR value is NaN");
     if (st & 8) fail(SGR_ERR_STATE, "NaN-bearing score list without sort scratch");
+    if (st & SGR_TC_TIMEOUT) fail(SGR_ERR_TIMEOUT, "a bounded wait of the tensor-core correlation ran out");
     // bit 4: libstdc++ would have read outside a NaN-bearing list; the result is the bounded one
 }
 
@@ -437,6 +438,28 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     ctx->trained = true;
 }
 
+// SGR_EXACT_SIMT=1 runs the exact correlation on CUDA cores (FP64) instead of the tensor cores, to
+// cross-check the two on a device (diagnostics).
+bool exact_simt() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("SGR_EXACT_SIMT");
+        on = (e && *e && *e != '0') ? 1 : 0;
+    }
+    return on == 1;
+}
+
+// Score-step correlation of nq query rows (LIMBS at A, norms at offset q0) with every reference row.
+void correlate(sgr_ctx* ctx, bool fp32, const int8_t* A, int nq, uint32_t q0, float* out, int64_t ld) {
+    if (fp32 || exact_simt())
+        launch_corr_simt(fp32, A, ctx->ref_limbs.p, nq, (int)ctx->R, ctx->G, ctx->Kp, ctx->q_f32.p + q0,
+                         ctx->ref_f32.p, ctx->q_rinv.p + q0, ctx->ref_rinv.p, ctx->q_n2.p + q0, ctx->ref_n2.p, out,
+                         ld, ctx->stream);
+    else
+        launch_corr_tc(A, ctx->ref_limbs.p, nq, (int)ctx->R, ctx->Kp, ctx->q_rinv.p + q0, ctx->ref_rinv.p,
+                       ctx->q_n2.p + q0, ctx->ref_n2.p, out, ld, ctx->status.p, ctx->stream);
+}
+
 // Score-step device pass over the first nq rows of `q` (already device resident).
 void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
     cudaStream_t s = ctx->stream;
@@ -477,9 +500,7 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
         const int nq = (int)std::min(chunk, Q - q0);
         const uint64_t c0 = launch_count();
         sp = ctx->prof.begin(ST_CORR, s);
-        launch_corr_simt(fp32, ctx->q_limbs.p + (size_t)q0 * 3 * ctx->Kp, ctx->ref_limbs.p, nq, (int)R, ctx->G,
-                         ctx->Kp, ctx->q_f32.p + q0, ctx->ref_f32.p, ctx->q_rinv.p + q0, ctx->ref_rinv.p,
-                         ctx->q_n2.p + q0, ctx->ref_n2.p, ctx->scores.p, R, s);
+        correlate(ctx, fp32, ctx->q_limbs.p + (size_t)q0 * 3 * ctx->Kp, nq, q0, ctx->scores.p, R);
         ctx->prof.end(sp, s);
         ctx->prof.acc.corr_launches += launch_count() - c0;
         sp = ctx->prof.begin(ST_SELECT, s);
@@ -785,7 +806,14 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
         lq[l] = make_lq(0, (int)mk.ctidx[2 * l + 1], p);
     }
     ctx->d_lq_label.upload(lq, s);
-    const int capq = std::min(pow2_at_least(std::max<int>(Wt, 32)), 8192);
+    // query sort buffer: the longest thre-pool row of this batch (rows beyond 8192 entries take the
+    // kernel's counting path)
+    std::vector<int32_t> qptr(Q + 1);
+    SGR_CUDA(cudaMemcpyAsync(qptr.data(), ctx->qf_indptr.p, (Q + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SGR_CUDA(cudaStreamSynchronize(s));
+    int qmax = 32;
+    for (uint32_t i = 0; i < Q; ++i) qmax = std::max(qmax, qptr[i + 1] - qptr[i]);
+    const int capq = std::min(pow2_at_least(qmax), 8192);
     const size_t smem = ft_persistent_smem((int)std::max<uint32_t>(Wt, 1), capq);
     if (smem > 220 * 1024) fail(SGR_ERR_UNSUPPORTED, "fine-tune gene pool too wide for shared memory");
     const int grid = ft_persistent_grid(smem);
@@ -1072,8 +1100,7 @@ sgr_status sgr_debug_scores(sgr_ctx* ctx, const sgr_csr* qry, float* out) {
         rank_rows(ctx, q, g, RANK_LIMBS, fp32 ? NORM_SEQ : NORM_NONE);
         DevBuf<float> sc;
         sc.ensure((size_t)Q * R);
-        launch_corr_simt(fp32, ctx->q_limbs.p, ctx->ref_limbs.p, (int)Q, (int)R, ctx->G, ctx->Kp, ctx->q_f32.p,
-                         ctx->ref_f32.p, ctx->q_rinv.p, ctx->ref_rinv.p, ctx->q_n2.p, ctx->ref_n2.p, sc.p, R, s);
+        correlate(ctx, fp32, ctx->q_limbs.p, (int)Q, 0, sc.p, R);
         SGR_CUDA(cudaMemcpyAsync(out, sc.p, (size_t)Q * R * sizeof(float), cudaMemcpyDeviceToHost, s));
         check_status(ctx);
     });

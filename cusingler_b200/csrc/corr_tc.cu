@@ -1,0 +1,366 @@
+// Score-step rank correlation on the 5th-generation tensor cores (tcgen05, kind::i8), exact.
+//
+// The reference computes every (query, reference) Spearman correlation with one FP32 fused
+// multiply-add chain per pair on CUDA cores (spearman, src/cusingler.cu:918-945 of
+// STOmics/cusingler).  Doubled centred ranks d = 2*rank - (G+1) are integers with |d| < G, so the
+// numerator N = sum_g d_q d_r is computed exactly here: d = 128 h + l (l in [-64, 63]) and the
+// Karatsuba limb s = h + l are int8, and
+//     P1 = H_q . H_r,  P2 = L_q . L_r,  P3 = S_q . S_r   (int32 accumulation in TMEM)
+//     N  = 128 (127 P1 + P3) - 127 P2                     (exact in FP64, |N| < 2^53)
+//     score = float((N * (1/sqrt(n_q))) * (1/sqrt(n_r)))   (FP64); a zero norm has a NaN
+//             reciprocal, so the score of a constant row is NaN as in the reference.
+//
+// Operands are the rank kernel's int8 rows [H | L | S] (3 * Kp bytes, Kp a multiple of 128), so one
+// TMA tensor map per operand covers all three limb planes and the K loop runs over 3 * Kp bytes; the
+// MMA warp sends each third of the K loop to its own accumulator (3 x 128 TMEM columns).
+//
+// Structure: persistent kernel, one CTA per SM, 256 threads:
+//   warp 0      TMA producer (128 x 128-byte boxes, 128B swizzle, STAGES-deep ring)
+//   warp 1      TMEM allocator and single-thread tcgen05.mma issuer (M = 128, N = 128, K = 32)
+//   warps 4..7  epilogue: tcgen05.ld 32x32b, exact recombination, shared-memory transpose,
+//               row-contiguous float stores
+// No TMA multicast is used.  Every mbarrier wait is bounded: on timeout the kernel records
+// SGR_TC_TIMEOUT in *status, drains its own TMA copies (bounded), frees TMEM and returns.
+
+#include <cuda.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "sgr_internal.h"
+
+namespace sgr {
+namespace {
+
+constexpr int BM = 128;
+constexpr int BN = 128;
+constexpr int BK = 128;  // bytes of K per stage (one 128-byte swizzle row)
+constexpr int STAGES = 6;
+constexpr int A_BYTES = BM * BK;
+constexpr int B_BYTES = BN * BK;
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int TMEM_COLS = 512;
+constexpr int EPI_STAGE_FLOATS = 32 * 33;  // per epilogue warp: 32 x 32 transpose buffer, padded
+constexpr long long WAIT_CYCLES = 4000000000LL;  // about 2 s at 1.9 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; false on timeout (or when another role already gave up).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+    const long long t0 = clock64();
+    for (uint32_t i = 0;; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if ((i & 63) == 63) {
+            if (*abort_flag) return false;
+            if (clock64() - t0 > WAIT_CYCLES) return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// K-major operand tile in shared memory with 128-byte swizzle: rows of 128 bytes, 8-row groups
+// 1024 bytes apart.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3fffu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// kind::i8 instruction descriptor: S32 accumulator, signed A and B, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_c, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_c),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+          "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+struct __align__(8) TcShared {
+    uint64_t full[STAGES];
+    uint64_t empty[STAGES];
+    uint64_t tmem_full;
+    uint64_t tmem_empty;
+    uint64_t drain;
+    uint32_t tmem_base;
+    int abort_flag;
+};
+
+__global__ void __launch_bounds__(256, 1)
+    corr_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nq, int R,
+                   int Kp, const double* __restrict__ rq, const double* __restrict__ rr,
+                   const int64_t* __restrict__ nq2, const int64_t* __restrict__ nr2, float* __restrict__ out,
+                   int64_t ld, int* status) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ TcShared sh;
+    // stage buffers must start on a 1024-byte boundary (128B swizzle atoms)
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tiles_n = (R + BN - 1) / BN, tiles_m = (nq + BM - 1) / BM;
+    const int n_tiles = tiles_m * tiles_n;
+    const int kblocks = 3 * Kp / BK, seg_blocks = Kp / BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(smem_u32(&sh.full[s]), 1);
+            mbar_init(smem_u32(&sh.empty[s]), 1);
+        }
+        mbar_init(smem_u32(&sh.tmem_full), 1);
+        mbar_init(smem_u32(&sh.tmem_empty), 4);
+        mbar_init(smem_u32(&sh.drain), 1);
+        sh.abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh.tmem_base)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sh.tmem_base;
+    volatile int* abort_flag = &sh.abort_flag;
+
+    if (warp == 0) {
+        // ---- TMA producer ------------------------------------------------------------------
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+                const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+                for (int kb = 0; kb < kblocks; ++kb, ++it) {
+                    const int s = it % STAGES;
+                    const uint32_t ph = (it / STAGES) & 1;
+                    if (!mbar_wait(smem_u32(&sh.empty[s]), ph ^ 1, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t a_dst = smem_u32(smem + s * STAGE_BYTES);
+                    const uint32_t b_dst = a_dst + A_BYTES;
+                    const uint32_t fb = smem_u32(&sh.full[s]);
+                    mbar_expect_tx(fb, STAGE_BYTES);
+                    tma_load_2d(a_dst, &tmA, kb * BK, m0, fb);
+                    tma_load_2d(b_dst, &tmB, kb * BK, n0, fb);
+                }
+            }
+            if (!ok) {
+                atomicOr(status, SGR_TC_TIMEOUT);
+                sh.abort_flag = 1;
+            }
+            // drain: every issued stage's copies land before the CTA can exit
+            for (uint32_t j = (it > STAGES ? it - STAGES : 0); j < it; ++j) {
+                const uint32_t s = j % STAGES, ph = (j / STAGES) & 1;
+                const long long t0 = clock64();
+                while (!mbar_try(smem_u32(&sh.full[s]), ph) && clock64() - t0 < WAIT_CYCLES) {
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer ----------------------------------------------------------------------
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_i8(BM, BN);
+            uint32_t it = 0, tile_iter = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++tile_iter) {
+                if (!mbar_wait(smem_u32(&sh.tmem_empty), (tile_iter & 1) ^ 1, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                for (int kb = 0; kb < kblocks; ++kb, ++it) {
+                    const int s = it % STAGES;
+                    const uint32_t ph = (it / STAGES) & 1;
+                    if (!mbar_wait(smem_u32(&sh.full[s]), ph, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const int seg = kb / seg_blocks;
+                    const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
+                    const uint64_t da = smem_desc(a_addr), db = smem_desc(a_addr + A_BYTES);
+                    const uint32_t tc = tmem + seg * BN;
+                    const bool first = (kb % seg_blocks) == 0;
+#pragma unroll
+                    for (int k = 0; k < BK / 32; ++k)
+                        umma_i8(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (first && k == 0) ? 0u : 1u);
+                    umma_commit(smem_u32(&sh.empty[s]));
+                }
+                if (!ok) break;
+                umma_commit(smem_u32(&sh.tmem_full));
+            }
+            if (!ok) {
+                atomicOr(status, SGR_TC_TIMEOUT);
+                sh.abort_flag = 1;
+            }
+            // every MMA this thread issued has finished before TMEM is freed
+            umma_commit(smem_u32(&sh.drain));
+            const long long t0 = clock64();
+            while (!mbar_try(smem_u32(&sh.drain), 0) && clock64() - t0 < WAIT_CYCLES) {
+            }
+        }
+    } else if (warp >= 4) {
+        // ---- epilogue ------------------------------------------------------------------------
+        // Each lane owns one query row; a 32 x 32 chunk is transposed through shared memory so that
+        // every store instruction writes one row's 32 consecutive scores (one 128-byte line).
+        const int quarter = warp & 3;
+        float* stage = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES) + quarter * EPI_STAGE_FLOATS;
+        uint32_t tile_iter = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++tile_iter) {
+            const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+            const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh.tmem_full), tile_iter & 1, abort_flag));
+            if (!got) {
+                if (lane == 0) {
+                    atomicOr(status, SGR_TC_TIMEOUT);
+                    sh.abort_flag = 1;
+                }
+                break;
+            }
+            tc_fence_after();
+            const int row0 = m0 + 32 * quarter;
+            const int q = row0 + lane;
+            const double rqv = q < nq ? rq[q] : 0.0;  // NaN when the query row is constant
+            const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
+            for (int c = 0; c < BN / 32; ++c) {
+                uint32_t p1[32], p2[32], p3[32];
+                tmem_ld32(lane_base + c * 32, p1);
+                tmem_ld32(lane_base + BN + c * 32, p2);
+                tmem_ld32(lane_base + 2 * BN + c * 32, p3);
+                tmem_wait_ld();
+                if (c == BN / 32 - 1) {
+                    // all of this warp's TMEM reads are done: release the accumulator
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(smem_u32(&sh.tmem_empty));
+                }
+                const int r0 = n0 + c * 32;
+                const double rrl = r0 + lane < R ? rr[r0 + lane] : 0.0;  // NaN for a constant reference row
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int T = 127 * (int)p1[j] + (int)p3[j];
+                    const double N = (double)T * 128.0 - (double)(int)p2[j] * 127.0;
+                    const double rrj = __shfl_sync(0xffffffffu, rrl, j);
+                    stage[lane * 33 + j] = (float)((N * rqv) * rrj);
+                }
+                __syncwarp();
+                if (r0 + lane < R) {
+                    const int rows = min(32, nq - row0);
+                    float* dst = out + (size_t)row0 * ld + r0 + lane;
+                    for (int i = 0; i < rows; ++i) dst[(size_t)i * ld] = stage[i * 33 + lane];
+                }
+                __syncwarp();
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        SGR_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (!p || q != cudaDriverEntryPointSuccess) fail(SGR_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<EncodeTiled>(p);
+    }
+    return fn;
+}
+
+// Tensor map of a [rows x (3 * Kp)] int8 limb matrix, 128 x 128-byte boxes, 128B swizzle.
+CUtensorMap limb_map(const int8_t* base, int rows, int Kp) {
+    CUtensorMap m;
+    cuuint64_t dims[2] = {(cuuint64_t)(3 * Kp), (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(3 * Kp)};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(base), dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(SGR_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
+
+}  // namespace
+
+size_t corr_tc_smem() { return (size_t)STAGES * STAGE_BYTES + 4 * EPI_STAGE_FLOATS * sizeof(float) + 1024; }
+
+void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
+                    const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s) {
+    if (nq <= 0 || R <= 0) return;
+    if (Kp % BK != 0 || (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15))
+        fail(SGR_ERR_INVALID_ARGUMENT, "tensor-core correlation: misaligned operands");
+    const CUtensorMap ta = limb_map(A, nq, Kp), tb = limb_map(B, R, Kp);
+    const size_t smem = corr_tc_smem();
+    SGR_CUDA(cudaFuncSetAttribute(corr_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long tiles = (long)((nq + BM - 1) / BM) * ((R + BN - 1) / BN);
+    const int grid = (int)std::min<long>(tiles, device_sm_count());
+    corr_tc_kernel<<<grid, 256, smem, s>>>(ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+}  // namespace sgr

@@ -12,14 +12,15 @@
 // Step 3 never builds a dense rank row.  With d = 2*rank - (|S|+1) and e = d + k (k = stored
 // entries of the row inside S), e is 0 at every implicit zero, so
 //     sum_g d_q d_r = sum_{g stored in both} e_q e_r - |S| k_q k_r.
-// Each reference row's thre-pool entries are sorted by value once (ref_presort_kernel), so for any
-// S one pass over the row, keeping the entries inside S, yields every kept entry's rank: runs of
-// equal values give (#less, #equal) directly.  The pass accumulates, per run of b kept entries with
-// a kept entries before it (z = 2a + b):  X = sum z * s, Y = s, Z1 = sum b z, Z2 = sum b z^2, where s
-// is the sum of the query's e over the run's genes, and then
+// Each reference row's thre-pool entries are sorted by value once (ref_presort_kernel), each with
+// the position where its run of equal values starts.  For any S, one pass over the row keeping the
+// entries inside S yields every kept entry's rank: a run of b kept entries with a kept entries
+// before it gives each of them 2 #less + #equal = z = 2a + b.  The pass accumulates
+// X = sum z s, Y = sum s (s = the query's e summed over the run's genes), Z1 = sum b z,
+// Z2 = sum b z^2, and then, exactly in int64,
 //     N   = X + (|S| - k_r) Y - |S| k_q k_r
-//     n_r = Z2 + 2 c Z1 + k_r c^2 + (|S| - k_r) k_r^2,   c = |S| - 2 k_r
-// exactly in int64.  The score is float((N * (1/sqrt(n_q))) * (1/sqrt(n_r))) in FP64, the same
+//     n_r = Z2 + 2 c Z1 + k_r c^2 + (|S| - k_r) k_r^2,   c = |S| - 2 k_r.
+// The score is float((N * (1/sqrt(n_q))) * (1/sqrt(n_r))) in FP64, the same
 // formula as the score step's exact mode.
 
 #include <algorithm>
@@ -36,8 +37,9 @@ namespace {
 
 constexpr int SENT = INT32_MIN;  // "gene not in S"
 
-// One warp per reference row: its thre-pool entries sorted by (value, gene), packed as
-// (value code << 16) | gene, where the code numbers the row's distinct values from 1 upward.
+// One warp per reference row: its thre-pool entries sorted by (value, gene), each packed as
+// gene | run_start << 16, where run_start is the row position of the first entry with the same
+// value.
 __global__ void __launch_bounds__(256) ref_presort_kernel(const float* data, const int32_t* idx, const int32_t* ptr,
                                                           uint32_t n_rows, int cap, uint32_t* out) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -53,36 +55,25 @@ __global__ void __launch_bounds__(256) ref_presort_kernel(const float* data, con
                                 : ~0ull;
             __syncwarp();
             if (k > 1) warp_bitonic(keys, n, lane);
-            int carry = 0;
-            for (int base = 0; base < k; base += 32) {
-                const int j = base + lane;
-                bool nr = false;
-                if (j < k) nr = j == 0 || (uint32_t)(keys[j] >> 32) != (uint32_t)(keys[j - 1] >> 32);
-                const unsigned m = __ballot_sync(FULL, nr);
-                const int code = carry + __popc(m & (0xffffffffu >> (31 - lane)));
-                if (j < k) out[beg + j] = ((uint32_t)code << 16) | (uint32_t)(keys[j] & 0xffffu);
-                carry += __popc(m);
+            for (int j = lane; j < k; j += 32) {
+                const uint32_t hv = (uint32_t)(keys[j] >> 32);
+                const uint32_t rs = (uint32_t)lower_hi(keys, k, hv);
+                out[beg + j] = (uint32_t)(keys[j] & 0xffffu) | (rs << 16);
             }
             __syncwarp();
         } else {
-            // rows longer than the sort buffer: positions and codes by counting
+            // rows longer than the sort buffer: position and run bounds by counting
             for (int i = lane; i < k; i += 32) {
                 const float v = canon_zero(data[beg + i]);
                 const int g = idx[beg + i];
-                int pos = 0, code = 1;
+                int pos = 0, rs = 0;
                 for (int j = 0; j < k; ++j) {
                     const float w = canon_zero(data[beg + j]);
                     const int h = idx[beg + j];
                     pos += (w < v) || (w == v && h < g);
-                    if (w < v) {
-                        // count w once: only at its smallest gene id
-                        bool first = true;
-                        for (int t = 0; t < k && first; ++t)
-                            if (canon_zero(data[beg + t]) == w && idx[beg + t] < h) first = false;
-                        code += first;
-                    }
+                    rs += w < v;
                 }
-                out[beg + pos] = ((uint32_t)code << 16) | (uint32_t)g;
+                out[beg + pos] = (uint32_t)g | ((uint32_t)rs << 16);
             }
         }
     }
@@ -255,6 +246,8 @@ __global__ void __launch_bounds__(256) ft_persistent_kernel(FtPersistentArgs a) 
             const int kq = sh.kq;
             const int64_t nq = sh.nq;
             const double rq = sh.rq;
+            // one lane per reference row: a single pass over the row's entries in value order,
+            // keeping the genes in S (see the comment at the top of this file)
             for (int f = tid; f < total; f += blockDim.x) {
                 int lo = 0, hi = ntop - 1;  // label slot: off[lo] <= f < off[lo+1]
                 while (lo < hi) {
@@ -265,33 +258,33 @@ __global__ void __launch_bounds__(256) ft_persistent_kernel(FtPersistentArgs a) 
                 const int r = (int)a.ctidx[2 * top[lo]] + (f - off[lo]);
                 const int beg = a.ref_ptr[r], end = a.ref_ptr[r + 1];
                 int64_t X = 0, Y = 0, Z1 = 0, Z2 = 0;
-                int ka = 0, b = 0, s = 0;
+                int ka = 0, b = 0, sum = 0;
                 uint32_t cur = 0xffffffffu;
                 for (int j = beg; j < end; ++j) {
                     const uint32_t ent = __ldg(a.ref_sorted + j);
                     const int v = eqv[ent & 0xffffu];
                     if (v == SENT) continue;
-                    const uint32_t code = ent >> 16;
-                    if (code != cur) {
+                    const uint32_t run = ent >> 16;
+                    if (run != cur) {
                         if (b) {
                             const int64_t z = 2 * ka + b;
-                            X += z * s;
-                            Y += s;
+                            X += z * sum;
+                            Y += sum;
                             Z1 += b * z;
                             Z2 += b * z * z;
                             ka += b;
                         }
                         b = 0;
-                        s = 0;
-                        cur = code;
+                        sum = 0;
+                        cur = run;
                     }
                     ++b;
-                    s += v;
+                    sum += v;
                 }
                 if (b) {
                     const int64_t z = 2 * ka + b;
-                    X += z * s;
-                    Y += s;
+                    X += z * sum;
+                    Y += sum;
                     Z1 += b * z;
                     Z2 += b * z * z;
                     ka += b;

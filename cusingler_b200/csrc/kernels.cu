@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
         const int64_t n2 = sq + (int64_t)(G - k) * k * k;
         if (lane == 0) {
             g.n2[it.slot] = n2;
-            g.rinv[it.slot] = n2 > 0 ? 1.0 / sqrt((double)n2) : 0.0;
+            g.rinv[it.slot] = n2 > 0 ? 1.0 / sqrt((double)n2) : __longlong_as_double(0x7ff8000000000000ll);
         }
 
         // 4) FP32 self-norm in the reference's order (fp32ref mode only)

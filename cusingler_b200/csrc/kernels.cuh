@@ -9,6 +9,11 @@ namespace sgr {
 
 int device_sm_count();
 
+// Device status bits (ctx->status): 1 CSR column out of range, 2 NaN value, 4 NaN-bearing list where
+// libstdc++ would have read out of bounds, 8 missing sort scratch, SGR_TC_TIMEOUT a bounded wait of
+// the tensor-core kernel ran out.
+constexpr int SGR_TC_TIMEOUT = 16;
+
 // Kernels launched by this process's library (read before and after a call to count its launches).
 uint64_t launch_count();
 void count_launch(uint64_t n = 1);
@@ -27,7 +32,7 @@ struct RankGroup {
     int32_t Kp;
     void* out;              // LIMBS: int8 [rows][3*Kp] planes H|L|S; D16: int16 [rows][Kp]
     int64_t* n2;            // per row: sum of d^2 (exact)
-    double* rinv;           // per row: 1/sqrt(n2), 0 when n2 == 0
+    double* rinv;           // per row: 1/sqrt(n2), NaN when n2 == 0
     float* f32norm;         // per row, fp32 reference-order sum of x^2 (x = d/2), or nullptr
 };
 
@@ -127,9 +132,14 @@ void launch_ft_select(const FtGroup* groups, const FtSelItem* items, uint32_t n_
                       float p, const float* scores, float* label_scores, float* scratch,
                       int64_t scratch_per_warp, int* status, cudaStream_t s);
 
+// Exact score-step correlation on the tensor cores (corr_tc.cu): A/B are LIMBS rows of 3 * Kp bytes.
+size_t corr_tc_smem();
+void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
+                    const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s);
+
 // Persistent exact fine-tune (finetune.cu).
 struct FtPersistentArgs {
-    const uint32_t* ref_sorted;   // per reference row: thre-pool entries by value, (code << 16) | gene
+    const uint32_t* ref_sorted;   // per reference row: thre-pool entries by value, gene | run start << 16
     const int32_t* ref_ptr;       // row offsets into ref_sorted
     const uint32_t* ctidx;        // (start, len) per label
     const uint32_t* ft_genes;     // fine-tune pair lists (thre ids)
