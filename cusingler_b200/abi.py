@@ -27,7 +27,7 @@ SYMBOLS = [
     "sgr_create", "sgr_destroy", "sgr_last_error", "sgr_set_mode", "sgr_train_ref", "sgr_score_first",
     "sgr_finetune", "sgr_annotate", "sgr_get_info", "sgr_get_u32", "sgr_debug_ranks", "sgr_debug_scores",
     "sgr_debug_stl_sort", "sgr_debug_stl_minmax", "sgr_set_stream", "sgr_set_profiling", "sgr_reset_timings",
-    "sgr_get_timings",
+    "sgr_get_timings", "sgr_select_labels_noalloc",
 ]
 
 
@@ -90,6 +90,7 @@ def lib():
             "sgr_set_profiling": (C.c_int, [vp, C.c_int]),
             "sgr_reset_timings": (C.c_int, [vp]),
             "sgr_get_timings": (C.c_int, [vp, C.POINTER(SgrTimings)]),
+            "sgr_select_labels_noalloc": (C.c_int, [vp, C.c_int64, u32, vp, u32, f32, f32, vp, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -245,6 +246,18 @@ class Annotator:
         out = np.zeros((csr.n_rows, inf.ref_rows), np.float32)
         self._check(self.L.sgr_debug_scores(self.h, C.byref(csr), out.ctypes.data))
         return out
+
+
+def select_labels_noalloc(d_scores, ld, n_rows, label_ranges, quantile, thre, d_label_scores, d_first, d_flags,
+                          stream=None):
+    """Allocation-free label selection on device buffers the caller owns (raw device pointers).
+
+    For callers that cannot allocate device memory (a framework that owns the GPU's memory, a
+    CUDA graph being recorded): the library uses a fixed 4 MiB device array of its own instead.
+    Returns the status code (0 = OK)."""
+    r = np.ascontiguousarray(label_ranges, np.uint32)
+    return lib().sgr_select_labels_noalloc(d_scores, ld, n_rows, r.ctypes.data, len(r) // 2, quantile, thre,
+                                           d_label_scores, d_first, d_flags, stream)
 
 
 def stl_sort(v):

@@ -128,6 +128,34 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
 sgr_status sgr_reset_timings(sgr_ctx* ctx);
 sgr_status sgr_get_timings(const sgr_ctx* ctx, sgr_timings* out);
 
+/* ---- Allocation-free selection -------------------------------------------------------------- */
+
+/* This entry point has no counterpart in the reference.  It is for callers that cannot allocate
+ * device memory: code running while another runtime owns the GPU's memory through its own pool and
+ * budget, code being recorded into a CUDA graph, or latency-bound code where a cudaMalloc/cudaFree
+ * would synchronise the device.  It does the score-step label selection of sgr_score_first (per
+ * label the `quantile` of a query row's scores over that label's reference columns, the first
+ * label, the candidate flags) on score rows the caller already holds on the device, and calls no
+ * cudaMalloc, cudaFree or allocating library routine.
+ *
+ *   d_scores        n_rows x ld floats on the current device (row q: query q's correlations)
+ *   label_ranges    host array, (start, len) of each label's columns, 2 * n_labels entries
+ *   d_label_scores  n_rows x n_labels floats (device); d_first_labels n_rows (device);
+ *   d_flags         n_rows x n_labels bytes (device) or NULL
+ *   stream          cudaStream_t of the current device (NULL: the default stream)
+ *
+ * The call only enqueues work on `stream`; results are ready when the stream reaches that point.
+ * Its temporary space is one fixed device array of 1,048,576 floats (4 MiB) inside the library,
+ * which every GPU that loads the library holds until the process exits; each label may therefore
+ * hold at most 131,072 reference columns (SGR_ERR_UNSUPPORTED beyond).  All calls share that
+ * array, so calls that overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller.  The first call on a device looks the array's address up; make that
+ * first call before any stream capture. */
+sgr_status sgr_select_labels_noalloc(const float* d_scores, int64_t ld, uint32_t n_rows,
+                                     const uint32_t* label_ranges, uint32_t n_labels, float quantile,
+                                     float finetune_thre, float* d_label_scores,
+                                     int32_t* d_first_labels, uint8_t* d_flags, void* stream);
+
 /* ---- Introspection (tests and tools) ------------------------------------------------------- */
 
 typedef struct sgr_info {
