@@ -425,7 +425,7 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     int32_t reff_nnz = 0;
     SGR_CUDA(cudaMemcpyAsync(&reff_nnz, ctx->reff_indptr.p + ctx->R, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     SGR_CUDA(cudaStreamSynchronize(s));
-    ctx->ref_sorted.ensure(std::max<int32_t>(reff_nnz, 1));
+    ctx->ref_sorted.ensure((size_t)std::max<int32_t>(reff_nnz, 1) + 4);  // + one 16-byte vector of slack
     launch_ref_presort(ctx->reff_data.p, ctx->reff_indices.p, ctx->reff_indptr.p, ctx->R,
                        std::min(pow2_at_least(std::max<int>(ctx->Wt, 32)), 8192), ctx->ref_sorted.p, s);
     ctx->d_ctidx.upload(mk.ctidx, s);

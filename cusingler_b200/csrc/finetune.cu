@@ -260,26 +260,35 @@ __global__ void __launch_bounds__(256) ft_persistent_kernel(FtPersistentArgs a) 
                 int64_t X = 0, Y = 0, Z1 = 0, Z2 = 0;
                 int ka = 0, b = 0, sum = 0;
                 uint32_t cur = 0xffffffffu;
-                for (int j = beg; j < end; ++j) {
-                    const uint32_t ent = __ldg(a.ref_sorted + j);
-                    const int v = eqv[ent & 0xffffu];
-                    if (v == SENT) continue;
-                    const uint32_t run = ent >> 16;
-                    if (run != cur) {
-                        if (b) {
-                            const int64_t z = 2 * ka + b;
-                            X += z * sum;
-                            Y += sum;
-                            Z1 += b * z;
-                            Z2 += b * z * z;
-                            ka += b;
+                // 16-byte loads of four entries (the list base is 16-byte aligned; the first and
+                // last words are masked to [beg, end))
+                for (int j4 = beg & ~3; j4 < end; j4 += 4) {
+                    const uint4 w4 = __ldg(reinterpret_cast<const uint4*>(a.ref_sorted + j4));
+                    const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int j = j4 + u;
+                        if (j < beg || j >= end) continue;
+                        const uint32_t ent = ws[u];
+                        const int v = eqv[ent & 0xffffu];
+                        if (v == SENT) continue;
+                        const uint32_t run = ent >> 16;
+                        if (run != cur) {
+                            if (b) {
+                                const int64_t z = 2 * ka + b;
+                                X += z * sum;
+                                Y += sum;
+                                Z1 += b * z;
+                                Z2 += b * z * z;
+                                ka += b;
+                            }
+                            b = 0;
+                            sum = 0;
+                            cur = run;
                         }
-                        b = 0;
-                        sum = 0;
-                        cur = run;
+                        ++b;
+                        sum += v;
                     }
-                    ++b;
-                    sum += v;
                 }
                 if (b) {
                     const int64_t z = 2 * ka + b;
