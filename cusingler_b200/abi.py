@@ -27,7 +27,8 @@ SYMBOLS = [
     "sgr_create", "sgr_destroy", "sgr_last_error", "sgr_set_mode", "sgr_train_ref", "sgr_score_first",
     "sgr_finetune", "sgr_annotate", "sgr_get_info", "sgr_get_u32", "sgr_debug_ranks", "sgr_debug_scores",
     "sgr_debug_stl_sort", "sgr_debug_stl_minmax", "sgr_set_stream", "sgr_set_profiling", "sgr_reset_timings",
-    "sgr_get_timings", "sgr_select_labels_noalloc",
+    "sgr_get_timings", "sgr_select_labels_noalloc", "sgr_mlp_train", "sgr_mlp_predict", "sgr_mlp_params",
+    "sgr_mlp_load", "sgr_mlp_debug_grads", "sgr_annotate_learned", "sgr_set_tuning",
 ]
 
 
@@ -47,7 +48,22 @@ class SgrTimings(C.Structure):
                 ("select_ms", C.c_double), ("finetune_ms", C.c_double), ("total_ms", C.c_double),
                 ("launches", C.c_uint64), ("corr_launches", C.c_uint64), ("rank_launches", C.c_uint64),
                 ("rank_bytes", C.c_uint64), ("corr_ops", C.c_uint64), ("cells", C.c_uint64),
-                ("ft_cell_rounds", C.c_uint64)]
+                ("ft_cell_rounds", C.c_uint64), ("mlp_ms", C.c_double), ("select_launches", C.c_uint64),
+                ("select_bytes", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class SgrMlpConfig(C.Structure):
+    _fields_ = [("hidden", C.c_uint32), ("epochs", C.c_uint32), ("batch", C.c_uint32), ("lr", C.c_float),
+                ("weight_decay", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("seed", C.c_uint64)]
+
+
+class SgrLearnedStats(C.Structure):
+    _fields_ = [("cells", C.c_uint64), ("decided", C.c_uint64), ("finetuned", C.c_uint64),
+                ("checked", C.c_uint64), ("check_agree", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -88,9 +104,17 @@ def lib():
             "sgr_debug_stl_minmax": (None, [vp, i32, C.POINTER(i32), C.POINTER(i32)]),
             "sgr_set_stream": (C.c_int, [vp, vp]),
             "sgr_set_profiling": (C.c_int, [vp, C.c_int]),
+            "sgr_set_tuning": (C.c_int, [vp, C.c_int, C.c_int]),
             "sgr_reset_timings": (C.c_int, [vp]),
             "sgr_get_timings": (C.c_int, [vp, C.POINTER(SgrTimings)]),
             "sgr_select_labels_noalloc": (C.c_int, [vp, C.c_int64, u32, vp, u32, f32, f32, vp, vp, vp, vp]),
+            "sgr_mlp_train": (C.c_int, [vp, vp, vp, u32, C.POINTER(SgrMlpConfig), C.POINTER(f32)]),
+            "sgr_mlp_predict": (C.c_int, [vp, vp, u32, vp, vp]),
+            "sgr_mlp_params": (C.c_int, [vp, vp, C.c_uint64, C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_uint64)]),
+            "sgr_mlp_load": (C.c_int, [vp, vp, u32, u32]),
+            "sgr_mlp_debug_grads": (C.c_int, [vp, vp, vp, u32, vp, C.POINTER(f32)]),
+            "sgr_annotate_learned": (C.c_int, [vp, C.POINTER(SgrCsr), f32, f32, C.c_int32, f32, f32, vp, vp,
+                                               C.POINTER(SgrLearnedStats)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -196,9 +220,61 @@ class Annotator:
                                         final.ctypes.data, _ptr(scores)))
         return (first, final, scores) if with_scores else (first, final)
 
+    # ---- learned proposal ----------------------------------------------------------------------
+    def mlp_train(self, label_scores, targets, epochs=20, batch=4096, lr=1e-3, weight_decay=0.01, hidden=256,
+                  seed=0):
+        x = np.ascontiguousarray(label_scores, np.float32)
+        y = np.ascontiguousarray(targets, np.int32)
+        cfg = SgrMlpConfig(hidden, epochs, batch, lr, weight_decay, 0.9, 0.999, 1e-8, seed)
+        loss = C.c_float()
+        self._check(self.L.sgr_mlp_train(self.h, x.ctypes.data, y.ctypes.data, len(y), C.byref(cfg), C.byref(loss)))
+        return loss.value
+
+    def mlp_predict(self, label_scores):
+        x = np.ascontiguousarray(label_scores, np.float32)
+        n = x.shape[0]
+        lab = np.zeros(n, np.int32)
+        conf = np.zeros(n, np.float32)
+        self._check(self.L.sgr_mlp_predict(self.h, x.ctypes.data, n, lab.ctypes.data, conf.ctypes.data))
+        return lab, conf
+
+    def mlp_params(self):
+        L, H, n = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        self._check(self.L.sgr_mlp_params(self.h, None, 0, C.byref(L), C.byref(H), C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        self._check(self.L.sgr_mlp_params(self.h, out.ctypes.data, out.size, None, None, None))
+        return out, L.value, H.value
+
+    def mlp_load(self, params, n_labels, hidden):
+        p = np.ascontiguousarray(params, np.float32)
+        self._check(self.L.sgr_mlp_load(self.h, p.ctypes.data, n_labels, hidden))
+
+    def mlp_debug_grads(self, features, targets):
+        x = np.ascontiguousarray(features, np.float32)
+        y = np.ascontiguousarray(targets, np.int32)
+        params, L, H = self.mlp_params()
+        g = np.zeros_like(params)
+        loss = C.c_float()
+        self._check(self.L.sgr_mlp_debug_grads(self.h, x.ctypes.data, y.ctypes.data, len(y), g.ctypes.data,
+                                               C.byref(loss)))
+        return g, loss.value
+
+    def annotate_learned(self, qry, quantile=0.8, thre=0.05, times=0, min_confidence=0.98, check_fraction=0.01):
+        csr, keep = self._csr(qry)
+        Q = csr.n_rows
+        first = np.zeros(Q, np.int32)
+        final = np.zeros(Q, np.int32)
+        st = SgrLearnedStats()
+        self._check(self.L.sgr_annotate_learned(self.h, C.byref(csr), quantile, thre, times, min_confidence,
+                                                check_fraction, first.ctypes.data, final.ctypes.data, C.byref(st)))
+        return first, final, st.as_dict()
+
     def set_stream(self, stream_ptr):
         """Run on a caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream); None = own."""
         self._check(self.L.sgr_set_stream(self.h, stream_ptr))
+
+    def set_tuning(self, what: int, value: int):
+        self._check(self.L.sgr_set_tuning(self.h, what, value))
 
     def set_profiling(self, on: bool = True):
         self._check(self.L.sgr_set_profiling(self.h, 1 if on else 0))

@@ -12,11 +12,13 @@
 #include <cstdlib>
 #include <cmath>
 #include <map>
+#include <random>
 #include <set>
 #include <string>
 #include <vector>
 
 #include "kernels.cuh"
+#include "mlp.h"
 #include "sgr_internal.h"
 #include "stl_order.h"
 
@@ -24,7 +26,7 @@ using namespace sgr;
 
 namespace {
 
-enum Stage { ST_H2D = 0, ST_RANK, ST_CORR, ST_SELECT, ST_FT, ST_COUNT };
+enum Stage { ST_H2D = 0, ST_RANK, ST_CORR, ST_SELECT, ST_FT, ST_MLP, ST_COUNT };
 
 // CUDA-event spans on the context's stream; resolved after the call's final synchronisation.
 struct Profiler {
@@ -63,7 +65,8 @@ struct Profiler {
             used = 0;
             return;
         }
-        double* slot[ST_COUNT] = {&acc.h2d_ms, &acc.rank_ms, &acc.corr_ms, &acc.select_ms, &acc.finetune_ms};
+        double* slot[ST_COUNT] = {&acc.h2d_ms, &acc.rank_ms, &acc.corr_ms, &acc.select_ms, &acc.finetune_ms,
+                                  &acc.mlp_ms};
         float first_last = 0.f;
         for (auto& sp : spans) {
             float ms = 0.f;
@@ -115,8 +118,29 @@ struct sgr_ctx {
     DevBuf<int32_t> d_gene_thre;
     DevBuf<LabelQ> d_lq_label;
     DevBuf<int> next_cell;
+    int ft_warps = 8;            // warps per CTA of the persistent fine-tune (8 or 32)
+    int ft_heavy = 6;            // candidates from which a cell takes the split path
+    DevBuf<int64_t> ft_keys;
+    DevBuf<int32_t> ft_ncand;
+    // split path state
+    DevBuf<int32_t> sp_cells;
+    DevBuf<uint8_t> sp_top;
+    DevBuf<int> sp_ntop, sp_rounds, sp_times, sp_state, sp_nS, sp_kq, sp_total, sp_off, sp_eqv;
+    DevBuf<int64_t> sp_nq;
+    DevBuf<double> sp_rq;
+    DevBuf<float> sp_scores, sp_nan;
+    DevBuf<int32_t> ft_order;
+    DevBuf<int> ft_order_n;
     DevBuf<int32_t> d_final, d_rounds;
     DevBuf<float> ft_scratch;
+
+    // learned proposal
+    Mlp mlp;
+    DevBuf<float> mlp_x;
+    DevBuf<uint8_t> mlp_bad, role;
+    DevBuf<int32_t> mlp_y, mlp_idx, mlp_yb, prop, plain, route_final;
+    DevBuf<float> mlp_xb, prop_conf, mlp_scores;
+    DevBuf<int> n_plain;
 
     // per-call query buffers
     DevBuf<float> q_data;
@@ -504,6 +528,8 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
         ctx->prof.end(sp, s);
         ctx->prof.acc.corr_launches += launch_count() - c0;
         sp = ctx->prof.begin(ST_SELECT, s);
+        ctx->prof.acc.select_launches++;
+        ctx->prof.acc.select_bytes += 4ull * (uint64_t)nq * R;
         launch_select_first(ctx->scores.p, R, nq, (int)L, ctx->lq.p, p, thre, ctx->q_n2.p + q0,
                             ctx->label_scores.p + (size_t)q0 * L, ctx->first.p + q0, ctx->flags.p + (size_t)q0 * L,
                             scratch, max_len, ctx->status.p, s);
@@ -793,7 +819,8 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
 // Exact-mode fine-tune: the persistent kernel over a device work queue.  `flags_dev` is the
 // Q x L candidate-flag matrix in device memory.
 void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev, float p, float thre, int times,
-                         int32_t* final_labels, int32_t* rounds_out) {
+                         int32_t* final_labels, int32_t* rounds_out, const int32_t* cell_list = nullptr,
+                         const int* n_list = nullptr) {
     cudaStream_t s = ctx->stream;
     const Markers& mk = ctx->mk;
     const uint32_t Q = q.n_rows, L = mk.n_labels, Wt = ctx->Wt;
@@ -814,10 +841,11 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     int qmax = 32;
     for (uint32_t i = 0; i < Q; ++i) qmax = std::max(qmax, qptr[i + 1] - qptr[i]);
     const int capq = std::min(pow2_at_least(qmax), 8192);
-    const size_t smem = ft_persistent_smem((int)std::max<uint32_t>(Wt, 1), capq);
+    const int nw = ctx->ft_warps;
+    const size_t smem = ft_persistent_smem((int)std::max<uint32_t>(Wt, 1), capq, nw);
     if (smem > 220 * 1024) fail(SGR_ERR_UNSUPPORTED, "fine-tune gene pool too wide for shared memory");
-    const int grid = ft_persistent_grid(smem);
-    const int64_t per_cta = (int64_t)ctx->R + 8 * (int64_t)max_label;
+    const int grid = ft_persistent_grid(smem, nw);
+    const int64_t per_cta = (int64_t)ctx->R + nw * (int64_t)max_label;
     ctx->ft_scratch.ensure((size_t)grid * per_cta);
     ctx->next_cell.ensure(1);
     SGR_CUDA(cudaMemsetAsync(ctx->next_cell.p, 0, sizeof(int), s));
@@ -841,6 +869,46 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     a.p = p;
     a.thre = thre;
     a.times = times;
+    // heaviest cells first (reference rows of their first-round candidates), so that the last cells
+    // on the work queue are light ones; cells with many candidates take the split path
+    std::vector<int32_t> heavy_cells;
+    {
+        int n = (int)Q;
+        std::vector<int32_t> list;
+        if (cell_list) {
+            SGR_CUDA(cudaMemcpyAsync(&n, n_list, sizeof(int), cudaMemcpyDeviceToHost, s));
+            SGR_CUDA(cudaStreamSynchronize(s));
+            list.resize(n);
+            if (n) SGR_CUDA(cudaMemcpyAsync(list.data(), cell_list, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        }
+        ctx->ft_keys.ensure(std::max(n, 1));
+        ctx->ft_ncand.ensure(std::max(n, 1));
+        launch_ft_keys(n, cell_list, (int)L, flags_dev, ctx->d_ctidx.p, ctx->ft_keys.p, ctx->ft_ncand.p, s);
+        std::vector<int64_t> keys(n);
+        std::vector<int32_t> ncand(n);
+        if (n) {
+            SGR_CUDA(cudaMemcpyAsync(keys.data(), ctx->ft_keys.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+            SGR_CUDA(cudaMemcpyAsync(ncand.data(), ctx->ft_ncand.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        }
+        SGR_CUDA(cudaStreamSynchronize(s));
+        std::vector<int32_t> order, heavy;
+        std::vector<int32_t> idx(n);
+        for (int i = 0; i < n; ++i) idx[i] = i;
+        std::stable_sort(idx.begin(), idx.end(), [&](int32_t x, int32_t y) { return keys[x] > keys[y]; });
+        for (int i : idx) {
+            const int32_t c = cell_list ? list[i] : i;
+            if (ncand[i] >= ctx->ft_heavy) heavy.push_back(c);
+            else order.push_back(c);
+        }
+        int n_order = (int)order.size();
+        ctx->ft_order.upload(order.empty() ? std::vector<int32_t>{0} : order, s);
+        ctx->ft_order_n.upload(&n_order, 1, s);
+        cell_list = ctx->ft_order.p;
+        n_list = ctx->ft_order_n.p;
+        heavy_cells.swap(heavy);
+    }
+    a.cell_list = cell_list;
+    a.n_list = n_list;
     a.next_cell = ctx->next_cell.p;
     a.final_labels = ctx->d_final.p;
     a.rounds = ctx->d_rounds.p;
@@ -850,8 +918,44 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     a.max_label = (int)max_label;
     a.capq = capq;
     a.status = ctx->status.p;
-    launch_ft_persistent(a, grid, smem, s);
+    launch_ft_persistent(a, grid, smem, nw, s);
+    // heavy cells: rounds spread over the whole GPU, in batches
+    for (size_t h0 = 0; h0 < heavy_cells.size(); h0 += 1024) {
+        const int H = (int)std::min<size_t>(1024, heavy_cells.size() - h0);
+        ctx->sp_cells.upload(heavy_cells.data() + h0, H, s);
+        ctx->sp_top.ensure((size_t)H * 256);
+        ctx->sp_ntop.ensure(H);
+        ctx->sp_rounds.ensure(H);
+        ctx->sp_times.ensure(H);
+        ctx->sp_state.ensure(H);
+        ctx->sp_nS.ensure(H);
+        ctx->sp_kq.ensure(H);
+        ctx->sp_total.ensure(H);
+        ctx->sp_off.ensure((size_t)H * 257);
+        ctx->sp_eqv.ensure((size_t)H * std::max<uint32_t>(Wt, 1));
+        ctx->sp_nq.ensure(H);
+        ctx->sp_rq.ensure(H);
+        ctx->sp_scores.ensure((size_t)H * ctx->R);
+        ctx->sp_nan.ensure((size_t)H * 8 * max_label);
+        SGR_CUDA(cudaMemsetAsync(ctx->sp_state.p, 0, H * sizeof(int), s));
+        FtSplit sp{ctx->sp_cells.p, ctx->sp_top.p, ctx->sp_ntop.p, ctx->sp_rounds.p, ctx->sp_times.p,
+                   ctx->sp_state.p, ctx->sp_nS.p, ctx->sp_kq.p, ctx->sp_nq.p, ctx->sp_rq.p, ctx->sp_total.p,
+                   ctx->sp_off.p, ctx->sp_eqv.p, ctx->sp_scores.p, ctx->sp_nan.p, (int)ctx->R};
+        const int max_chunks = (int)((ctx->R + 255) / 256);
+        std::vector<int> state(H);
+        // each round drops at least one candidate, so L + 2 rounds finish every cell
+        for (uint32_t round = 0;; ++round) {
+            if (round > L + 3) fail(SGR_ERR_STATE, "fine-tune split path did not converge");
+            launch_split_round(a, sp, H, max_chunks, s);
+            SGR_CUDA(cudaMemcpyAsync(state.data(), ctx->sp_state.p, H * sizeof(int), cudaMemcpyDeviceToHost, s));
+            SGR_CUDA(cudaStreamSynchronize(s));
+            bool all = true;
+            for (int v : state) all &= v == 2;
+            if (all) break;
+        }
+    }
     ctx->prof.end(sp_ft, s);
+    if (!final_labels) return;  // caller reads ctx->d_final / d_rounds itself
     SGR_CUDA(cudaMemcpyAsync(final_labels, ctx->d_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     std::vector<int32_t> rounds(Q);
     SGR_CUDA(cudaMemcpyAsync(rounds.data(), ctx->d_rounds.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -914,6 +1018,21 @@ sgr_status sgr_set_stream(sgr_ctx* ctx, void* stream) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
     return SGR_OK;
+}
+
+sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value) {
+    if (!ctx) return SGR_ERR_INVALID_ARGUMENT;
+    if (what == 0) {
+        if (value != 8 && value != 32) return SGR_ERR_INVALID_ARGUMENT;
+        ctx->ft_warps = value;
+        return SGR_OK;
+    }
+    if (what == 1) {
+        if (value < 2) return SGR_ERR_INVALID_ARGUMENT;
+        ctx->ft_heavy = value;
+        return SGR_OK;
+    }
+    return SGR_ERR_INVALID_ARGUMENT;
 }
 
 sgr_status sgr_set_profiling(sgr_ctx* ctx, int on) {
@@ -1103,6 +1222,183 @@ sgr_status sgr_debug_scores(sgr_ctx* ctx, const sgr_csr* qry, float* out) {
         correlate(ctx, fp32, ctx->q_limbs.p, (int)Q, 0, sc.p, R);
         SGR_CUDA(cudaMemcpyAsync(out, sc.p, (size_t)Q * R * sizeof(float), cudaMemcpyDeviceToHost, s));
         check_status(ctx);
+    });
+}
+
+// ---- learned proposal --------------------------------------------------------------------------
+
+sgr_status sgr_mlp_train(sgr_ctx* ctx, const float* label_scores, const int32_t* targets, uint32_t n,
+                         const sgr_mlp_config* cfg, float* final_loss) {
+    return guarded(ctx, [&] {
+        if (ctx->device < 0) fail(SGR_ERR_STATE, "host-only context");
+        if (!ctx->markers_ready) fail(SGR_ERR_STATE, "train the reference first (the label count)");
+        if (!label_scores || !targets || !cfg || n == 0) fail(SGR_ERR_INVALID_ARGUMENT, "empty training set");
+        const int L = (int)ctx->mk.n_labels;
+        cudaStream_t s = ctx->stream;
+        Mlp& m = ctx->mlp;
+        m.init(L, cfg->hidden ? (int)cfg->hidden : 256, cfg->seed, s);
+        ctx->mlp_scores.upload(label_scores, (size_t)n * L, s);
+        ctx->mlp_x.ensure((size_t)n * L);
+        ctx->mlp_bad.ensure(n);
+        m.features(ctx->mlp_scores.p, (int)n, ctx->mlp_x.p, ctx->mlp_bad.p, s);
+        std::vector<uint8_t> bad(n);
+        SGR_CUDA(cudaMemcpyAsync(bad.data(), ctx->mlp_bad.p, n, cudaMemcpyDeviceToHost, s));
+        SGR_CUDA(cudaStreamSynchronize(s));
+        std::vector<int32_t> good;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (targets[i] < 0 || targets[i] >= L) fail(SGR_ERR_INVALID_ARGUMENT, "target label out of range");
+            if (!bad[i]) good.push_back((int32_t)i);
+        }
+        if (good.empty()) fail(SGR_ERR_INVALID_ARGUMENT, "no training row without NaN scores");
+        ctx->mlp_y.upload(targets, n, s);
+        const int B = (int)std::max<uint32_t>(1, std::min<uint32_t>(cfg->batch ? cfg->batch : 4096, (uint32_t)good.size()));
+        ctx->mlp_xb.ensure((size_t)B * L);
+        ctx->mlp_yb.ensure(B);
+        ctx->mlp_idx.ensure(good.size());
+        std::mt19937_64 rng(cfg->seed ^ 0x5DEECE66Dull);
+        float last = 0.f;
+        const int epochs = cfg->epochs ? (int)cfg->epochs : 20;
+        for (int e = 0; e < epochs; ++e) {
+            std::shuffle(good.begin(), good.end(), rng);
+            ctx->mlp_idx.upload(good, s);
+            for (size_t b0 = 0; b0 < good.size(); b0 += B) {
+                const int nb = (int)std::min<size_t>(B, good.size() - b0);
+                m.gather(ctx->mlp_x.p, ctx->mlp_y.p, ctx->mlp_idx.p + b0, nb, ctx->mlp_xb.p, ctx->mlp_yb.p, s);
+                m.forward(ctx->mlp_xb.p, nb, s);
+                m.backward(ctx->mlp_xb.p, ctx->mlp_yb.p, nb, s);
+                m.adamw(cfg->lr, cfg->beta1, cfg->beta2, cfg->eps, cfg->weight_decay, s);
+                if (e == epochs - 1 && b0 + B >= good.size()) {
+                    std::vector<float> rl(nb);
+                    SGR_CUDA(cudaMemcpyAsync(rl.data(), m.row_loss.p, nb * sizeof(float), cudaMemcpyDeviceToHost, s));
+                    SGR_CUDA(cudaStreamSynchronize(s));
+                    double t = 0;
+                    for (float x : rl) t += x;
+                    last = (float)(t / nb);
+                }
+            }
+        }
+        if (final_loss) *final_loss = last;
+    });
+}
+
+sgr_status sgr_mlp_predict(sgr_ctx* ctx, const float* label_scores, uint32_t n, int32_t* labels, float* confidence) {
+    return guarded(ctx, [&] {
+        if (!ctx->mlp.ready) fail(SGR_ERR_STATE, "no trained proposal network");
+        const int L = ctx->mlp.L;
+        cudaStream_t s = ctx->stream;
+        ctx->mlp_scores.upload(label_scores, (size_t)n * L, s);
+        ctx->mlp_x.ensure((size_t)n * L);
+        ctx->mlp_bad.ensure(n);
+        ctx->prop.ensure(n);
+        ctx->prop_conf.ensure(n);
+        ctx->mlp.features(ctx->mlp_scores.p, (int)n, ctx->mlp_x.p, ctx->mlp_bad.p, s);
+        ctx->mlp.predict(ctx->mlp_x.p, (int)n, ctx->prop.p, ctx->prop_conf.p, s);
+        SGR_CUDA(cudaMemcpyAsync(labels, ctx->prop.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        SGR_CUDA(cudaMemcpyAsync(confidence, ctx->prop_conf.p, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    });
+}
+
+sgr_status sgr_mlp_params(sgr_ctx* ctx, float* out, uint64_t cap, uint32_t* n_labels, uint32_t* hidden,
+                          uint64_t* n_params) {
+    return guarded(ctx, [&] {
+        if (!ctx->mlp.ready) fail(SGR_ERR_STATE, "no proposal network");
+        if (n_labels) *n_labels = (uint32_t)ctx->mlp.L;
+        if (hidden) *hidden = (uint32_t)ctx->mlp.H;
+        if (n_params) *n_params = ctx->mlp.n_params;
+        if (out) {
+            if (cap < ctx->mlp.n_params) fail(SGR_ERR_INVALID_ARGUMENT, "parameter buffer too small");
+            SGR_CUDA(cudaMemcpyAsync(out, ctx->mlp.w.p, ctx->mlp.n_params * sizeof(float), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+        }
+    });
+}
+
+sgr_status sgr_mlp_load(sgr_ctx* ctx, const float* params, uint32_t n_labels, uint32_t hidden) {
+    return guarded(ctx, [&] {
+        if (ctx->device < 0) fail(SGR_ERR_STATE, "host-only context");
+        if (!params || n_labels == 0 || hidden == 0) fail(SGR_ERR_INVALID_ARGUMENT, "bad parameters");
+        ctx->mlp.init((int)n_labels, (int)hidden, 0, ctx->stream);
+        ctx->mlp.set_params(params, ctx->stream);
+    });
+}
+
+sgr_status sgr_mlp_debug_grads(sgr_ctx* ctx, const float* features, const int32_t* targets, uint32_t n, float* grads,
+                               float* loss) {
+    return guarded(ctx, [&] {
+        if (!ctx->mlp.ready) fail(SGR_ERR_STATE, "no proposal network");
+        Mlp& m = ctx->mlp;
+        cudaStream_t s = ctx->stream;
+        ctx->mlp_xb.upload(features, (size_t)n * m.L, s);
+        ctx->mlp_yb.upload(targets, n, s);
+        m.forward(ctx->mlp_xb.p, (int)n, s);
+        m.backward(ctx->mlp_xb.p, ctx->mlp_yb.p, (int)n, s);
+        std::vector<float> rl(n);
+        SGR_CUDA(cudaMemcpyAsync(grads, m.g.p, m.n_params * sizeof(float), cudaMemcpyDeviceToHost, s));
+        SGR_CUDA(cudaMemcpyAsync(rl.data(), m.row_loss.p, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+        SGR_CUDA(cudaStreamSynchronize(s));
+        double t = 0;
+        for (float x : rl) t += x;
+        if (loss) *loss = (float)(t / n);
+    });
+}
+
+sgr_status sgr_annotate_learned(sgr_ctx* ctx, const sgr_csr* qry, float quantile, float finetune_thre,
+                                int32_t finetune_times, float min_confidence, float check_fraction,
+                                int32_t* first_labels, int32_t* final_labels, sgr_learned_stats* stats) {
+    return guarded(ctx, [&] {
+        if (!ctx->trained) fail(SGR_ERR_STATE, "annotate before train");
+        if (ctx->mode != SGR_MODE_EXACT) fail(SGR_ERR_STATE, "the learned form runs in exact mode");
+        if (!ctx->mlp.ready || ctx->mlp.L != (int)ctx->mk.n_labels) fail(SGR_ERR_STATE, "no proposal network");
+        if (!first_labels || !final_labels) fail(SGR_ERR_INVALID_ARGUMENT, "null output");
+        reset_status(ctx);
+        DevCsr q = query_on_device(ctx, qry);
+        const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
+        if (stats) *stats = sgr_learned_stats{};
+        if (Q == 0) return;
+        cudaStream_t s = ctx->stream;
+        score_device(ctx, q, quantile, finetune_thre);
+        const int sp = ctx->prof.begin(ST_MLP, s);
+        ctx->mlp_x.ensure((size_t)Q * L);
+        ctx->mlp_bad.ensure(Q);
+        ctx->prop.ensure(Q);
+        ctx->prop_conf.ensure(Q);
+        ctx->route_final.ensure(Q);
+        ctx->plain.ensure(Q);
+        ctx->role.ensure(Q);
+        ctx->n_plain.ensure(1);
+        ctx->mlp.features(ctx->label_scores.p, (int)Q, ctx->mlp_x.p, ctx->mlp_bad.p, s);
+        ctx->mlp.predict(ctx->mlp_x.p, (int)Q, ctx->prop.p, ctx->prop_conf.p, s);
+        SGR_CUDA(cudaMemsetAsync(ctx->n_plain.p, 0, sizeof(int), s));
+        const uint32_t per10k = (uint32_t)std::lround(std::min(std::max(check_fraction, 0.f), 1.f) * 10000.f);
+        launch_learned_route((int)Q, (int)L, ctx->flags.p, ctx->mlp_bad.p, ctx->prop.p, ctx->prop_conf.p,
+                             min_confidence, per10k, 0x243F6A8885A308D3ull, ctx->route_final.p, ctx->plain.p,
+                             ctx->n_plain.p, ctx->role.p, s);
+        ctx->prof.end(sp, s);
+        finetune_persistent(ctx, q, ctx->flags.p, quantile, finetune_thre, finetune_times, nullptr, nullptr,
+                            ctx->plain.p, ctx->n_plain.p);
+        std::vector<int32_t> rf(Q), ff(Q);
+        std::vector<uint8_t> role(Q);
+        SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        SGR_CUDA(cudaMemcpyAsync(rf.data(), ctx->route_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        SGR_CUDA(cudaMemcpyAsync(ff.data(), ctx->d_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        SGR_CUDA(cudaMemcpyAsync(role.data(), ctx->role.p, Q, cudaMemcpyDeviceToHost, s));
+        check_status(ctx);
+        sgr_learned_stats st{};
+        st.cells = Q;
+        for (uint32_t i = 0; i < Q; ++i) {
+            if (role[i] == 0) {
+                final_labels[i] = rf[i];
+                st.decided++;
+            } else {
+                final_labels[i] = ff[i];
+                st.finetuned++;
+                if (role[i] == 2) {
+                    st.checked++;
+                    st.check_agree += rf[i] == ff[i];
+                }
+            }
+        }
+        if (stats) *stats = st;
     });
 }
 

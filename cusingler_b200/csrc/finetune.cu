@@ -79,217 +79,193 @@ __global__ void __launch_bounds__(256) ref_presort_kernel(const float* data, con
     }
 }
 
+// Fine-tune workload of a cell: the reference rows of its first-round candidates (0 when it has at
+// most one candidate and needs no round).
+__global__ void ft_keys_kernel(int n, const int32_t* list, int L, const uint8_t* flags, const uint32_t* ctidx,
+                               int64_t* keys, int32_t* ncand) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int q = list ? list[i] : i;
+    const uint8_t* f = flags + (int64_t)q * L;
+    int64_t w = 0;
+    int c = 0;
+    for (int l = 0; l < L; ++l)
+        if (f[l]) {
+            ++c;
+            w += ctidx[2 * l + 1];
+        }
+    keys[i] = c >= 2 ? w : 0;
+    ncand[i] = c;
+}
+
 struct FtShared {
     int cell, ntop, nS, kq, rounds, done;
     int64_t nq;
     double rq;
 };
 
-__global__ void __launch_bounds__(256) ft_persistent_kernel(FtPersistentArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
+// Candidates of a cell: its flagged labels in ascending order (src/cusingler.cu:1305-1312).  Warp.
+__device__ int warp_flagged_labels(const uint8_t* flags, int L, uint8_t* top, int lane) {
+    int n = 0;
+    for (int base = 0; base < L; base += 32) {
+        const int l = base + lane;
+        const bool f = l < L && flags[l] != 0;
+        const unsigned m = __ballot_sync(FULL, f);
+        if (f) top[n + __popc(m & ((1u << lane) - 1u))] = (uint8_t)l;
+        n += __popc(m);
+    }
+    return n;
+}
+
+// Gene set S of a candidate list: union over ordered pairs of the first min(len, gene_thre(n))
+// genes of the pair's fine-tune list (src/cusingler.cu:1141-1156), as bits over the thre pool.
+// CTA-wide; returns |S| to every thread.
+template <int NW>
+__device__ int cta_gene_set(const FtPersistentArgs& a, const uint8_t* top, int ntop, uint32_t* bits, int* red) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int Wt = a.Wt, L = a.L;
-    const int nwords = (Wt + 31) / 32;
-    int* eqv = reinterpret_cast<int*>(smem);                                     // Wt
-    uint32_t* bits = reinterpret_cast<uint32_t*>(eqv + ((Wt + 3) & ~3));         // nwords
-    uint64_t* qkeys = reinterpret_cast<uint64_t*>(bits + ((nwords + 3) & ~3));   // capq (8-byte aligned)
-    int* hist = reinterpret_cast<int*>(qkeys + a.capq);                          // 8 * 256
-    float* lsc = reinterpret_cast<float*>(hist + 8 * 256);                       // 256
-    int* off = reinterpret_cast<int*>(lsc + 256);                                // 257
-    int* red = off + 257;                                                        // 8 (+pad)
-    uint8_t* top = reinterpret_cast<uint8_t*>(red + 16);                         // 256
-    uint8_t* ntopv = top + 256;                                                  // 256
-    __shared__ FtShared sh;
+    const int nwords = (a.Wt + 31) / 32;
+    for (int w = tid; w < nwords; w += NW * 32) bits[w] = 0u;
+    __syncthreads();
+    const int gthre = a.gene_thre[ntop];
+    for (int pr = warp; pr < ntop * ntop; pr += NW) {
+        const int i = pr / ntop, j = pr % ntop;
+        if (i == j) continue;
+        const int li = top[i], lj = top[j];
+        const uint32_t pos = a.ft_idx[2 * ((size_t)li * a.L + lj)];
+        int len = (int)a.ft_idx[2 * ((size_t)li * a.L + lj) + 1];
+        if (len > gthre) len = gthre;
+        for (int e = lane; e < len; e += 32) {
+            const uint32_t g = a.ft_genes[pos + e];
+            atomicOr(&bits[g >> 5], 1u << (g & 31));
+        }
+    }
+    __syncthreads();
+    int cnt = 0;
+    for (int w = tid; w < nwords; w += NW * 32) cnt += __popc(bits[w]);
+    cnt = __reduce_add_sync(FULL, cnt);
+    if (lane == 0) red[warp] = cnt;
+    __syncthreads();
+    int t = 0;
+    for (int w = 0; w < NW; ++w) t += red[w];
+    __syncthreads();
+    return t;
+}
 
-    float* scores = a.scratch + (size_t)blockIdx.x * a.scratch_per_cta;
-    float* nan_scratch = scores + a.max_rcand;
-
-    for (;;) {
-        if (tid == 0) sh.cell = atomicAdd(a.next_cell, 1);
-        __syncthreads();
-        const int cell = sh.cell;
-        if (cell >= a.Q) break;
-
-        // candidates: flagged labels in ascending order (src/cusingler.cu:1305-1312)
-        if (warp == 0) {
-            int n = 0;
-            for (int base = 0; base < L; base += 32) {
-                const int l = base + lane;
-                const bool f = l < L && a.flags[(size_t)cell * L + l] != 0;
-                const unsigned m = __ballot_sync(FULL, f);
-                if (f) top[n + __popc(m & ((1u << lane) - 1u))] = (uint8_t)l;
-                n += __popc(m);
+// The query's e-values over S: 0 at genes of S it does not store, |S| - k + 2 #less + #equal at
+// stored ones, SENT outside S.  CTA-wide (the ranking itself by warp 0); sets *kq, *nq, *rq.
+template <int NW>
+__device__ void cta_query_ranks(const FtPersistentArgs& a, int cell, int nS, const uint32_t* bits, int* eqv,
+                                uint64_t* qkeys, int* kq_out, int64_t* nq_out, double* rq_out) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int g = tid; g < a.Wt; g += NW * 32) eqv[g] = (bits[g >> 5] >> (g & 31)) & 1u ? 0 : SENT;
+    __syncthreads();
+    if (warp == 0) {
+        const int beg = a.qf_ptr[cell], end = a.qf_ptr[cell + 1];
+        int k = 0;
+        for (int base = beg; base < end; base += 32) {
+            const int i = base + lane;
+            bool hit = false;
+            uint64_t key = 0;
+            if (i < end) {
+                const int g = a.qf_idx[i];
+                if ((bits[g >> 5] >> (g & 31)) & 1u) {
+                    hit = true;
+                    key = ((uint64_t)ord_key(canon_zero(a.qf_data[i])) << 32) | (uint32_t)g;
+                }
             }
-            if (lane == 0) {
-                sh.ntop = n;
-                sh.rounds = 0;
-                sh.done = 0;
+            const unsigned m = __ballot_sync(FULL, hit);
+            if (hit) {
+                const int o = k + __popc(m & ((1u << lane) - 1u));
+                if (o < a.capq) qkeys[o] = key;
+            }
+            k += __popc(m);
+        }
+        __syncwarp();
+        int64_t sq = 0;
+        if (k <= a.capq) {
+            int n = 1;
+            while (n < k) n <<= 1;
+            for (int i = k + lane; i < n; i += 32) qkeys[i] = ~0ull;
+            __syncwarp();
+            if (k > 1) warp_bitonic(qkeys, n, lane);
+            for (int j = lane; j < k; j += 32) {
+                const uint64_t key = qkeys[j];
+                const uint32_t hv = (uint32_t)(key >> 32);
+                const int lo = lower_hi(qkeys, k, hv), hi = upper_hi(qkeys, k, hv);
+                const int e = nS - k + 2 * lo + (hi - lo);
+                eqv[(int)(uint32_t)key] = e;
+                sq += (int64_t)(e - k) * (e - k);
+            }
+        } else {
+            for (int i = beg + lane; i < end; i += 32) {
+                const int g = a.qf_idx[i];
+                if (!((bits[g >> 5] >> (g & 31)) & 1u)) continue;
+                const float v = canon_zero(a.qf_data[i]);
+                int less = 0, eq = 0;
+                for (int j = beg; j < end; ++j) {
+                    const int h = a.qf_idx[j];
+                    if (!((bits[h >> 5] >> (h & 31)) & 1u)) continue;
+                    const float w = canon_zero(a.qf_data[j]);
+                    less += w < v;
+                    eq += w == v;
+                }
+                const int e = nS - k + 2 * less + eq;
+                eqv[g] = e;
+                sq += (int64_t)(e - k) * (e - k);
             }
         }
-        __syncthreads();
-        int times_used = 0;
-        for (;;) {
-            const int ntop = sh.ntop;
-            if (!(ntop > 1 && (a.times == 0 || times_used++ < a.times))) break;
-            // 1) gene set S over the thre pool
-            for (int w = tid; w < nwords; w += blockDim.x) bits[w] = 0u;
-            __syncthreads();
-            const int gthre = a.gene_thre[ntop];
-            for (int pr = warp; pr < ntop * ntop; pr += 8) {
-                const int i = pr / ntop, j = pr % ntop;
-                if (i == j) continue;
-                const int li = top[i], lj = top[j];
-                const uint32_t pos = a.ft_idx[2 * ((size_t)li * L + lj)];
-                int len = (int)a.ft_idx[2 * ((size_t)li * L + lj) + 1];
-                if (len > gthre) len = gthre;
-                for (int e = lane; e < len; e += 32) {
-                    const uint32_t g = a.ft_genes[pos + e];
-                    atomicOr(&bits[g >> 5], 1u << (g & 31));
-                }
-            }
-            __syncthreads();
-            int cnt = 0;
-            for (int w = tid; w < nwords; w += blockDim.x) cnt += __popc(bits[w]);
-            cnt = __reduce_add_sync(FULL, cnt);
-            if (lane == 0) red[warp] = cnt;
-            __syncthreads();
-            if (tid == 0) {
-                int t = 0;
-                for (int w = 0; w < 8; ++w) t += red[w];
-                sh.nS = t;
-                sh.rounds++;
-            }
-            __syncthreads();
-            const int nS = sh.nS;
-            if (nS < 20) {  // keep the first candidate (src/cusingler.cu:1158-1159)
-                if (tid == 0) sh.ntop = 1;
-                __syncthreads();
-                continue;
-            }
-            // 2) query ranks over S: e = |S| - k + 2 #less + #equal at stored genes, 0 elsewhere in S
-            for (int g = tid; g < Wt; g += blockDim.x) eqv[g] = (bits[g >> 5] >> (g & 31)) & 1u ? 0 : SENT;
-            __syncthreads();
-            if (warp == 0) {
-                const int beg = a.qf_ptr[cell], end = a.qf_ptr[cell + 1];
-                int k = 0;
-                for (int base = beg; base < end; base += 32) {
-                    const int i = base + lane;
-                    bool hit = false;
-                    uint64_t key = 0;
-                    if (i < end) {
-                        const int g = a.qf_idx[i];
-                        if ((bits[g >> 5] >> (g & 31)) & 1u) {
-                            hit = true;
-                            key = ((uint64_t)ord_key(canon_zero(a.qf_data[i])) << 32) | (uint32_t)g;
-                        }
-                    }
-                    const unsigned m = __ballot_sync(FULL, hit);
-                    if (hit) {
-                        const int o = k + __popc(m & ((1u << lane) - 1u));
-                        if (o < a.capq) qkeys[o] = key;
-                    }
-                    k += __popc(m);
-                }
-                __syncwarp();
-                int64_t sq = 0;
-                if (k <= a.capq) {
-                    int n = 1;
-                    while (n < k) n <<= 1;
-                    for (int i = k + lane; i < n; i += 32) qkeys[i] = ~0ull;
-                    __syncwarp();
-                    if (k > 1) warp_bitonic(qkeys, n, lane);
-                    for (int j = lane; j < k; j += 32) {
-                        const uint64_t key = qkeys[j];
-                        const uint32_t hv = (uint32_t)(key >> 32);
-                        const int lo = lower_hi(qkeys, k, hv), hi = upper_hi(qkeys, k, hv);
-                        const int e = nS - k + 2 * lo + (hi - lo);
-                        eqv[(int)(uint32_t)key] = e;
-                        sq += (int64_t)(e - k) * (e - k);
-                    }
-                } else {
-                    for (int i = beg + lane; i < end; i += 32) {
-                        const int g = a.qf_idx[i];
-                        if (!((bits[g >> 5] >> (g & 31)) & 1u)) continue;
-                        const float v = canon_zero(a.qf_data[i]);
-                        int less = 0, eq = 0;
-                        for (int j = beg; j < end; ++j) {
-                            const int h = a.qf_idx[j];
-                            if (!((bits[h >> 5] >> (h & 31)) & 1u)) continue;
-                            const float w = canon_zero(a.qf_data[j]);
-                            less += w < v;
-                            eq += w == v;
-                        }
-                        const int e = nS - k + 2 * less + eq;
-                        eqv[g] = e;
-                        sq += (int64_t)(e - k) * (e - k);
-                    }
-                }
-                for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(FULL, sq, o);
-                if (lane == 0) {
-                    const int64_t nq = sq + (int64_t)(nS - k) * k * k;
-                    sh.kq = k;
-                    sh.nq = nq;
-                    sh.rq = nq > 0 ? 1.0 / sqrt((double)nq) : 0.0;
-                }
-            }
-            if (tid == 0) {
-                int o = 0;
-                for (int i = 0; i < ntop; ++i) {
-                    off[i] = o;
-                    o += (int)a.ctidx[2 * top[i] + 1];
-                }
-                off[ntop] = o;
-            }
-            __syncthreads();
-            // 3) correlation with every reference cell of every candidate label
-            const int total = off[ntop];
-            const int kq = sh.kq;
-            const int64_t nq = sh.nq;
-            const double rq = sh.rq;
-            // one lane per reference row: a single pass over the row's entries in value order,
-            // keeping the genes in S (see the comment at the top of this file)
-            for (int f = tid; f < total; f += blockDim.x) {
-                int lo = 0, hi = ntop - 1;  // label slot: off[lo] <= f < off[lo+1]
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (off[mid] <= f) lo = mid;
-                    else hi = mid - 1;
-                }
-                const int r = (int)a.ctidx[2 * top[lo]] + (f - off[lo]);
-                const int beg = a.ref_ptr[r], end = a.ref_ptr[r + 1];
-                int64_t X = 0, Y = 0, Z1 = 0, Z2 = 0;
-                int ka = 0, b = 0, sum = 0;
-                uint32_t cur = 0xffffffffu;
-                // 16-byte loads of four entries (the list base is 16-byte aligned; the first and
-                // last words are masked to [beg, end))
-                for (int j4 = beg & ~3; j4 < end; j4 += 4) {
-                    const uint4 w4 = __ldg(reinterpret_cast<const uint4*>(a.ref_sorted + j4));
-                    const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(FULL, sq, o);
+        if (lane == 0) {
+            const int64_t nq = sq + (int64_t)(nS - k) * k * k;
+            *kq_out = k;
+            *nq_out = nq;
+            *rq_out = nq > 0 ? 1.0 / sqrt((double)nq) : 0.0;
+        }
+    }
+    __syncthreads();
+}
+
+// Reference-row slot layout of a candidate list: label i's rows are [off[i], off[i+1]).  Thread 0.
+__device__ void label_offsets(const FtPersistentArgs& a, const uint8_t* top, int ntop, int* off) {
+    int o = 0;
+    for (int i = 0; i < ntop; ++i) {
+        off[i] = o;
+        o += (int)a.ctidx[2 * top[i] + 1];
+    }
+    off[ntop] = o;
+}
+
+// Exact correlation over S of the query (eqv, kq, nq) with reference row slot f of the list.
+// One thread: one pass over the row's value-sorted entries (see the top of this file).
+__device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const int* off, int ntop, int f,
+                           const int* eqv, int nS, int kq, int64_t nq, double rq) {
+    int lo = 0, hi = ntop - 1;  // label slot: off[lo] <= f < off[lo+1]
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= f) lo = mid;
+        else hi = mid - 1;
+    }
+    const int r = (int)a.ctidx[2 * top[lo]] + (f - off[lo]);
+    const int beg = a.ref_ptr[r], end = a.ref_ptr[r + 1];
+    int64_t X = 0, Y = 0, Z1 = 0, Z2 = 0;
+    int ka = 0, b = 0, sum = 0;
+    uint32_t cur = 0xffffffffu;
+    // 16-byte loads of four entries (the list base is 16-byte aligned and padded; the first and
+    // last words are masked to [beg, end)); the next load is issued before the current is used
+    uint4 nxt = __ldg(reinterpret_cast<const uint4*>(a.ref_sorted + (beg & ~3)));
+    for (int j4 = beg & ~3; j4 < end; j4 += 4) {
+        const uint4 w4 = nxt;
+        if (j4 + 4 < end) nxt = __ldg(reinterpret_cast<const uint4*>(a.ref_sorted + j4 + 4));
+        const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int j = j4 + u;
-                        if (j < beg || j >= end) continue;
-                        const uint32_t ent = ws[u];
-                        const int v = eqv[ent & 0xffffu];
-                        if (v == SENT) continue;
-                        const uint32_t run = ent >> 16;
-                        if (run != cur) {
-                            if (b) {
-                                const int64_t z = 2 * ka + b;
-                                X += z * sum;
-                                Y += sum;
-                                Z1 += b * z;
-                                Z2 += b * z * z;
-                                ka += b;
-                            }
-                            b = 0;
-                            sum = 0;
-                            cur = run;
-                        }
-                        ++b;
-                        sum += v;
-                    }
-                }
+        for (int u = 0; u < 4; ++u) {
+            const int j = j4 + u;
+            if (j < beg || j >= end) continue;
+            const uint32_t ent = ws[u];
+            const int v = eqv[ent & 0xffffu];
+            if (v == SENT) continue;
+            const uint32_t run = ent >> 16;
+            if (run != cur) {
                 if (b) {
                     const int64_t z = 2 * ka + b;
                     X += z * sum;
@@ -298,50 +274,134 @@ __global__ void __launch_bounds__(256) ft_persistent_kernel(FtPersistentArgs a) 
                     Z2 += b * z * z;
                     ka += b;
                 }
-                const int64_t kr = ka;
-                const int64_t N = X + ((int64_t)nS - kr) * Y - (int64_t)nS * kq * kr;
-                const int64_t c = (int64_t)nS - 2 * kr;
-                const int64_t nr = Z2 + 2 * c * Z1 + kr * c * c + ((int64_t)nS - kr) * kr * kr;
-                float sc;
-                if (nq == 0 || nr == 0) sc = __int_as_float(0x7fffffff);
-                else sc = (float)(((double)N * rq) * (1.0 / sqrt((double)nr)));
-                scores[f] = sc;
+                b = 0;
+                sum = 0;
+                cur = run;
             }
-            __syncthreads();
-            // 4) per-label quantile, then keep / drop (src/cusingler.cu:1256-1295)
-            for (int i = warp; i < ntop; i += 8) {
-                LabelQ q = a.lq_label[top[i]];
-                const float v = quantile_warp(scores + off[i], q, a.p, hist + 256 * warp,
-                                                  nan_scratch + (size_t)warp * a.max_label, lane, a.status);
-                if (lane == 0) lsc[i] = v;
+            ++b;
+            sum += v;
+        }
+    }
+    if (b) {
+        const int64_t z = 2 * ka + b;
+        X += z * sum;
+        Y += sum;
+        Z1 += b * z;
+        Z2 += b * z * z;
+        ka += b;
+    }
+    const int64_t kr = ka;
+    const int64_t N = X + ((int64_t)nS - kr) * Y - (int64_t)nS * kq * kr;
+    const int64_t c = (int64_t)nS - 2 * kr;
+    const int64_t nr = Z2 + 2 * c * Z1 + kr * c * c + ((int64_t)nS - kr) * kr * kr;
+    if (nq == 0 || nr == 0) return __int_as_float(0x7fffffff);
+    return (float)(((double)N * rq) * (1.0 / sqrt((double)nr)));
+}
+
+// Per-label quantiles of the scores laid out by off[] (warps over labels).  CTA-wide.
+template <int NW>
+__device__ void cta_label_quantiles(const FtPersistentArgs& a, const uint8_t* top, const int* off, int ntop,
+                                    const float* scores, float* lsc, int* hist, float* nan_scratch) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = warp; i < ntop; i += NW) {
+        LabelQ q = a.lq_label[top[i]];
+        const float v = quantile_warp(scores + off[i], q, a.p, hist + 256 * warp,
+                                      nan_scratch + (size_t)warp * a.max_label, lane, a.status);
+        if (lane == 0) lsc[i] = v;
+    }
+    (void)tid;
+    __syncthreads();
+}
+
+// The reference's keep / drop rule (src/cusingler.cu:1270-1295) on the list order: returns the new
+// list length, the new list in top.  One thread.
+__device__ int decide_top(const float* lsc, int ntop, uint8_t* top, uint8_t* tmp, float thre) {
+    int mn, mx;
+    stl::minmax(lsc, ntop, &mn, &mx);
+    const float lo = lsc[mn], hi = lsc[mx];
+    const float t = __fsub_rn(hi, thre);
+    int n = 0;
+    if (!(hi != hi)) {
+        for (int i = 0; i < ntop; ++i) {
+            const float s = lsc[i];
+            if (s <= lo || s < t) continue;
+            if (s == hi) {
+                for (int j = n; j > 0; --j) tmp[j] = tmp[j - 1];
+                tmp[0] = top[i];
+            } else {
+                tmp[n] = top[i];
             }
-            __syncthreads();
-            if (tid == 0) {
-                int mn, mx;
-                stl::minmax(lsc, ntop, &mn, &mx);
-                const float lo = lsc[mn], hi = lsc[mx];
-                const float t = __fsub_rn(hi, a.thre);
-                int n = 0;
-                if (!(hi != hi)) {
-                    for (int i = 0; i < ntop; ++i) {
-                        const float s = lsc[i];
-                        if (s <= lo || s < t) continue;
-                        if (s == hi) {
-                            for (int j = n; j > 0; --j) ntopv[j] = ntopv[j - 1];
-                            ntopv[0] = top[i];
-                        } else {
-                            ntopv[n] = top[i];
-                        }
-                        ++n;
-                    }
-                }
-                if (n == 0) {
-                    ntopv[0] = top[0];
-                    n = 1;
-                }
-                for (int i = 0; i < n; ++i) top[i] = ntopv[i];
+            ++n;
+        }
+    }
+    if (n == 0) {
+        tmp[0] = top[0];
+        n = 1;
+    }
+    for (int i = 0; i < n; ++i) top[i] = tmp[i];
+    return n;
+}
+
+template <int NW>
+__global__ void __launch_bounds__(NW * 32) ft_persistent_kernel(FtPersistentArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int Wt = a.Wt, L = a.L;
+    const int nwords = (Wt + 31) / 32;
+    int* eqv = reinterpret_cast<int*>(smem);                                     // Wt
+    uint32_t* bits = reinterpret_cast<uint32_t*>(eqv + ((Wt + 3) & ~3));         // nwords
+    uint64_t* qkeys = reinterpret_cast<uint64_t*>(bits + ((nwords + 3) & ~3));   // capq (8-byte aligned)
+    int* hist = reinterpret_cast<int*>(qkeys + a.capq);                          // NW * 256
+    float* lsc = reinterpret_cast<float*>(hist + NW * 256);                      // 256
+    int* off = reinterpret_cast<int*>(lsc + 256);                                // 257
+    int* red = off + 257;                                                        // NW
+    uint8_t* top = reinterpret_cast<uint8_t*>(red + NW);                         // 256
+    uint8_t* ntopv = top + 256;                                                  // 256
+    __shared__ FtShared sh;
+
+    float* scores = a.scratch + (size_t)blockIdx.x * a.scratch_per_cta;
+    float* nan_scratch = scores + a.max_rcand;
+
+    for (;;) {
+        if (tid == 0) {
+            const int i = atomicAdd(a.next_cell, 1);
+            const int n = a.cell_list ? *a.n_list : a.Q;
+            sh.cell = i < n ? (a.cell_list ? a.cell_list[i] : i) : -1;
+        }
+        __syncthreads();
+        const int cell = sh.cell;
+        if (cell < 0) break;
+        if (warp == 0) {
+            const int n = warp_flagged_labels(a.flags + (size_t)cell * L, L, top, lane);
+            if (lane == 0) {
                 sh.ntop = n;
+                sh.rounds = 0;
             }
+        }
+        __syncthreads();
+        int times_used = 0;
+        for (;;) {
+            const int ntop = sh.ntop;
+            if (!(ntop > 1 && (a.times == 0 || times_used++ < a.times))) break;
+            const int nS = cta_gene_set<NW>(a, top, ntop, bits, red);
+            if (tid == 0) sh.rounds++;
+            if (nS < 20) {  // keep the first candidate (src/cusingler.cu:1158-1159)
+                if (tid == 0) sh.ntop = 1;
+                __syncthreads();
+                continue;
+            }
+            cta_query_ranks<NW>(a, cell, nS, bits, eqv, qkeys, &sh.kq, &sh.nq, &sh.rq);
+            if (tid == 0) label_offsets(a, top, ntop, off);
+            __syncthreads();
+            const int total = off[ntop];
+            const int kq = sh.kq;
+            const int64_t nq = sh.nq;
+            const double rq = sh.rq;
+            for (int f = tid; f < total; f += NW * 32)
+                scores[f] = row_score(a, top, off, ntop, f, eqv, nS, kq, nq, rq);
+            __syncthreads();
+            cta_label_quantiles<NW>(a, top, off, ntop, scores, lsc, hist, nan_scratch);
+            if (tid == 0) sh.ntop = decide_top(lsc, ntop, top, ntopv, a.thre);
             __syncthreads();
         }
         if (tid == 0) {
@@ -352,15 +412,166 @@ __global__ void __launch_bounds__(256) ft_persistent_kernel(FtPersistentArgs a) 
     }
 }
 
+// ---- split path: one round of many heavy cells spread over the whole GPU ----------------------
+//
+// State per heavy cell i (device arrays of FtSplit): candidate list, its length, rounds, times used,
+// active flag; per round: the query's e-values, |S|, k_q, n_q, label offsets, and the scores.
+
+// Round setup per heavy cell: round condition, gene set, query ranks, label offsets.  grid = H.
+__global__ void __launch_bounds__(256) split_prepare_kernel(FtPersistentArgs a, FtSplit sp) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int NW = 8;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i = blockIdx.x;
+    const int Wt = a.Wt, L = a.L;
+    const int nwords = (Wt + 31) / 32;
+    int* eqv = reinterpret_cast<int*>(smem);
+    uint32_t* bits = reinterpret_cast<uint32_t*>(eqv + ((Wt + 3) & ~3));
+    uint64_t* qkeys = reinterpret_cast<uint64_t*>(bits + ((nwords + 3) & ~3));
+    int* red = reinterpret_cast<int*>(qkeys + a.capq);
+    __shared__ int s_ntop, s_go;
+    uint8_t* top = sp.top + (size_t)i * 256;
+    const int cell = sp.cells[i];
+    if (tid == 0) {
+        if (sp.state[i] == 0) {  // first round: candidates from the flags
+            s_ntop = -1;
+        } else {
+            s_ntop = sp.ntop[i];
+        }
+    }
+    __syncthreads();
+    if (s_ntop < 0) {
+        if (warp == 0) {
+            const int n = warp_flagged_labels(a.flags + (size_t)cell * L, L, top, lane);
+            if (lane == 0) {
+                s_ntop = n;
+                sp.ntop[i] = n;
+                sp.rounds[i] = 0;
+                sp.times[i] = 0;
+                sp.state[i] = 1;
+            }
+        }
+        __syncthreads();
+    }
+    const int ntop = s_ntop;
+    if (tid == 0) {
+        bool go = sp.state[i] == 1 && ntop > 1;
+        if (go && a.times != 0) go = sp.times[i]++ < a.times;
+        if (!go) {
+            if (sp.state[i] == 1) {
+                a.final_labels[cell] = ntop > 0 ? (int32_t)top[0] : 0;
+                if (a.rounds) a.rounds[cell] = sp.rounds[i];
+            }
+            sp.state[i] = 2;  // finished
+        } else {
+            sp.rounds[i]++;
+        }
+        s_go = go;
+        sp.total[i] = 0;
+    }
+    __syncthreads();
+    if (!s_go) return;
+    const int nS = cta_gene_set<NW>(a, top, ntop, bits, red);
+    if (nS < 20) {  // keep the first candidate
+        if (tid == 0) sp.ntop[i] = 1;
+        return;
+    }
+    __shared__ int s_kq;
+    __shared__ int64_t s_nq;
+    __shared__ double s_rq;
+    cta_query_ranks<NW>(a, cell, nS, bits, eqv, qkeys, &s_kq, &s_nq, &s_rq);
+    int* geqv = sp.eqv + (size_t)i * Wt;
+    for (int g = tid; g < Wt; g += NW * 32) geqv[g] = eqv[g];
+    if (tid == 0) {
+        label_offsets(a, top, ntop, sp.off + (size_t)i * 257);
+        sp.nS[i] = nS;
+        sp.kq[i] = s_kq;
+        sp.nq[i] = s_nq;
+        sp.rq[i] = s_rq;
+        sp.total[i] = sp.off[(size_t)i * 257 + ntop];
+    }
+}
+
+// Scores of 256-row chunks of every heavy cell's candidate rows.  grid = (chunks, H).
+__global__ void __launch_bounds__(256) split_scan_kernel(FtPersistentArgs a, FtSplit sp) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int i = blockIdx.y;
+    const int total = sp.total[i];
+    const int f = blockIdx.x * 256 + threadIdx.x;
+    if ((int)blockIdx.x * 256 >= total) return;
+    int* eqv = reinterpret_cast<int*>(smem);
+    int* off = eqv + ((a.Wt + 3) & ~3);
+    uint8_t* top = reinterpret_cast<uint8_t*>(off + 260);
+    const int* geqv = sp.eqv + (size_t)i * a.Wt;
+    const int ntop = sp.ntop[i];
+    for (int g = threadIdx.x; g < a.Wt; g += 256) eqv[g] = geqv[g];
+    for (int t = threadIdx.x; t <= ntop; t += 256) off[t] = sp.off[(size_t)i * 257 + t];
+    for (int t = threadIdx.x; t < ntop; t += 256) top[t] = sp.top[(size_t)i * 256 + t];
+    __syncthreads();
+    if (f < total)
+        sp.scores[(size_t)i * sp.max_rcand + f] =
+            row_score(a, top, off, ntop, f, eqv, sp.nS[i], sp.kq[i], sp.nq[i], sp.rq[i]);
+}
+
+// Per-label quantiles and the keep / drop rule per heavy cell.  grid = H.
+__global__ void __launch_bounds__(256) split_decide_kernel(FtPersistentArgs a, FtSplit sp) {
+    constexpr int NW = 8;
+    __shared__ int hist[NW * 256];
+    __shared__ float lsc[256];
+    __shared__ int off[257];
+    __shared__ uint8_t top[256], tmp[256];
+    const int i = blockIdx.x;
+    if (sp.total[i] == 0) return;  // finished, or kept its first candidate this round
+    const int ntop = sp.ntop[i];
+    for (int t = threadIdx.x; t <= ntop; t += 256) off[t] = sp.off[(size_t)i * 257 + t];
+    for (int t = threadIdx.x; t < ntop; t += 256) top[t] = sp.top[(size_t)i * 256 + t];
+    __syncthreads();
+    cta_label_quantiles<NW>(a, top, off, ntop, sp.scores + (size_t)i * sp.max_rcand, lsc, hist,
+                            sp.nan_scratch + (size_t)i * NW * a.max_label);
+    if (threadIdx.x == 0) {
+        const int n = decide_top(lsc, ntop, top, tmp, a.thre);
+        for (int t = 0; t < n; ++t) sp.top[(size_t)i * 256 + t] = top[t];
+        sp.ntop[i] = n;
+    }
+}
+
 }  // namespace
 
-size_t ft_persistent_smem(int Wt, int capq) {
+size_t split_prepare_smem(int Wt, int capq) {
+    const int nwords = (Wt + 31) / 32;
+    return sizeof(int) * ((Wt + 3) & ~3) + sizeof(uint32_t) * ((nwords + 3) & ~3) + sizeof(uint64_t) * capq +
+           sizeof(int) * 16;
+}
+
+void launch_split_round(const FtPersistentArgs& a, const FtSplit& sp, int H, int max_chunks, cudaStream_t s) {
+    const size_t sm1 = split_prepare_smem(a.Wt, a.capq);
+    SGR_CUDA(cudaFuncSetAttribute(split_prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+    split_prepare_kernel<<<H, 256, sm1, s>>>(a, sp);
+    SGR_LAUNCH_CHECK();
+    const size_t sm2 = sizeof(int) * (((a.Wt + 3) & ~3) + 260) + 256;
+    SGR_CUDA(cudaFuncSetAttribute(split_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    split_scan_kernel<<<dim3(max_chunks, H), 256, sm2, s>>>(a, sp);
+    SGR_LAUNCH_CHECK();
+    split_decide_kernel<<<H, 256, 0, s>>>(a, sp);
+    SGR_LAUNCH_CHECK();
+    count_launch(3);
+}
+
+void launch_ft_keys(int n, const int32_t* list, int L, const uint8_t* flags, const uint32_t* ctidx, int64_t* keys,
+                    int32_t* ncand, cudaStream_t s) {
+    if (n <= 0) return;
+    ft_keys_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, list, L, flags, ctidx, keys, ncand);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+size_t ft_persistent_smem(int Wt, int capq, int nw) {
     const int nwords = (Wt + 31) / 32;
     size_t b = 0;
     b += sizeof(int) * ((Wt + 3) & ~3);
     b += sizeof(uint32_t) * ((nwords + 3) & ~3);
     b += sizeof(uint64_t) * capq;
-    b += sizeof(int) * 8 * 256 + sizeof(float) * 256 + sizeof(int) * (257 + 16) + 512;
+    b += sizeof(int) * (size_t)nw * 256 + sizeof(float) * 256 + sizeof(int) * (257 + nw) + 512;
     return (b + 15) & ~size_t(15);
 }
 
@@ -376,17 +587,27 @@ void launch_ref_presort(const float* data, const int32_t* idx, const int32_t* pt
     count_launch();
 }
 
-int ft_persistent_grid(size_t smem) {
-    SGR_CUDA(cudaFuncSetAttribute(ft_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+namespace {
+template <int NW>
+int ft_grid_t(size_t smem) {
+    SGR_CUDA(cudaFuncSetAttribute(ft_persistent_kernel<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ft_persistent_kernel, 256, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ft_persistent_kernel<NW>, NW * 32, smem);
     if (per_sm < 1) per_sm = 1;
     return device_sm_count() * per_sm;
 }
+}  // namespace
 
-void launch_ft_persistent(const FtPersistentArgs& a, int grid, size_t smem, cudaStream_t s) {
-    SGR_CUDA(cudaFuncSetAttribute(ft_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    ft_persistent_kernel<<<grid, 256, smem, s>>>(a);
+int ft_persistent_grid(size_t smem, int nw) { return nw == 32 ? ft_grid_t<32>(smem) : ft_grid_t<8>(smem); }
+
+void launch_ft_persistent(const FtPersistentArgs& a, int grid, size_t smem, int nw, cudaStream_t s) {
+    if (nw == 32) {
+        SGR_CUDA(cudaFuncSetAttribute(ft_persistent_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ft_persistent_kernel<32><<<grid, 1024, smem, s>>>(a);
+    } else {
+        SGR_CUDA(cudaFuncSetAttribute(ft_persistent_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ft_persistent_kernel<8><<<grid, 256, smem, s>>>(a);
+    }
     SGR_LAUNCH_CHECK();
     count_launch();
 }

@@ -154,6 +154,8 @@ struct FtPersistentArgs {
     const uint8_t* flags;         // Q x L first-round candidate flags
     float p, thre;
     int times;
+    const int32_t* cell_list;     // cells to fine-tune (nullptr: all Q cells)
+    const int* n_list;            // device count of cell_list (read by the kernel)
     int* next_cell;               // work-queue counter (zeroed before launch)
     int32_t* final_labels;
     int32_t* rounds;
@@ -163,9 +165,34 @@ struct FtPersistentArgs {
     int* status;
 };
 
-size_t ft_persistent_smem(int Wt, int capq);
-int ft_persistent_grid(size_t smem);
-void launch_ft_persistent(const FtPersistentArgs& a, int grid, size_t smem, cudaStream_t s);
+// Split path for heavy cells: state arrays of H cells (device), one round per launch_split_round.
+struct FtSplit {
+    const int32_t* cells;   // H query cells
+    uint8_t* top;           // H x 256 candidate lists
+    int* ntop;              // H
+    int* rounds;            // H
+    int* times;             // H
+    int* state;             // H: 0 not started, 1 active, 2 finished
+    int* nS;                // H
+    int* kq;                // H
+    int64_t* nq;            // H
+    double* rq;             // H
+    int* total;             // H: candidate reference rows of this round (0 when no scan)
+    int* off;               // H x 257 label offsets
+    int* eqv;               // H x Wt query e-values
+    float* scores;          // H x max_rcand
+    float* nan_scratch;     // H x 8 x max_label
+    int max_rcand;
+};
+
+void launch_split_round(const FtPersistentArgs& a, const FtSplit& sp, int H, int max_chunks, cudaStream_t s);
+
+size_t ft_persistent_smem(int Wt, int capq, int nw);
+void launch_ft_keys(int n, const int32_t* list, int L, const uint8_t* flags, const uint32_t* ctidx, int64_t* keys,
+                    int32_t* ncand, cudaStream_t s);
+// nw: warps per CTA (8 or 32)
+int ft_persistent_grid(size_t smem, int nw);
+void launch_ft_persistent(const FtPersistentArgs& a, int grid, size_t smem, int nw, cudaStream_t s);
 void launch_ref_presort(const float* data, const int32_t* idx, const int32_t* ptr, uint32_t n_rows, int cap,
                         uint32_t* out, cudaStream_t s);
 

@@ -122,11 +122,74 @@ typedef struct sgr_timings {
     uint64_t corr_ops;      /* algorithmic ops 2*Q*R*G of the score-step correlation             */
     uint64_t cells;         /* query cells annotated                                             */
     uint64_t ft_cell_rounds;/* fine-tune (cell, round) pairs                                     */
+    double mlp_ms;          /* learned form: features, proposal network, routing                 */
+    uint64_t select_launches;
+    uint64_t select_bytes;  /* algorithmic bytes 4*Q*R read by the score-step selection          */
 } sgr_timings;
 
 sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
+
+/* Launch-shape choices.  what 0: warps per CTA of the persistent fine-tune kernel (8 or 32);
+ * what 1: candidate count from which a cell's fine-tune rounds are spread over the whole GPU
+ * instead of one CTA (>= 2; large values disable the split path). */
+sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value);
 sgr_status sgr_reset_timings(sgr_ctx* ctx);
 sgr_status sgr_get_timings(const sgr_ctx* ctx, sgr_timings* out);
+
+/* ---- Learned proposal ------------------------------------------------------------------------ */
+
+/* These entry points have no counterpart in the reference.  A small network (first-round
+ * per-label scores minus their maximum -> 256 -> GELU -> 256 -> GELU -> labels, BF16 working weights,
+ * FP32 master weights and accumulation, trained by the library's own CUDA kernels with AdamW)
+ * proposes each cell's final label, so that confident cells can skip the fine-tune loop.  Its
+ * inputs are (score - the cell's best score) / 0.05, clipped below at -8. */
+typedef struct sgr_mlp_config {
+    uint32_t hidden;        /* width of both hidden layers (default 256 when 0)        */
+    uint32_t epochs;        /* passes over the training rows (default 20 when 0)       */
+    uint32_t batch;         /* rows per step (default 4096 when 0)                     */
+    float lr;               /* AdamW step size, e.g. 1e-3                              */
+    float weight_decay;     /* decoupled weight decay on the weight matrices           */
+    float beta1, beta2, eps;
+    uint64_t seed;          /* initialisation and shuffling                            */
+} sgr_mlp_config;
+
+typedef struct sgr_learned_stats {
+    uint64_t cells;         /* query cells                                              */
+    uint64_t decided;       /* final label decided without fine-tune (0 or 1 candidate,
+                               or a confident proposal)                                 */
+    uint64_t finetuned;     /* cells that ran the plain fine-tune                      */
+    uint64_t checked;       /* confident proposals re-run plain to measure agreement   */
+    uint64_t check_agree;   /* ... of which the plain final label equals the proposal  */
+} sgr_learned_stats;
+
+/* Trains the proposal network on n rows of first-round label scores (host, n x n_labels, as
+ * sgr_score_first returns them) and their plain-method final labels.  Rows holding NaN are skipped.
+ * final_loss (may be NULL) receives the mean cross-entropy of the last step. */
+sgr_status sgr_mlp_train(sgr_ctx* ctx, const float* label_scores, const int32_t* targets, uint32_t n,
+                         const sgr_mlp_config* cfg, float* final_loss);
+
+/* Proposed label and its softmax probability for n rows of label scores (host arrays). */
+sgr_status sgr_mlp_predict(sgr_ctx* ctx, const float* label_scores, uint32_t n, int32_t* labels,
+                           float* confidence);
+
+/* Copies the FP32 parameters (layout W1[H][L], b1[H], W2[H][H], b2[H], W3[L][H], b3[L]) into `out`
+ * (capacity `cap` floats, may be NULL to query sizes); sgr_mlp_load installs such a vector. */
+sgr_status sgr_mlp_params(sgr_ctx* ctx, float* out, uint64_t cap, uint32_t* n_labels, uint32_t* hidden,
+                          uint64_t* n_params);
+sgr_status sgr_mlp_load(sgr_ctx* ctx, const float* params, uint32_t n_labels, uint32_t hidden);
+
+/* One forward and backward pass (no update) on n rows of features (host, n x n_labels, already
+ * centred) and targets: the mean loss and the flat gradient (same layout as the parameters). */
+sgr_status sgr_mlp_debug_grads(sgr_ctx* ctx, const float* features, const int32_t* targets, uint32_t n,
+                               float* grads, float* loss);
+
+/* The learned form of sgr_annotate: score step, proposal, then the plain fine-tune only for cells
+ * whose proposal is below `min_confidence`, is not one of their candidates, or whose scores hold
+ * NaN; a `check_fraction` sample of the confident cells is re-run plain as well (their plain result
+ * is returned) and counted in stats. */
+sgr_status sgr_annotate_learned(sgr_ctx* ctx, const sgr_csr* qry, float quantile, float finetune_thre,
+                                int32_t finetune_times, float min_confidence, float check_fraction,
+                                int32_t* first_labels, int32_t* final_labels, sgr_learned_stats* stats);
 
 /* ---- Allocation-free selection -------------------------------------------------------------- */
 
