@@ -120,6 +120,7 @@ struct sgr_ctx {
     DevBuf<int> next_cell;
     int ft_warps = 8;            // warps per CTA of the persistent fine-tune (8 or 32)
     int ft_heavy = 6;            // candidates from which a cell takes the split path
+    size_t score_chunk_bytes = (size_t)1 << 30;  // score-step correlation block (queries x reference)
     DevBuf<int64_t> ft_keys;
     DevBuf<int32_t> ft_ncand;
     // split path state
@@ -177,8 +178,6 @@ struct sgr_ctx {
 };
 
 namespace {
-
-constexpr int kScoreChunkBytes = 1 << 30;  // score-step correlation block (queries x reference)
 
 int pow2_at_least(int v) {
     int n = 1;
@@ -518,7 +517,8 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
     ctx->label_scores.ensure((size_t)Q * L);
     ctx->first.ensure(Q);
     ctx->flags.ensure((size_t)Q * L);
-    const uint32_t chunk = (uint32_t)std::max<size_t>(1, std::min<size_t>(Q, kScoreChunkBytes / (4 * (size_t)R)));
+    const uint32_t chunk =
+        (uint32_t)std::max<size_t>(1, std::min<size_t>(Q, ctx->score_chunk_bytes / (4 * (size_t)R)));
     ctx->scores.ensure((size_t)chunk * R);
     for (uint32_t q0 = 0; q0 < Q; q0 += chunk) {
         const int nq = (int)std::min(chunk, Q - q0);
@@ -1030,6 +1030,11 @@ sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value) {
     if (what == 1) {
         if (value < 2) return SGR_ERR_INVALID_ARGUMENT;
         ctx->ft_heavy = value;
+        return SGR_OK;
+    }
+    if (what == 2) {
+        if (value < 1) return SGR_ERR_INVALID_ARGUMENT;
+        ctx->score_chunk_bytes = (size_t)value << 20;
         return SGR_OK;
     }
     return SGR_ERR_INVALID_ARGUMENT;

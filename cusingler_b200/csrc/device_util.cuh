@@ -94,9 +94,16 @@ __device__ __forceinline__ int warp_incl_scan(int x, int lane) {
 }
 
 // Key of the j-th smallest (0-based) of v[0..n) by 4 passes of an 8-bit radix histogram.
-__device__ uint32_t warp_select(const float* v, int n, int j, int* hist, int lane) {
-    uint32_t prefix = 0, mask = 0;
-    for (int shift = 24; shift >= 0; shift -= 8) {
+// `common` high bits are shared by every key (from the list's minimum and maximum): the radix
+// passes start below them.
+__device__ uint32_t warp_select(const float* v, int n, int j, int* hist, int lane, uint32_t kmin = 0,
+                                int common = 0) {
+    uint32_t mask = common ? ~0u << (32 - common) : 0u;
+    uint32_t prefix = kmin & mask;
+    const int low = 32 - common;  // bits still to resolve
+    int shift = low - 8;
+    for (;; shift -= 8) {
+        if (shift < 0) shift = 0;
         for (int b = lane; b < 256; b += 32) hist[b] = 0;
         __syncwarp();
         for (int i = lane; i < n; i += 32) {
@@ -132,12 +139,103 @@ __device__ uint32_t warp_select(const float* v, int n, int j, int* hist, int lan
         prefix |= (uint32_t)bin << shift;
         mask |= 0xffu << shift;
         __syncwarp();
+        if (shift == 0) break;
     }
     return prefix;
 }
 
 __device__ __forceinline__ uint32_t warp_min_u32(uint32_t x) { return __reduce_min_sync(FULL, x); }
 __device__ __forceinline__ uint32_t warp_max_u32(uint32_t x) { return __reduce_max_sync(FULL, x); }
+
+// Keys of order statistics j and j+1 (0-based) of v[0..n) (no NaN, kmin < kmax) by one warp: a
+// 256-bin histogram over a monotone linear map of [min, max] locates the bin holding statistic j;
+// that bin's keys (at most 256) are compacted into `buf` (the histogram's memory) and sorted.
+// Returns false (nothing decided) when the bin is larger than 256 or the range is degenerate.
+__device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane, uint32_t kmin, uint32_t kmax,
+                              uint32_t* ka, uint32_t* kb) {
+    const float fmin = key_float(kmin), fmax = key_float(kmax);
+    const float span = fmax - fmin;
+    if (!(span > 1e-30f) || !(span < 1e30f)) return false;
+    const float scale = 256.0f / span;
+    auto bin_of = [&](float x) { return min(255, (int)((x - fmin) * scale)); };
+    for (int b = lane; b < 256; b += 32) hist[b] = 0;
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) atomicAdd(&hist[bin_of(v[i])], 1);
+    __syncwarp();
+    int c[8], s = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        c[t] = hist[8 * lane + t];
+        s += c[t];
+    }
+    const int incl = warp_incl_scan(s, lane), excl = incl - s;
+    const unsigned own = __ballot_sync(FULL, excl <= j && j < incl);
+    const int src = __ffs(own) - 1;
+    int bin = 0, before = 0, cnt = 0;
+    if (lane == src) {
+        int acc = excl;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            if (j < acc + c[t]) {
+                bin = 8 * lane + t;
+                before = acc;
+                cnt = c[t];
+                break;
+            }
+            acc += c[t];
+        }
+    }
+    bin = __shfl_sync(FULL, bin, src);
+    before = __shfl_sync(FULL, before, src);
+    cnt = __shfl_sync(FULL, cnt, src);
+    if (cnt > 256) return false;
+    __syncwarp();
+    uint32_t* buf = reinterpret_cast<uint32_t*>(hist);
+    int w = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int i = base + lane;
+        bool in = false;
+        uint32_t u = 0;
+        if (i < n) {
+            const float x = v[i];
+            in = bin_of(x) == bin;
+            u = ord_key(x);
+        }
+        const unsigned m = __ballot_sync(FULL, in);
+        if (in) buf[w + __popc(m & ((1u << lane) - 1u))] = u;
+        w += __popc(m);
+    }
+    int np = 1;
+    while (np < cnt) np <<= 1;
+    for (int i = cnt + lane; i < np; i += 32) buf[i] = 0xffffffffu;
+    __syncwarp();
+    for (int size = 2; size <= np; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = lane; t < (np >> 1); t += 32) {
+                const int a = 2 * t - (t & (stride - 1)), b = a + stride;
+                const uint32_t x = buf[a], y = buf[b];
+                if ((x > y) == ((a & size) == 0)) {
+                    buf[a] = y;
+                    buf[b] = x;
+                }
+            }
+            __syncwarp();
+        }
+    const int r = j - before;
+    *ka = buf[r];
+    if (r + 1 < cnt) {
+        *kb = buf[r + 1];
+    } else {
+        uint32_t nxt = 0xffffffffu;
+        for (int i = lane; i < n; i += 32) {
+            const uint32_t u = ord_key(v[i]);
+            if (u > *ka) nxt = min(nxt, u);
+        }
+        *kb = __reduce_min_sync(FULL, nxt);
+    }
+    __syncwarp();
+    return true;
+}
 
 // The reference's percentile(v, n, p) (src/cusingler.cu:947-978) for one score list, by one warp.
 // Lists holding NaN are sorted exactly as libstdc++ would, in `scratch` (n floats), by lane 0.
@@ -146,8 +244,17 @@ __device__ float quantile_warp(const float* v, const LabelQ& lq, float p, int* h
     const int n = lq.len;
     if (lq.kind == 0) return v[0];
     bool nan = false;
-    for (int i = lane; i < n; i += 32) nan |= (v[i] != v[i]);
+    uint32_t kmin = 0xffffffffu, kmax = 0u;
+    for (int i = lane; i < n; i += 32) {
+        const float x = v[i];
+        nan |= x != x;
+        const uint32_t u = ord_key(x);
+        kmin = min(kmin, u);
+        kmax = max(kmax, u);
+    }
     nan = __any_sync(FULL, nan);
+    kmin = __reduce_min_sync(FULL, kmin);
+    kmax = __reduce_max_sync(FULL, kmax);
     if (nan) {
         float r = 0.f;
         if (scratch == nullptr) {
@@ -167,16 +274,13 @@ __device__ float quantile_warp(const float* v, const LabelQ& lq, float p, int* h
         __syncwarp();
         return __shfl_sync(FULL, r, 0);
     }
-    if (lq.kind == 1 || lq.kind == 2) {
-        uint32_t m = lq.kind == 1 ? 0xffffffffu : 0u;
-        for (int i = lane; i < n; i += 32) {
-            const uint32_t u = ord_key(v[i]);
-            m = lq.kind == 1 ? min(m, u) : max(m, u);
-        }
-        m = lq.kind == 1 ? warp_min_u32(m) : warp_max_u32(m);
-        return key_float(m);
-    }
-    const uint32_t ka = warp_select(v, n, lq.k - 1, hist, lane);
+    if (lq.kind == 1) return key_float(kmin);
+    if (lq.kind == 2) return key_float(kmax);
+    if (kmin == kmax) return interp(p, lq.prev_index, lq.step, key_float(kmin), key_float(kmin));
+    uint32_t ka, kb;
+    if (bucket_select(v, n, lq.k - 1, hist, lane, kmin, kmax, &ka, &kb))
+        return interp(p, lq.prev_index, lq.step, key_float(ka), key_float(kb));
+    ka = warp_select(v, n, lq.k - 1, hist, lane);
     int le = 0;
     uint32_t nxt = 0xffffffffu;
     for (int i = lane; i < n; i += 32) {
@@ -186,7 +290,7 @@ __device__ float quantile_warp(const float* v, const LabelQ& lq, float p, int* h
     }
     le = __reduce_add_sync(FULL, le);
     nxt = warp_min_u32(nxt);
-    const uint32_t kb = le > lq.k ? ka : nxt;
+    kb = le > lq.k ? ka : nxt;
     return interp(p, lq.prev_index, lq.step, key_float(ka), key_float(kb));
 }
 
