@@ -118,6 +118,8 @@ struct sgr_ctx {
     DevBuf<int32_t> d_gene_thre;
     DevBuf<LabelQ> d_lq_label;
     DevBuf<int> next_cell;
+    DevBuf<RankItem> rank_overflow;  // rows ranked by the rank kernel's large-buffer tier
+    DevBuf<int> rank_n_overflow;
     int ft_warps = 8;            // warps per CTA of the persistent fine-tune (8 or 32)
     int ft_heavy = 6;            // candidates from which a cell takes the split path
     size_t score_chunk_bytes = (size_t)1 << 30;  // score-step correlation block (queries x reference)
@@ -357,6 +359,8 @@ void rank_rows(sgr_ctx* ctx, const DevCsr& m, const RankGroup& grp, int out_mode
     a.max_Kp = grp.Kp;
     a.cap = sort_cap(grp.G);
     a.status = ctx->status.p;
+    a.overflow = ctx->rank_overflow.ensure(std::max<uint32_t>(m.n_rows, 1));
+    a.n_overflow = ctx->rank_n_overflow.ensure(1);
     launch_rank(a, ctx->stream);
 }
 

@@ -52,7 +52,8 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     uint64_t* keys = reinterpret_cast<uint64_t*>(smem + (size_t)warp * warp_bytes);
     unsigned char* stage = reinterpret_cast<unsigned char*>(keys + a.cap);
-    for (uint32_t item = blockIdx.x * wpb + warp; item < a.n_items; item += gridDim.x * wpb) {
+    const uint32_t n_items = a.n_items_dev ? (uint32_t)*a.n_items_dev : a.n_items;
+    for (uint32_t item = blockIdx.x * wpb + warp; item < n_items; item += gridDim.x * wpb) {
         RankItem it;
         if (a.items) {
             it = a.items[item];
@@ -65,38 +66,42 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
         const int G = g.G, Kp = g.Kp;
         const int beg = a.indptr[it.row], end = a.indptr[it.row + 1];
 
-        // 1) compact the row's entries in the gene subset into (value key, position) sort keys
+        // 1) compact the row's entries in the gene subset into (value key, position) sort keys;
+        //    four chunks of 32 entries per step, their loads issued before any is used
         int k = 0, bad = 0;
-        for (int base = beg; base < end; base += 32) {
-            const int i = base + lane;
-            bool hit = false;
-            uint64_t key = 0;
-            if (i < end) {
-                const int c = __ldg(a.indices + i);
-                if ((unsigned)c >= a.n_cols) {
-                    bad |= 1;
-                } else {
-                    const int pos = __ldg(g.colmap + c);
-                    if (pos >= 0) {
-                        float v = __ldg(a.data + i);
-                        if (v != v) bad |= 2;
-                        v = canon_zero(v);
-                        hit = true;
-                        key = ((uint64_t)ord_key(v) << 32) | (uint32_t)pos;
-                    }
+        for (int base = beg; base < end; base += 128) {
+            int c[4], pos[4];
+            float v[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const int i = base + 32 * t + lane;
+                c[t] = i < end ? __ldg(a.indices + i) : -1;
+                bad |= (i < end && (unsigned)c[t] >= a.n_cols) ? 1 : 0;
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t) pos[t] = (unsigned)c[t] < a.n_cols ? __ldg(g.colmap + c[t]) : -1;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) v[t] = pos[t] >= 0 ? __ldg(a.data + base + 32 * t + lane) : 0.f;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const bool hit = pos[t] >= 0;
+                if (hit && v[t] != v[t]) bad |= 2;
+                const unsigned m = __ballot_sync(FULL, hit);
+                if (hit) {
+                    const int idx = k + __popc(m & ((1u << lane) - 1u));
+                    if (idx < a.cap) keys[idx] = ((uint64_t)ord_key(canon_zero(v[t])) << 32) | (uint32_t)pos[t];
                 }
+                k += __popc(m);
             }
-            const unsigned m = __ballot_sync(FULL, hit);
-            if (hit) {
-                const int idx = k + __popc(m & ((1u << lane) - 1u));
-                if (idx < a.cap) keys[idx] = key;
-            }
-            k += __popc(m);
         }
         bad = __reduce_or_sync(FULL, bad);
         if (bad && lane == 0) atomicOr(a.status, bad);
         __syncwarp();
         const bool fits = k <= a.cap;
+        if (!fits && a.overflow) {  // ranked by the second, large-buffer launch
+            if (lane == 0) a.overflow[atomicAdd(a.n_overflow, 1)] = it;
+            continue;
+        }
         if (fits && k > 1) {
             int n = 1;
             while (n < k) n <<= 1;
@@ -112,13 +117,14 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
             int h0, l0, s0;
             split_limbs(d0, h0, l0, s0);
             uint32_t* st = reinterpret_cast<uint32_t*>(stage);
-            for (int w = lane; w < 3 * Kp / 4; w += 32) {
-                const int plane = (4 * w) / Kp, pos = (4 * w) % Kp;
-                const uint32_t fb = (uint8_t)(int8_t)(plane == 0 ? h0 : plane == 1 ? l0 : s0);
-                uint32_t word = 0;
-                for (int b = 0; b < 4; ++b)
-                    if (pos + b < G) word |= fb << (8 * b);
-                st[w] = word;
+            const int wpp = Kp / 4;  // words per plane (Kp is a multiple of 16)
+#pragma unroll
+            for (int plane = 0; plane < 3; ++plane) {
+                const uint32_t full = (uint32_t)(uint8_t)(int8_t)(plane == 0 ? h0 : plane == 1 ? l0 : s0) * 0x01010101u;
+                for (int w = lane; w < wpp; w += 32) {
+                    const int left = G - 4 * w;  // subset positions in this word
+                    st[plane * wpp + w] = left >= 4 ? full : left <= 0 ? 0u : full & ((1u << (8 * left)) - 1u);
+                }
             }
         } else {
             int16_t* st = reinterpret_cast<int16_t*>(stage);
@@ -498,8 +504,8 @@ namespace {
 int sm_count() { return device_sm_count(); }
 }  // namespace
 
-void launch_rank(const RankLaunch& a, cudaStream_t s) {
-    if (a.n_items == 0) return;
+namespace {
+void launch_rank_tier(const RankLaunch& a, long max_blocks, cudaStream_t s) {
     const int stage_bytes = a.out_mode == RANK_LIMBS ? 3 * a.max_Kp : 2 * a.max_Kp;
     const int warp_bytes = ((a.cap * 8 + stage_bytes) + 15) & ~15;
     const int budget = 200 * 1024;
@@ -509,11 +515,32 @@ void launch_rank(const RankLaunch& a, cudaStream_t s) {
     const int smem = wpb * warp_bytes;
     SGR_CUDA(cudaFuncSetAttribute(rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int per_sm = std::max(1, std::min(8, (228 * 1024) / (smem + 1024)));
-    long blocks = ((long)a.n_items + wpb - 1) / wpb;
-    blocks = std::min<long>(blocks, (long)sm_count() * per_sm * 4);
-    rank_kernel<<<(unsigned)blocks, 32 * wpb, smem, s>>>(a, warp_bytes);
+    long blocks = (long)sm_count() * per_sm;
+    if (max_blocks > 0) blocks = std::min(blocks * 4, (max_blocks + wpb - 1) / wpb);
+    rank_kernel<<<(unsigned)std::max(1L, blocks), 32 * wpb, smem, s>>>(a, warp_bytes);
     SGR_LAUNCH_CHECK();
     count_launch();
+}
+}  // namespace
+
+void launch_rank(const RankLaunch& a, cudaStream_t s) {
+    if (a.n_items == 0) return;
+    constexpr int kSmallCap = 512;
+    if (!a.overflow || a.cap <= kSmallCap) {
+        RankLaunch b = a;
+        b.overflow = nullptr;
+        launch_rank_tier(b, a.n_items, s);
+        return;
+    }
+    SGR_CUDA(cudaMemsetAsync(a.n_overflow, 0, sizeof(int), s));
+    RankLaunch small = a;
+    small.cap = kSmallCap;
+    launch_rank_tier(small, a.n_items, s);
+    RankLaunch big = a;
+    big.items = a.overflow;
+    big.n_items_dev = a.n_overflow;
+    big.overflow = nullptr;
+    launch_rank_tier(big, 0, s);  // grid sized to the device: the row count is on the device
 }
 
 void launch_filter_count(const int32_t* indptr, const int32_t* indices, uint32_t n_rows, uint32_t n_cols,

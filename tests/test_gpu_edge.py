@@ -78,6 +78,52 @@ def test_single_cell_labels_and_unsorted_columns(mode):
     _run_both(prob, mode)
 
 
+@pytest.mark.parametrize("mode", [abi.MODE_FP32REF, abi.MODE_EXACT])
+def test_dense_rows_take_the_large_sort_tier(mode):
+    """Rows with more marker entries than the rank kernel's small sort buffer (512) are ranked by
+    its second, large-buffer launch: dense rows with distinct, tied and negative values, in the
+    query and in the reference, ranked bit-exactly and annotated like the oracle (13 labels,
+    over a thousand marker genes)."""
+    ref, qry, L = H.dataset("small")
+    rng = np.random.default_rng(7)
+
+    def rows_of(m, n):
+        return [list(zip(m.indices[m.indptr[i]:m.indptr[i + 1]], m.data[m.indptr[i]:m.indptr[i + 1]]))
+                for i in range(n)]
+
+    def dense(n_cols, kind):
+        if kind == 0:    # distinct values
+            v = rng.permutation(n_cols).astype(np.float32) + 0.5
+        elif kind == 1:  # few distinct values: long tie runs
+            v = rng.integers(1, 6, n_cols).astype(np.float32)
+        else:            # mixed signs with some stored zeros
+            v = np.round(rng.normal(0, 2, n_cols), 1).astype(np.float32)
+        return list(zip(range(n_cols), v))
+
+    rows_q = rows_of(qry, 64)
+    for i, kind in ((2, 0), (9, 1), (17, 2), (30, 0)):
+        rows_q[i] = dense(qry.n_cols, kind)
+    rows_r = rows_of(ref, ref.n_rows)
+    for i, kind in ((4, 0), (120, 1), (333, 2)):
+        rows_r[i] = dense(ref.n_cols, kind)
+    q = _csr_from_rows(rows_q, qry.n_cols)
+    r = _csr_from_rows(rows_r, ref.n_cols)
+    prob = O.Problem(r, q, synth.names("CT", L), ref.labels, synth.names("G", ref.n_cols),
+                     synth.names("G", qry.n_cols))
+    _run_both(prob, mode)
+    a = abi.Annotator(gpuid=0, mode=mode)
+    a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
+    assert len(a.u32(0)) > 512
+    orc = O.Oracle(prob)
+    orc.train()
+    d_qry = a.debug_ranks(prob.qry)
+    d_ref = a.debug_ranks()
+    for i in range(q.n_rows):
+        assert np.array_equal(d_qry[i], orc.rank_row(1, i)), i
+    for i in (3, 4, 5, 119, 120, 333):
+        assert np.array_equal(d_ref[i], orc.rank_row(0, i)), i
+
+
 def test_gene_intersection():
     ref, qry, L = H.dataset("tiny")
     rg = synth.names("G", ref.n_cols)
