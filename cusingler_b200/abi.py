@@ -49,7 +49,8 @@ class SgrTimings(C.Structure):
                 ("launches", C.c_uint64), ("corr_launches", C.c_uint64), ("rank_launches", C.c_uint64),
                 ("rank_bytes", C.c_uint64), ("corr_ops", C.c_uint64), ("cells", C.c_uint64),
                 ("ft_cell_rounds", C.c_uint64), ("mlp_ms", C.c_double), ("select_launches", C.c_uint64),
-                ("select_bytes", C.c_uint64)]
+                ("select_bytes", C.c_uint64), ("ft_queue_cells", C.c_uint64), ("ft_split_cells", C.c_uint64),
+                ("ft_split_rounds", C.c_uint64), ("ft_split_rows", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

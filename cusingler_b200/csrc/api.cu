@@ -113,6 +113,7 @@ struct sgr_ctx {
     std::vector<int64_t> h_ref_n2;
     DevBuf<float> reff_data;
     DevBuf<int32_t> reff_indices, reff_indptr;
+    DevBuf<int32_t> reff_ptr4;     // padded row offsets of ref_sorted
     DevBuf<uint32_t> ref_sorted;       // thre-pool entries of each reference row, by value
     DevBuf<uint32_t> d_ctidx, d_ft_genes, d_ft_idx;
     DevBuf<int32_t> d_gene_thre;
@@ -449,12 +450,20 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     SGR_CUDA(cudaMemcpyAsync(ctx->h_ref_n2.data(), ctx->ref_n2.p, ctx->R * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     // fine-tune: reference compacted to the thre pool, each row's entries sorted by value
     filter_csr(ctx, rm, ctx->ref_map_thre.p, ctx->reff_data, ctx->reff_indices, ctx->reff_indptr);
-    int32_t reff_nnz = 0;
-    SGR_CUDA(cudaMemcpyAsync(&reff_nnz, ctx->reff_indptr.p + ctx->R, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    // row starts on 16-byte boundaries, lengths padded to whole vectors of four entries
+    std::vector<int32_t> fptr(ctx->R + 1), fptr4(ctx->R + 1, 0);
+    SGR_CUDA(cudaMemcpyAsync(fptr.data(), ctx->reff_indptr.p, (ctx->R + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                             s));
     SGR_CUDA(cudaStreamSynchronize(s));
-    ctx->ref_sorted.ensure((size_t)std::max<int32_t>(reff_nnz, 1) + 4);  // + one 16-byte vector of slack
-    launch_ref_presort(ctx->reff_data.p, ctx->reff_indices.p, ctx->reff_indptr.p, ctx->R,
-                       std::min(pow2_at_least(std::max<int>(ctx->Wt, 32)), 8192), ctx->ref_sorted.p, s);
+    for (uint32_t r = 0; r < ctx->R; ++r) {
+        const int64_t next = (int64_t)fptr4[r] + ((fptr[r + 1] - fptr[r] + 3) & ~3);
+        if (next > INT32_MAX) fail(SGR_ERR_UNSUPPORTED, "fine-tune reference lists exceed 2^31 entries");
+        fptr4[r + 1] = (int32_t)next;
+    }
+    ctx->reff_ptr4.upload(fptr4, s);
+    ctx->ref_sorted.ensure((size_t)std::max<int32_t>(fptr4[ctx->R], 4));
+    launch_ref_presort(ctx->reff_data.p, ctx->reff_indices.p, ctx->reff_indptr.p, ctx->reff_ptr4.p, ctx->R,
+                       std::min(pow2_at_least(std::max<int>(ctx->Wt, 32)), 8192), ctx->Wt, ctx->ref_sorted.p, s);
     ctx->d_ctidx.upload(mk.ctidx, s);
     ctx->d_ft_genes.upload(mk.ft_genes.empty() ? std::vector<uint32_t>{0} : mk.ft_genes, s);
     ctx->d_ft_idx.upload(mk.ft_idx, s);
@@ -857,7 +866,7 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     ctx->d_rounds.ensure(Q);
     FtPersistentArgs a{};
     a.ref_sorted = ctx->ref_sorted.p;
-    a.ref_ptr = ctx->reff_indptr.p;
+    a.ref_ptr = ctx->reff_ptr4.p;
     a.ctidx = ctx->d_ctidx.p;
     a.ft_genes = ctx->d_ft_genes.p;
     a.ft_idx = ctx->d_ft_idx.p;
@@ -905,6 +914,8 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
             else order.push_back(c);
         }
         int n_order = (int)order.size();
+        ctx->prof.acc.ft_queue_cells += (uint64_t)n_order;
+        ctx->prof.acc.ft_split_cells += heavy.size();
         ctx->ft_order.upload(order.empty() ? std::vector<int32_t>{0} : order, s);
         ctx->ft_order_n.upload(&n_order, 1, s);
         cell_list = ctx->ft_order.p;
@@ -946,15 +957,20 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
                    ctx->sp_state.p, ctx->sp_nS.p, ctx->sp_kq.p, ctx->sp_nq.p, ctx->sp_rq.p, ctx->sp_total.p,
                    ctx->sp_off.p, ctx->sp_eqv.p, ctx->sp_scores.p, ctx->sp_nan.p, (int)ctx->R};
         const int max_chunks = (int)((ctx->R + 255) / 256);
-        std::vector<int> state(H);
+        std::vector<int> state(H), total(H);
         // each round drops at least one candidate, so L + 2 rounds finish every cell
         for (uint32_t round = 0;; ++round) {
             if (round > L + 3) fail(SGR_ERR_STATE, "fine-tune split path did not converge");
             launch_split_round(a, sp, H, max_chunks, s);
             SGR_CUDA(cudaMemcpyAsync(state.data(), ctx->sp_state.p, H * sizeof(int), cudaMemcpyDeviceToHost, s));
+            SGR_CUDA(cudaMemcpyAsync(total.data(), ctx->sp_total.p, H * sizeof(int), cudaMemcpyDeviceToHost, s));
             SGR_CUDA(cudaStreamSynchronize(s));
+            ctx->prof.acc.ft_split_rounds++;
             bool all = true;
-            for (int v : state) all &= v == 2;
+            for (int i = 0; i < H; ++i) {
+                all &= state[i] == 2;
+                ctx->prof.acc.ft_split_rows += (uint64_t)total[i];
+            }
             if (all) break;
         }
     }

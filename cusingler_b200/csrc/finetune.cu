@@ -12,14 +12,17 @@
 // Step 3 never builds a dense rank row.  With d = 2*rank - (|S|+1) and e = d + k (k = stored
 // entries of the row inside S), e is 0 at every implicit zero, so
 //     sum_g d_q d_r = sum_{g stored in both} e_q e_r - |S| k_q k_r.
-// Each reference row's thre-pool entries are sorted by value once (ref_presort_kernel), each with
-// the position where its run of equal values starts.  For any S, one pass over the row keeping the
-// entries inside S yields every kept entry's rank: a run of b kept entries with a kept entries
-// before it gives each of them 2 #less + #equal = z = 2a + b.  The pass accumulates
-// X = sum z s, Y = sum s (s = the query's e summed over the run's genes), Z1 = sum b z,
-// Z2 = sum b z^2, and then, exactly in int64,
+// Each reference row's thre-pool entries are sorted by value once (ref_presort_kernel), the last
+// entry of each run of equal values flagged.  For any S, one pass over the row keeping the entries
+// inside S yields every kept entry's rank: a run of b kept entries with a kept entries before it
+// gives each of them 2 #less + #equal = z = 2a + b.  The pass accumulates per run
+// X = sum z s, Y = sum s (s = the query's e summed over the run's genes) and T = sum (b^3 - b);
+// the other two sums are closed forms of k_r, the kept count: Z1 = sum b z = k_r^2 (the z of a run
+// average the odd numbers 2i + 1 it covers) and Z2 = sum b z^2 = ((4 k_r^3 - k_r) - T) / 3 (sum of
+// (2i + 1)^2 minus each run's tie spread).  Then, exactly in int64,
 //     N   = X + (|S| - k_r) Y - |S| k_q k_r
 //     n_r = Z2 + 2 c Z1 + k_r c^2 + (|S| - k_r) k_r^2,   c = |S| - 2 k_r.
+// Rows are padded to whole 16-byte vectors with entries of gene id Wt, whose e-value is SENT.
 // The score is float((N * (1/sqrt(n_q))) * (1/sqrt(n_r))) in FP64, the same
 // formula as the score step's exact mode.
 
@@ -38,15 +41,20 @@ namespace {
 constexpr int SENT = INT32_MIN;  // "gene not in S"
 
 // One warp per reference row: its thre-pool entries sorted by (value, gene), each packed as
-// gene | run_start << 16, where run_start is the row position of the first entry with the same
-// value.
+// gene | last << 31, where last marks the final entry of a run of equal values.  Row r is written at
+// ptr4[r] and padded to ptr4[r + 1] (a multiple of 4 entries) with pad_gene | 1 << 31.
 __global__ void __launch_bounds__(256) ref_presort_kernel(const float* data, const int32_t* idx, const int32_t* ptr,
-                                                          uint32_t n_rows, int cap, uint32_t* out) {
+                                                          const int32_t* ptr4, uint32_t n_rows, int cap,
+                                                          uint32_t pad_gene, uint32_t* out) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     uint64_t* keys = reinterpret_cast<uint64_t*>(smem) + (size_t)warp * cap;
+    constexpr uint32_t LAST = 0x80000000u;
     for (uint32_t row = blockIdx.x * wpb + warp; row < n_rows; row += gridDim.x * wpb) {
         const int beg = ptr[row], k = ptr[row + 1] - beg;
+        uint32_t* o = out + ptr4[row];
+        const int k4 = ptr4[row + 1] - ptr4[row];
+        for (int j = k + lane; j < k4; j += 32) o[j] = pad_gene | LAST;
         if (k <= cap) {
             int n = 1;
             while (n < k) n <<= 1;
@@ -56,24 +64,24 @@ __global__ void __launch_bounds__(256) ref_presort_kernel(const float* data, con
             __syncwarp();
             if (k > 1) warp_bitonic(keys, n, lane);
             for (int j = lane; j < k; j += 32) {
-                const uint32_t hv = (uint32_t)(keys[j] >> 32);
-                const uint32_t rs = (uint32_t)lower_hi(keys, k, hv);
-                out[beg + j] = (uint32_t)(keys[j] & 0xffffu) | (rs << 16);
+                const uint64_t key = keys[j];
+                const bool last = j + 1 == k || (uint32_t)(keys[j + 1] >> 32) != (uint32_t)(key >> 32);
+                o[j] = (uint32_t)(key & 0xffffu) | (last ? LAST : 0u);
             }
             __syncwarp();
         } else {
-            // rows longer than the sort buffer: position and run bounds by counting
+            // rows longer than the sort buffer: position and run end by counting
             for (int i = lane; i < k; i += 32) {
                 const float v = canon_zero(data[beg + i]);
                 const int g = idx[beg + i];
-                int pos = 0, rs = 0;
+                int pos = 0, eq_after = 0;
                 for (int j = 0; j < k; ++j) {
                     const float w = canon_zero(data[beg + j]);
                     const int h = idx[beg + j];
                     pos += (w < v) || (w == v && h < g);
-                    rs += w < v;
+                    eq_after += w == v && h > g;
                 }
-                out[beg + pos] = (uint32_t)g | ((uint32_t)rs << 16);
+                o[pos] = (uint32_t)g | (eq_after == 0 ? LAST : 0u);
             }
         }
     }
@@ -158,6 +166,7 @@ __device__ void cta_query_ranks(const FtPersistentArgs& a, int cell, int nS, con
                                 uint64_t* qkeys, int* kq_out, int64_t* nq_out, double* rq_out) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int g = tid; g < a.Wt; g += NW * 32) eqv[g] = (bits[g >> 5] >> (g & 31)) & 1u ? 0 : SENT;
+    if (tid == 0) eqv[a.Wt] = SENT;  // the pad entries' gene id
     __syncthreads();
     if (warp == 0) {
         const int beg = a.qf_ptr[cell], end = a.qf_ptr[cell + 1];
@@ -246,53 +255,39 @@ __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const 
         else hi = mid - 1;
     }
     const int r = (int)a.ctidx[2 * top[lo]] + (f - off[lo]);
-    const int beg = a.ref_ptr[r], end = a.ref_ptr[r + 1];
-    int64_t X = 0, Y = 0, Z1 = 0, Z2 = 0;
-    int ka = 0, b = 0, sum = 0;
-    uint32_t cur = 0xffffffffu;
-    // 16-byte loads of four entries (the list base is 16-byte aligned and padded; the first and
-    // last words are masked to [beg, end)); the next load is issued before the current is used
-    uint4 nxt = __ldg(reinterpret_cast<const uint4*>(a.ref_sorted + (beg & ~3)));
-    for (int j4 = beg & ~3; j4 < end; j4 += 4) {
+    const int beg = a.ref_ptr[r], n4 = (a.ref_ptr[r + 1] - beg) >> 2;
+    const uint4* p = reinterpret_cast<const uint4*>(a.ref_sorted + beg);
+    // Per entry: b, sum of the open run; at a run's last entry (flag bit 31) the run is closed with
+    // masks instead of a branch, since some lane of the warp closes a run at almost every step.
+    // Bounds (|S| <= Wt <= 40000, e <= 2|S|): sum, Y, z * sum / z < 2^32, b^3 < 2^63.
+    uint32_t b = 0, sum = 0, ka = 0, Y = 0;
+    uint64_t X = 0, T = 0;
+    uint4 nxt = n4 > 0 ? __ldg(p) : make_uint4(0u, 0u, 0u, 0u);
+    for (int t = 0; t < n4; ++t) {
         const uint4 w4 = nxt;
-        if (j4 + 4 < end) nxt = __ldg(reinterpret_cast<const uint4*>(a.ref_sorted + j4 + 4));
+        if (t + 1 < n4) nxt = __ldg(p + t + 1);
         const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int j = j4 + u;
-            if (j < beg || j >= end) continue;
             const uint32_t ent = ws[u];
             const int v = eqv[ent & 0xffffu];
-            if (v == SENT) continue;
-            const uint32_t run = ent >> 16;
-            if (run != cur) {
-                if (b) {
-                    const int64_t z = 2 * ka + b;
-                    X += z * sum;
-                    Y += sum;
-                    Z1 += b * z;
-                    Z2 += b * z * z;
-                    ka += b;
-                }
-                b = 0;
-                sum = 0;
-                cur = run;
-            }
-            ++b;
-            sum += v;
+            b += v >= 0 ? 1u : 0u;
+            sum += (uint32_t)max(v, 0);
+            const uint32_t m = (uint32_t)((int32_t)ent >> 31);  // all ones at a run's last entry
+            const uint32_t bm = b & m, sm = sum & m;
+            X += (uint64_t)(2 * ka + bm) * sm;
+            Y += sm;
+            T += (uint64_t)bm * (bm * bm - 1u);
+            ka += bm;
+            b &= ~m;
+            sum &= ~m;
         }
     }
-    if (b) {
-        const int64_t z = 2 * ka + b;
-        X += z * sum;
-        Y += sum;
-        Z1 += b * z;
-        Z2 += b * z * z;
-        ka += b;
-    }
     const int64_t kr = ka;
-    const int64_t N = X + ((int64_t)nS - kr) * Y - (int64_t)nS * kq * kr;
+    const int64_t N = (int64_t)X + ((int64_t)nS - kr) * (int64_t)Y - (int64_t)nS * kq * kr;
     const int64_t c = (int64_t)nS - 2 * kr;
+    const int64_t Z1 = kr * kr;
+    const int64_t Z2 = (4 * kr * kr * kr - kr - (int64_t)T) / 3;
     const int64_t nr = Z2 + 2 * c * Z1 + kr * c * c + ((int64_t)nS - kr) * kr * kr;
     if (nq == 0 || nr == 0) return __int_as_float(0x7fffffff);
     return (float)(((double)N * rq) * (1.0 / sqrt((double)nr)));
@@ -348,8 +343,8 @@ __global__ void __launch_bounds__(NW * 32) ft_persistent_kernel(FtPersistentArgs
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int Wt = a.Wt, L = a.L;
     const int nwords = (Wt + 31) / 32;
-    int* eqv = reinterpret_cast<int*>(smem);                                     // Wt
-    uint32_t* bits = reinterpret_cast<uint32_t*>(eqv + ((Wt + 3) & ~3));         // nwords
+    int* eqv = reinterpret_cast<int*>(smem);                                     // Wt + 1
+    uint32_t* bits = reinterpret_cast<uint32_t*>(eqv + ((Wt + 4) & ~3));         // nwords
     uint64_t* qkeys = reinterpret_cast<uint64_t*>(bits + ((nwords + 3) & ~3));   // capq (8-byte aligned)
     int* hist = reinterpret_cast<int*>(qkeys + a.capq);                          // NW * 256
     float* lsc = reinterpret_cast<float*>(hist + NW * 256);                      // 256
@@ -426,7 +421,7 @@ __global__ void __launch_bounds__(256) split_prepare_kernel(FtPersistentArgs a, 
     const int Wt = a.Wt, L = a.L;
     const int nwords = (Wt + 31) / 32;
     int* eqv = reinterpret_cast<int*>(smem);
-    uint32_t* bits = reinterpret_cast<uint32_t*>(eqv + ((Wt + 3) & ~3));
+    uint32_t* bits = reinterpret_cast<uint32_t*>(eqv + ((Wt + 4) & ~3));
     uint64_t* qkeys = reinterpret_cast<uint64_t*>(bits + ((nwords + 3) & ~3));
     int* red = reinterpret_cast<int*>(qkeys + a.capq);
     __shared__ int s_ntop, s_go;
@@ -500,11 +495,12 @@ __global__ void __launch_bounds__(256) split_scan_kernel(FtPersistentArgs a, FtS
     const int f = blockIdx.x * 256 + threadIdx.x;
     if ((int)blockIdx.x * 256 >= total) return;
     int* eqv = reinterpret_cast<int*>(smem);
-    int* off = eqv + ((a.Wt + 3) & ~3);
+    int* off = eqv + ((a.Wt + 4) & ~3);
     uint8_t* top = reinterpret_cast<uint8_t*>(off + 260);
     const int* geqv = sp.eqv + (size_t)i * a.Wt;
     const int ntop = sp.ntop[i];
     for (int g = threadIdx.x; g < a.Wt; g += 256) eqv[g] = geqv[g];
+    if (threadIdx.x == 0) eqv[a.Wt] = SENT;
     for (int t = threadIdx.x; t <= ntop; t += 256) off[t] = sp.off[(size_t)i * 257 + t];
     for (int t = threadIdx.x; t < ntop; t += 256) top[t] = sp.top[(size_t)i * 256 + t];
     __syncthreads();
@@ -539,7 +535,7 @@ __global__ void __launch_bounds__(256) split_decide_kernel(FtPersistentArgs a, F
 
 size_t split_prepare_smem(int Wt, int capq) {
     const int nwords = (Wt + 31) / 32;
-    return sizeof(int) * ((Wt + 3) & ~3) + sizeof(uint32_t) * ((nwords + 3) & ~3) + sizeof(uint64_t) * capq +
+    return sizeof(int) * ((Wt + 4) & ~3) + sizeof(uint32_t) * ((nwords + 3) & ~3) + sizeof(uint64_t) * capq +
            sizeof(int) * 16;
 }
 
@@ -548,7 +544,7 @@ void launch_split_round(const FtPersistentArgs& a, const FtSplit& sp, int H, int
     SGR_CUDA(cudaFuncSetAttribute(split_prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
     split_prepare_kernel<<<H, 256, sm1, s>>>(a, sp);
     SGR_LAUNCH_CHECK();
-    const size_t sm2 = sizeof(int) * (((a.Wt + 3) & ~3) + 260) + 256;
+    const size_t sm2 = sizeof(int) * (((a.Wt + 4) & ~3) + 260) + 256;
     SGR_CUDA(cudaFuncSetAttribute(split_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
     split_scan_kernel<<<dim3(max_chunks, H), 256, sm2, s>>>(a, sp);
     SGR_LAUNCH_CHECK();
@@ -568,21 +564,21 @@ void launch_ft_keys(int n, const int32_t* list, int L, const uint8_t* flags, con
 size_t ft_persistent_smem(int Wt, int capq, int nw) {
     const int nwords = (Wt + 31) / 32;
     size_t b = 0;
-    b += sizeof(int) * ((Wt + 3) & ~3);
+    b += sizeof(int) * ((Wt + 4) & ~3);
     b += sizeof(uint32_t) * ((nwords + 3) & ~3);
     b += sizeof(uint64_t) * capq;
     b += sizeof(int) * (size_t)nw * 256 + sizeof(float) * 256 + sizeof(int) * (257 + nw) + 512;
     return (b + 15) & ~size_t(15);
 }
 
-void launch_ref_presort(const float* data, const int32_t* idx, const int32_t* ptr, uint32_t n_rows, int cap,
-                        uint32_t* out, cudaStream_t s) {
+void launch_ref_presort(const float* data, const int32_t* idx, const int32_t* ptr, const int32_t* ptr4,
+                        uint32_t n_rows, int cap, uint32_t pad_gene, uint32_t* out, cudaStream_t s) {
     if (!n_rows) return;
     int wpb = std::max(1, std::min(8, (200 * 1024) / (cap * 8)));
     const size_t smem = (size_t)wpb * cap * 8;
     SGR_CUDA(cudaFuncSetAttribute(ref_presort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const unsigned blocks = std::min<unsigned>((n_rows + wpb - 1) / wpb, device_sm_count() * 8);
-    ref_presort_kernel<<<blocks, 32 * wpb, smem, s>>>(data, idx, ptr, n_rows, cap, out);
+    ref_presort_kernel<<<blocks, 32 * wpb, smem, s>>>(data, idx, ptr, ptr4, n_rows, cap, pad_gene, out);
     SGR_LAUNCH_CHECK();
     count_launch();
 }

@@ -125,6 +125,10 @@ typedef struct sgr_timings {
     double mlp_ms;          /* learned form: features, proposal network, routing                 */
     uint64_t select_launches;
     uint64_t select_bytes;  /* algorithmic bytes 4*Q*R read by the score-step selection          */
+    uint64_t ft_queue_cells;/* fine-tune cells run whole by one CTA of the work-queue kernel      */
+    uint64_t ft_split_cells;/* fine-tune cells whose rounds were spread over the GPU             */
+    uint64_t ft_split_rounds;/* rounds of the spread path (each: prepare, scan, decide launches)  */
+    uint64_t ft_split_rows; /* reference rows scored by the spread path, summed over its rounds   */
 } sgr_timings;
 
 sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
