@@ -17,8 +17,10 @@
 // Structure: persistent kernel, one CTA per SM, 256 threads:
 //   warp 0      TMA producer (128 x 128-byte boxes, 128B swizzle, STAGES-deep ring)
 //   warp 1      TMEM allocator and single-thread tcgen05.mma issuer (M = 128, N = 128, K = 32)
-//   warps 4..7  epilogue: tcgen05.ld 32x32b, exact recombination, shared-memory transpose,
-//               row-contiguous float stores
+//   warps 4..11 epilogue, two warps per TMEM lane quadrant (warp % 4), one column half each:
+//               tcgen05.ld 32x32b, exact recombination, scores into a 128 x 128 staging tile in
+//               shared memory, TMEM released, then row-contiguous 16-byte stores from the staging
+//               tile, which overlap the next tile's MMAs
 // No TMA multicast is used.  Every mbarrier wait is bounded: on timeout the kernel records
 // SGR_TC_TIMEOUT in *status, drains its own TMA copies (bounded), frees TMEM and returns.
 
@@ -36,12 +38,14 @@ namespace {
 constexpr int BM = 128;
 constexpr int BN = 128;
 constexpr int BK = 128;  // bytes of K per stage (one 128-byte swizzle row)
-constexpr int STAGES = 6;
+constexpr int STAGES = 5;
 constexpr int A_BYTES = BM * BK;
 constexpr int B_BYTES = BN * BK;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int TMEM_COLS = 512;
-constexpr int EPI_STAGE_FLOATS = 32 * 33;  // per epilogue warp: 32 x 32 transpose buffer, padded
+constexpr int EPI_WARPS = 8;                // warps 4 .. 11
+constexpr int THREADS = 32 * (4 + EPI_WARPS);
+constexpr int STAGING_BYTES = BM * BN * 4;  // one score tile; 16-byte chunks XOR-swizzled by row
 constexpr long long WAIT_CYCLES = 4000000000LL;  // about 2 s at 1.9 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -126,6 +130,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         : "r"(taddr));
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+        "[%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -140,7 +153,7 @@ struct __align__(8) TcShared {
     int abort_flag;
 };
 
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(THREADS, 1)
     corr_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nq, int R,
                    int Kp, const double* __restrict__ rq, const double* __restrict__ rr,
                    const int64_t* __restrict__ nq2, const int64_t* __restrict__ nr2, float* __restrict__ out,
@@ -161,7 +174,7 @@ __global__ void __launch_bounds__(256, 1)
             mbar_init(smem_u32(&sh.empty[s]), 1);
         }
         mbar_init(smem_u32(&sh.tmem_full), 1);
-        mbar_init(smem_u32(&sh.tmem_empty), 4);
+        mbar_init(smem_u32(&sh.tmem_empty), EPI_WARPS);
         mbar_init(smem_u32(&sh.drain), 1);
         sh.abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -256,10 +269,15 @@ __global__ void __launch_bounds__(256, 1)
         }
     } else if (warp >= 4) {
         // ---- epilogue ------------------------------------------------------------------------
-        // Each lane owns one query row; a 32 x 32 chunk is transposed through shared memory so that
-        // every store instruction writes one row's 32 consecutive scores (one 128-byte line).
-        const int quarter = warp & 3;
-        float* stage = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES) + quarter * EPI_STAGE_FLOATS;
+        // Lane = tile row (32 * quarter + lane); this warp's 64 columns are scored into the staging
+        // tile, TMEM is released, and the warp then stores its 32 rows x 64 columns, 16 lanes per
+        // row.  Staging row r holds 16-byte chunk c at position c ^ (r & 7): conflict-free for both
+        // the row-per-lane writes and the row-contiguous reads.  A warp reads back only what it
+        // wrote, so the next tile may overwrite the staging rows once the warp's stores are issued.
+        const int quarter = warp & 3, half = (warp - 4) >> 2;
+        float4* staging = reinterpret_cast<float4*>(smem + STAGES * STAGE_BYTES);
+        const bool vec_store = (ld % 4) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+        const int row = 32 * quarter + lane;
         uint32_t tile_iter = 0;
         for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++tile_iter) {
             const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
@@ -272,39 +290,55 @@ __global__ void __launch_bounds__(256, 1)
                 break;
             }
             tc_fence_after();
-            const int row0 = m0 + 32 * quarter;
-            const int q = row0 + lane;
+            const int q = m0 + row;
             const double rqv = q < nq ? rq[q] : 0.0;  // NaN when the query row is constant
             const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
-            for (int c = 0; c < BN / 32; ++c) {
-                uint32_t p1[32], p2[32], p3[32];
-                tmem_ld32(lane_base + c * 32, p1);
-                tmem_ld32(lane_base + BN + c * 32, p2);
-                tmem_ld32(lane_base + 2 * BN + c * 32, p3);
+            float4* srow = staging + row * (BN / 4);
+#pragma unroll 1
+            for (int c = 0; c < 4; ++c) {
+                const int col0 = half * 64 + c * 16;
+                uint32_t p1[16], p2[16], p3[16];
+                tmem_ld16(lane_base + col0, p1);
+                tmem_ld16(lane_base + BN + col0, p2);
+                tmem_ld16(lane_base + 2 * BN + col0, p3);
                 tmem_wait_ld();
-                if (c == BN / 32 - 1) {
-                    // all of this warp's TMEM reads are done: release the accumulator
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(smem_u32(&sh.tmem_empty));
-                }
-                const int r0 = n0 + c * 32;
-                const double rrl = r0 + lane < R ? rr[r0 + lane] : 0.0;  // NaN for a constant reference row
+                const int r0 = n0 + col0;
+                const double rrl = (lane < 16 && r0 + lane < R) ? rr[r0 + lane] : 0.0;  // NaN: constant ref row
+                float v[16];
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int T = 127 * (int)p1[j] + (int)p3[j];
-                    const double N = (double)T * 128.0 - (double)(int)p2[j] * 127.0;
+                for (int j = 0; j < 16; ++j) {
+                    // |N| < 2^53: the int64 value converts to double exactly
+                    const int64_t N = 128ll * (127ll * (int)p1[j] + (int)p3[j]) - 127ll * (int)p2[j];
                     const double rrj = __shfl_sync(0xffffffffu, rrl, j);
-                    stage[lane * 33 + j] = (float)((N * rqv) * rrj);
+                    v[j] = (float)(((double)N * rqv) * rrj);
                 }
-                __syncwarp();
-                if (r0 + lane < R) {
-                    const int rows = min(32, nq - row0);
-                    float* dst = out + (size_t)row0 * ld + r0 + lane;
-                    for (int i = 0; i < rows; ++i) dst[(size_t)i * ld] = stage[i * 33 + lane];
-                }
-                __syncwarp();
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    srow[((col0 >> 2) + u) ^ (row & 7)] = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
             }
+            // all of this warp's TMEM reads are done: release its share of the accumulator
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh.tmem_empty));
+            const int sub = lane >> 4, c4 = half * 16 + (lane & 15);
+            const int col = n0 + 4 * c4;
+#pragma unroll 4
+            for (int i = 0; i < 16; ++i) {
+                const int rr_ = 32 * quarter + 2 * i + sub;
+                const int qq = m0 + rr_;
+                if (qq >= nq || col >= R) continue;
+                const float4 val = staging[rr_ * (BN / 4) + (c4 ^ (rr_ & 7))];
+                float* dst = out + (size_t)qq * ld + col;
+                if (vec_store && col + 3 < R) {
+                    *reinterpret_cast<float4*>(dst) = val;
+                } else {
+                    dst[0] = val.x;
+                    if (col + 1 < R) dst[1] = val.y;
+                    if (col + 2 < R) dst[2] = val.z;
+                    if (col + 3 < R) dst[3] = val.w;
+                }
+            }
+            __syncwarp();
         }
     }
     __syncthreads();
@@ -346,7 +380,7 @@ CUtensorMap limb_map(const int8_t* base, int rows, int Kp) {
 
 }  // namespace
 
-size_t corr_tc_smem() { return (size_t)STAGES * STAGE_BYTES + 4 * EPI_STAGE_FLOATS * sizeof(float) + 1024; }
+size_t corr_tc_smem() { return (size_t)STAGES * STAGE_BYTES + STAGING_BYTES + 1024; }
 
 void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
                     const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s) {
@@ -358,7 +392,7 @@ void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, con
     SGR_CUDA(cudaFuncSetAttribute(corr_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long tiles = (long)((nq + BM - 1) / BM) * ((R + BN - 1) / BN);
     const int grid = (int)std::min<long>(tiles, device_sm_count());
-    corr_tc_kernel<<<grid, 256, smem, s>>>(ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status);
+    corr_tc_kernel<<<grid, THREADS, smem, s>>>(ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status);
     SGR_LAUNCH_CHECK();
     count_launch();
 }
