@@ -119,6 +119,7 @@ struct sgr_ctx {
     DevBuf<int32_t> d_gene_thre;
     DevBuf<LabelQ> d_lq_label;
     DevBuf<int> next_cell;
+    DevBuf<int32_t> d_lorder;  // label ids by reference-cell count, longest first (score-step selection)
     DevBuf<RankItem> rank_overflow;  // rows ranked by the rank kernel's large-buffer tier
     DevBuf<int> rank_n_overflow;
     int ft_warps = 8;            // warps per CTA of the persistent fine-tune (8 or 32)
@@ -521,6 +522,11 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
             if (ctx->h_ref_n2[r] == 0) lq[l].has_nan = 1, any_nan_ref = true;
     }
     ctx->lq.upload(lq, s);
+    std::vector<int32_t> lorder(L);
+    for (uint32_t l = 0; l < L; ++l) lorder[l] = (int32_t)l;
+    std::stable_sort(lorder.begin(), lorder.end(),
+                     [&](int32_t x, int32_t y) { return ctx->mk.ctidx[2 * x + 1] > ctx->mk.ctidx[2 * y + 1]; });
+    ctx->d_lorder.upload(lorder, s);
     uint32_t max_len = 1;
     for (uint32_t l = 0; l < L; ++l) max_len = std::max(max_len, ctx->mk.ctidx[2 * l + 1]);
     float* scratch = nullptr;
@@ -545,7 +551,7 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
         ctx->prof.acc.select_bytes += 4ull * (uint64_t)nq * R;
         launch_select_first(ctx->scores.p, R, nq, (int)L, ctx->lq.p, p, thre, ctx->q_n2.p + q0,
                             ctx->label_scores.p + (size_t)q0 * L, ctx->first.p + q0, ctx->flags.p + (size_t)q0 * L,
-                            scratch, max_len, ctx->status.p, s);
+                            scratch, max_len, ctx->status.p, (int)R, ctx->d_lorder.p, s);
         ctx->prof.end(sp, s);
     }
     ctx->prof.acc.cells += Q;

@@ -281,6 +281,15 @@ __global__ void __launch_bounds__(THREADS, 1)
         uint32_t tile_iter = 0;
         for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++tile_iter) {
             const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+            // norms of this tile's rows and columns, loaded while the accumulator is still being computed
+            const int q = m0 + row;
+            const double rqv = q < nq ? rq[q] : 0.0;  // NaN when the query row is constant
+            double rrv[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int r = n0 + half * 64 + c * 16 + lane;
+                rrv[c] = (lane < 16 && r < R) ? rr[r] : 0.0;  // NaN for a constant reference row
+            }
             const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh.tmem_full), tile_iter & 1, abort_flag));
             if (!got) {
                 if (lane == 0) {
@@ -290,31 +299,37 @@ __global__ void __launch_bounds__(THREADS, 1)
                 break;
             }
             tc_fence_after();
-            const int q = m0 + row;
-            const double rqv = q < nq ? rq[q] : 0.0;  // NaN when the query row is constant
             const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
             float4* srow = staging + row * (BN / 4);
-#pragma unroll 1
+            // TMEM reads run one 16-column chunk ahead of the arithmetic
+            uint32_t acc[2][3][16];
+            tmem_ld16(lane_base + half * 64, acc[0][0]);
+            tmem_ld16(lane_base + BN + half * 64, acc[0][1]);
+            tmem_ld16(lane_base + 2 * BN + half * 64, acc[0][2]);
+            tmem_wait_ld();
+#pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int col0 = half * 64 + c * 16;
-                uint32_t p1[16], p2[16], p3[16];
-                tmem_ld16(lane_base + col0, p1);
-                tmem_ld16(lane_base + BN + col0, p2);
-                tmem_ld16(lane_base + 2 * BN + col0, p3);
-                tmem_wait_ld();
-                const int r0 = n0 + col0;
-                const double rrl = (lane < 16 && r0 + lane < R) ? rr[r0 + lane] : 0.0;  // NaN: constant ref row
+                if (c + 1 < 4) {
+                    tmem_ld16(lane_base + col0 + 16, acc[(c + 1) & 1][0]);
+                    tmem_ld16(lane_base + BN + col0 + 16, acc[(c + 1) & 1][1]);
+                    tmem_ld16(lane_base + 2 * BN + col0 + 16, acc[(c + 1) & 1][2]);
+                }
+                const uint32_t* p1 = acc[c & 1][0];
+                const uint32_t* p2 = acc[c & 1][1];
+                const uint32_t* p3 = acc[c & 1][2];
                 float v[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     // |N| < 2^53: the int64 value converts to double exactly
                     const int64_t N = 128ll * (127ll * (int)p1[j] + (int)p3[j]) - 127ll * (int)p2[j];
-                    const double rrj = __shfl_sync(0xffffffffu, rrl, j);
+                    const double rrj = __shfl_sync(0xffffffffu, rrv[c], j);
                     v[j] = (float)(((double)N * rqv) * rrj);
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
                     srow[((col0 >> 2) + u) ^ (row & 7)] = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+                if (c + 1 < 4) tmem_wait_ld();
             }
             // all of this warp's TMEM reads are done: release its share of the accumulator
             tc_fence_before();

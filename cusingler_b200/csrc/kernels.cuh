@@ -99,9 +99,12 @@ struct LabelQ {
     int32_t pad;
 };
 
+// row_len: floats of a score row that the labels cover.  With `lorder` (label ids, longest first)
+// and rows of at most 200 KB, each block stages its row in shared memory before selecting.
 void launch_select_first(const float* scores, int64_t ld, int nq, int L, const LabelQ* lq, float p,
                          float thre, const int64_t* qn2, float* label_scores, int32_t* first, uint8_t* flags,
-                         float* scratch, int64_t scratch_per_warp, int* status, cudaStream_t s);
+                         float* scratch, int64_t scratch_per_warp, int* status, int row_len, const int32_t* lorder,
+                         cudaStream_t s);
 
 // ---- fine-tune ----------------------------------------------------------------------------------
 struct FtGroup {
