@@ -113,7 +113,9 @@ struct sgr_ctx {
     std::vector<int64_t> h_ref_n2;
     DevBuf<float> reff_data;
     DevBuf<int32_t> reff_indices, reff_indptr;
-    DevBuf<int32_t> reff_ptr4;     // padded row offsets of ref_sorted
+    DevBuf<int32_t> d_blk_base;    // fine-tune lists: first 32-row block of each label
+    DevBuf<int32_t> d_ell_off;     // fine-tune lists: start of each 32-row block in ref_sorted
+    uint32_t R32 = 0;              // reference rows with each label's range padded to a multiple of 32
     DevBuf<uint32_t> ref_sorted;       // thre-pool entries of each reference row, by value
     DevBuf<uint32_t> d_ctidx, d_ft_genes, d_ft_idx;
     DevBuf<int32_t> d_gene_thre;
@@ -451,20 +453,43 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     SGR_CUDA(cudaMemcpyAsync(ctx->h_ref_n2.data(), ctx->ref_n2.p, ctx->R * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     // fine-tune: reference compacted to the thre pool, each row's entries sorted by value
     filter_csr(ctx, rm, ctx->ref_map_thre.p, ctx->reff_data, ctx->reff_indices, ctx->reff_indptr);
-    // row starts on 16-byte boundaries, lengths padded to whole vectors of four entries
-    std::vector<int32_t> fptr(ctx->R + 1), fptr4(ctx->R + 1, 0);
+    // 32-row blocks per label: a block is as long as its longest row, rounded up to 4 entries
+    std::vector<int32_t> fptr(ctx->R + 1);
     SGR_CUDA(cudaMemcpyAsync(fptr.data(), ctx->reff_indptr.p, (ctx->R + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost,
                              s));
     SGR_CUDA(cudaStreamSynchronize(s));
-    for (uint32_t r = 0; r < ctx->R; ++r) {
-        const int64_t next = (int64_t)fptr4[r] + ((fptr[r + 1] - fptr[r] + 3) & ~3);
-        if (next > INT32_MAX) fail(SGR_ERR_UNSUPPORTED, "fine-tune reference lists exceed 2^31 entries");
-        fptr4[r + 1] = (int32_t)next;
+    const uint32_t L = mk.n_labels;
+    std::vector<int32_t> blk_base(L + 1), ell_base(std::max<uint32_t>(ctx->R, 1)), ell_len(std::max<uint32_t>(ctx->R, 1));
+    std::vector<int32_t> ell_off{0};
+    ctx->R32 = 0;
+    for (uint32_t l = 0; l < L; ++l) {
+        const uint32_t start = mk.ctidx[2 * l], len = mk.ctidx[2 * l + 1];
+        blk_base[l] = (int32_t)ell_off.size() - 1;
+        ctx->R32 += (len + 31) & ~31u;
+        for (uint32_t b0 = 0; b0 < len; b0 += 32) {
+            const uint32_t nb = std::min<uint32_t>(32, len - b0);
+            int mx = 0;
+            for (uint32_t t = 0; t < nb; ++t) mx = std::max(mx, fptr[start + b0 + t + 1] - fptr[start + b0 + t]);
+            const int len4 = (mx + 3) & ~3;
+            for (uint32_t t = 0; t < nb; ++t) {
+                ell_base[start + b0 + t] = ell_off.back() + 4 * (int32_t)t;
+                ell_len[start + b0 + t] = len4;
+            }
+            const int64_t next = (int64_t)ell_off.back() + 32ll * len4;
+            if (next > INT32_MAX) fail(SGR_ERR_UNSUPPORTED, "fine-tune reference lists exceed 2^31 entries");
+            ell_off.push_back((int32_t)next);
+        }
     }
-    ctx->reff_ptr4.upload(fptr4, s);
-    ctx->ref_sorted.ensure((size_t)std::max<int32_t>(fptr4[ctx->R], 4));
-    launch_ref_presort(ctx->reff_data.p, ctx->reff_indices.p, ctx->reff_indptr.p, ctx->reff_ptr4.p, ctx->R,
+    blk_base[L] = (int32_t)ell_off.size() - 1;
+    ctx->d_blk_base.upload(blk_base, s);
+    ctx->d_ell_off.upload(ell_off, s);
+    DevBuf<int32_t> d_base, d_len;
+    d_base.upload(ell_base, s);
+    d_len.upload(ell_len, s);
+    ctx->ref_sorted.ensure((size_t)std::max<int32_t>(ell_off.back(), 4));
+    launch_ref_presort(ctx->reff_data.p, ctx->reff_indices.p, ctx->reff_indptr.p, d_base.p, d_len.p, ctx->R,
                        std::min(pow2_at_least(std::max<int>(ctx->Wt, 32)), 8192), ctx->Wt, ctx->ref_sorted.p, s);
+    SGR_CUDA(cudaStreamSynchronize(s));  // the row tables are freed on return
     ctx->d_ctidx.upload(mk.ctidx, s);
     ctx->d_ft_genes.upload(mk.ft_genes.empty() ? std::vector<uint32_t>{0} : mk.ft_genes, s);
     ctx->d_ft_idx.upload(mk.ft_idx, s);
@@ -864,7 +889,7 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     const size_t smem = ft_persistent_smem((int)std::max<uint32_t>(Wt, 1), capq, nw);
     if (smem > 220 * 1024) fail(SGR_ERR_UNSUPPORTED, "fine-tune gene pool too wide for shared memory");
     const int grid = ft_persistent_grid(smem, nw);
-    const int64_t per_cta = (int64_t)ctx->R + nw * (int64_t)max_label;
+    const int64_t per_cta = (int64_t)ctx->R32 + nw * (int64_t)max_label;
     ctx->ft_scratch.ensure((size_t)grid * per_cta);
     ctx->next_cell.ensure(1);
     SGR_CUDA(cudaMemsetAsync(ctx->next_cell.p, 0, sizeof(int), s));
@@ -872,7 +897,8 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     ctx->d_rounds.ensure(Q);
     FtPersistentArgs a{};
     a.ref_sorted = ctx->ref_sorted.p;
-    a.ref_ptr = ctx->reff_ptr4.p;
+    a.blk_base = ctx->d_blk_base.p;
+    a.ell_off = ctx->d_ell_off.p;
     a.ctidx = ctx->d_ctidx.p;
     a.ft_genes = ctx->d_ft_genes.p;
     a.ft_idx = ctx->d_ft_idx.p;
@@ -935,7 +961,7 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     a.rounds = ctx->d_rounds.p;
     a.scratch = ctx->ft_scratch.p;
     a.scratch_per_cta = per_cta;
-    a.max_rcand = (int)ctx->R;
+    a.max_rcand = (int)ctx->R32;
     a.max_label = (int)max_label;
     a.capq = capq;
     a.status = ctx->status.p;
@@ -956,13 +982,13 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
         ctx->sp_eqv.ensure((size_t)H * std::max<uint32_t>(Wt, 1));
         ctx->sp_nq.ensure(H);
         ctx->sp_rq.ensure(H);
-        ctx->sp_scores.ensure((size_t)H * ctx->R);
+        ctx->sp_scores.ensure((size_t)H * ctx->R32);
         ctx->sp_nan.ensure((size_t)H * 8 * max_label);
         SGR_CUDA(cudaMemsetAsync(ctx->sp_state.p, 0, H * sizeof(int), s));
         FtSplit sp{ctx->sp_cells.p, ctx->sp_top.p, ctx->sp_ntop.p, ctx->sp_rounds.p, ctx->sp_times.p,
                    ctx->sp_state.p, ctx->sp_nS.p, ctx->sp_kq.p, ctx->sp_nq.p, ctx->sp_rq.p, ctx->sp_total.p,
-                   ctx->sp_off.p, ctx->sp_eqv.p, ctx->sp_scores.p, ctx->sp_nan.p, (int)ctx->R};
-        const int max_chunks = (int)((ctx->R + 255) / 256);
+                   ctx->sp_off.p, ctx->sp_eqv.p, ctx->sp_scores.p, ctx->sp_nan.p, (int)ctx->R32};
+        const int max_chunks = (int)((ctx->R32 + 255) / 256);
         std::vector<int> state(H), total(H);
         // each round drops at least one candidate, so L + 2 rounds finish every cell
         for (uint32_t round = 0;; ++round) {

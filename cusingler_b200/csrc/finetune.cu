@@ -22,7 +22,11 @@
 // (2i + 1)^2 minus each run's tie spread).  Then, exactly in int64,
 //     N   = X + (|S| - k_r) Y - |S| k_q k_r
 //     n_r = Z2 + 2 c Z1 + k_r c^2 + (|S| - k_r) k_r^2,   c = |S| - 2 k_r.
-// Rows are padded to whole 16-byte vectors with entries of gene id Wt, whose e-value is SENT.
+// Layout: the rows of each label form blocks of 32 consecutive rows; a block stores entry j of its
+// t-th row at block start + (j / 4) * 128 + t * 4 + j % 4 and is as long as its longest row (rounded
+// up to 4), shorter rows padded with entries of gene id Wt, whose e-value is SENT.  One warp scores
+// the 32 rows of a block, one lane each, so a warp's 16-byte load of entry vector j / 4 covers 512
+// contiguous bytes.
 // The score is float((N * (1/sqrt(n_q))) * (1/sqrt(n_r))) in FP64, the same
 // formula as the score step's exact mode.
 
@@ -41,20 +45,20 @@ namespace {
 constexpr int SENT = INT32_MIN;  // "gene not in S"
 
 // One warp per reference row: its thre-pool entries sorted by (value, gene), each packed as
-// gene | last << 31, where last marks the final entry of a run of equal values.  Row r is written at
-// ptr4[r] and padded to ptr4[r + 1] (a multiple of 4 entries) with pad_gene | 1 << 31.
+// gene | last << 31, where last marks the final entry of a run of equal values.  Entry j of row r is
+// written at ell_base[r] + (j / 4) * 128 + j % 4; entries k .. ell_len[r] - 1 are pad_gene | 1 << 31.
 __global__ void __launch_bounds__(256) ref_presort_kernel(const float* data, const int32_t* idx, const int32_t* ptr,
-                                                          const int32_t* ptr4, uint32_t n_rows, int cap,
-                                                          uint32_t pad_gene, uint32_t* out) {
+                                                          const int32_t* ell_base, const int32_t* ell_len,
+                                                          uint32_t n_rows, int cap, uint32_t pad_gene, uint32_t* out) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     uint64_t* keys = reinterpret_cast<uint64_t*>(smem) + (size_t)warp * cap;
     constexpr uint32_t LAST = 0x80000000u;
     for (uint32_t row = blockIdx.x * wpb + warp; row < n_rows; row += gridDim.x * wpb) {
         const int beg = ptr[row], k = ptr[row + 1] - beg;
-        uint32_t* o = out + ptr4[row];
-        const int k4 = ptr4[row + 1] - ptr4[row];
-        for (int j = k + lane; j < k4; j += 32) o[j] = pad_gene | LAST;
+        uint32_t* ob = out + ell_base[row];
+        auto o = [ob](int j) -> uint32_t& { return ob[(j >> 2) * 128 + (j & 3)]; };
+        for (int j = k + lane; j < ell_len[row]; j += 32) o(j) = pad_gene | LAST;
         if (k <= cap) {
             int n = 1;
             while (n < k) n <<= 1;
@@ -66,7 +70,7 @@ __global__ void __launch_bounds__(256) ref_presort_kernel(const float* data, con
             for (int j = lane; j < k; j += 32) {
                 const uint64_t key = keys[j];
                 const bool last = j + 1 == k || (uint32_t)(keys[j + 1] >> 32) != (uint32_t)(key >> 32);
-                o[j] = (uint32_t)(key & 0xffffu) | (last ? LAST : 0u);
+                o(j) = (uint32_t)(key & 0xffffu) | (last ? LAST : 0u);
             }
             __syncwarp();
         } else {
@@ -81,7 +85,7 @@ __global__ void __launch_bounds__(256) ref_presort_kernel(const float* data, con
                     pos += (w < v) || (w == v && h < g);
                     eq_after += w == v && h > g;
                 }
-                o[pos] = (uint32_t)g | (eq_after == 0 ? LAST : 0u);
+                o(pos) = (uint32_t)g | (eq_after == 0 ? LAST : 0u);
             }
         }
     }
@@ -234,12 +238,14 @@ __device__ void cta_query_ranks(const FtPersistentArgs& a, int cell, int nS, con
     __syncthreads();
 }
 
-// Reference-row slot layout of a candidate list: label i's rows are [off[i], off[i+1]).  Thread 0.
+// Reference-row slot layout of a candidate list: label i's rows are [off[i], off[i] + len), each
+// label's range padded to a multiple of 32 slots so that a warp's 32 slots are one row block.
+// Thread 0.
 __device__ void label_offsets(const FtPersistentArgs& a, const uint8_t* top, int ntop, int* off) {
     int o = 0;
     for (int i = 0; i < ntop; ++i) {
         off[i] = o;
-        o += (int)a.ctidx[2 * top[i] + 1];
+        o += ((int)a.ctidx[2 * top[i] + 1] + 31) & ~31;
     }
     off[ntop] = o;
 }
@@ -254,9 +260,11 @@ __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const 
         if (off[mid] <= f) lo = mid;
         else hi = mid - 1;
     }
-    const int r = (int)a.ctidx[2 * top[lo]] + (f - off[lo]);
-    const int beg = a.ref_ptr[r], n4 = (a.ref_ptr[r + 1] - beg) >> 2;
-    const uint4* p = reinterpret_cast<const uint4*>(a.ref_sorted + beg);
+    const int lab = top[lo], j = f - off[lo];
+    if (j >= (int)a.ctidx[2 * lab + 1]) return 0.f;  // padding slot of the label's range
+    const int blk = a.blk_base[lab] + (j >> 5);
+    const int beg = a.ell_off[blk], n4 = (a.ell_off[blk + 1] - beg) >> 7;
+    const uint4* p = reinterpret_cast<const uint4*>(a.ref_sorted + beg) + (j & 31);
     // Per entry: b, sum of the open run; at a run's last entry (flag bit 31) the run is closed with
     // masks instead of a branch, since some lane of the warp closes a run at almost every step.
     // Bounds (|S| <= Wt <= 40000, e <= 2|S|): sum, Y, z * sum / z < 2^32, b^3 < 2^63.
@@ -265,7 +273,7 @@ __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const 
     uint4 nxt = n4 > 0 ? __ldg(p) : make_uint4(0u, 0u, 0u, 0u);
     for (int t = 0; t < n4; ++t) {
         const uint4 w4 = nxt;
-        if (t + 1 < n4) nxt = __ldg(p + t + 1);
+        if (t + 1 < n4) nxt = __ldg(p + 32 * (t + 1));
         const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -571,14 +579,15 @@ size_t ft_persistent_smem(int Wt, int capq, int nw) {
     return (b + 15) & ~size_t(15);
 }
 
-void launch_ref_presort(const float* data, const int32_t* idx, const int32_t* ptr, const int32_t* ptr4,
-                        uint32_t n_rows, int cap, uint32_t pad_gene, uint32_t* out, cudaStream_t s) {
+void launch_ref_presort(const float* data, const int32_t* idx, const int32_t* ptr, const int32_t* ell_base,
+                        const int32_t* ell_len, uint32_t n_rows, int cap, uint32_t pad_gene, uint32_t* out,
+                        cudaStream_t s) {
     if (!n_rows) return;
     int wpb = std::max(1, std::min(8, (200 * 1024) / (cap * 8)));
     const size_t smem = (size_t)wpb * cap * 8;
     SGR_CUDA(cudaFuncSetAttribute(ref_presort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const unsigned blocks = std::min<unsigned>((n_rows + wpb - 1) / wpb, device_sm_count() * 8);
-    ref_presort_kernel<<<blocks, 32 * wpb, smem, s>>>(data, idx, ptr, ptr4, n_rows, cap, pad_gene, out);
+    ref_presort_kernel<<<blocks, 32 * wpb, smem, s>>>(data, idx, ptr, ell_base, ell_len, n_rows, cap, pad_gene, out);
     SGR_LAUNCH_CHECK();
     count_launch();
 }

@@ -148,8 +148,9 @@ void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, con
 
 // Persistent exact fine-tune (finetune.cu).
 struct FtPersistentArgs {
-    const uint32_t* ref_sorted;   // per reference row: thre-pool entries by value, gene | run end << 31
-    const int32_t* ref_ptr;       // row offsets into ref_sorted (multiples of 4; rows padded)
+    const uint32_t* ref_sorted;   // thre-pool entries by value, gene | run end << 31, in 32-row blocks
+    const int32_t* blk_base;      // per label: its first row block
+    const int32_t* ell_off;       // per row block: start in ref_sorted (blocks + 1 entries)
     const uint32_t* ctidx;        // (start, len) per label
     const uint32_t* ft_genes;     // fine-tune pair lists (thre ids)
     const uint32_t* ft_idx;       // (start, len) per ordered label pair
@@ -202,9 +203,10 @@ void launch_ft_keys(int n, const int32_t* list, int L, const uint8_t* flags, con
 // nw: warps per CTA (8 or 32)
 int ft_persistent_grid(size_t smem, int nw);
 void launch_ft_persistent(const FtPersistentArgs& a, int grid, size_t smem, int nw, cudaStream_t s);
-// Value-sorted, run-flagged fine-tune lists of the reference rows; row r at ptr4[r], padded to
-// ptr4[r + 1] with pad_gene entries.
-void launch_ref_presort(const float* data, const int32_t* idx, const int32_t* ptr, const int32_t* ptr4,
-                        uint32_t n_rows, int cap, uint32_t pad_gene, uint32_t* out, cudaStream_t s);
+// Value-sorted, run-flagged fine-tune lists of the reference rows in 32-row blocks: entry j of row r
+// at ell_base[r] + (j / 4) * 128 + j % 4, padded to ell_len[r] entries with pad_gene entries.
+void launch_ref_presort(const float* data, const int32_t* idx, const int32_t* ptr, const int32_t* ell_base,
+                        const int32_t* ell_len, uint32_t n_rows, int cap, uint32_t pad_gene, uint32_t* out,
+                        cudaStream_t s);
 
 }  // namespace sgr
