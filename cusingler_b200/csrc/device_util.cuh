@@ -189,6 +189,22 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
     before = __shfl_sync(FULL, before, src);
     cnt = __shfl_sync(FULL, cnt, src);
     if (cnt > 256) return false;
+    // when statistic j is the last of its bin and j + 1 exists, statistic j + 1 is the smallest value
+    // of the next non-empty bin: collect that bin too (the bins between are empty)
+    int nb = -1, total = cnt;
+    if (j + 1 >= before + cnt && j + 1 < n) {
+        int cand = 256, ccand = 0;
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+            if (cand == 256 && 8 * lane + t > bin && c[t] > 0) {
+                cand = 8 * lane + t;
+                ccand = c[t];
+            }
+        nb = __reduce_min_sync(FULL, cand);
+        const int cnb = __reduce_add_sync(FULL, cand == nb ? ccand : 0);
+        if (cnt + cnb <= 256) total = cnt + cnb;
+        else nb = -1;
+    }
     __syncwarp();
     uint32_t* buf = reinterpret_cast<uint32_t*>(hist);
     int w = 0;
@@ -198,7 +214,8 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
         uint32_t u = 0;
         if (i < n) {
             const float x = v[i];
-            in = bin_of(x) == bin;
+            const int b = bin_of(x);
+            in = b == bin || b == nb;
             u = ord_key(x);
         }
         const unsigned m = __ballot_sync(FULL, in);
@@ -206,8 +223,8 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
         w += __popc(m);
     }
     int np = 1;
-    while (np < cnt) np <<= 1;
-    for (int i = cnt + lane; i < np; i += 32) buf[i] = 0xffffffffu;
+    while (np < total) np <<= 1;
+    for (int i = total + lane; i < np; i += 32) buf[i] = 0xffffffffu;
     __syncwarp();
     for (int size = 2; size <= np; size <<= 1)
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
@@ -223,7 +240,7 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
         }
     const int r = j - before;
     *ka = buf[r];
-    if (r + 1 < cnt) {
+    if (r + 1 < total) {
         *kb = buf[r + 1];
     } else {
         uint32_t nxt = 0xffffffffu;
@@ -237,24 +254,12 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
     return true;
 }
 
-// The reference's percentile(v, n, p) (src/cusingler.cu:947-978) for one score list, by one warp.
-// Lists holding NaN are sorted exactly as libstdc++ would, in `scratch` (n floats), by lane 0.
-__device__ float quantile_warp(const float* v, const LabelQ& lq, float p, int* hist, float* scratch, int lane,
-                               int* status) {
+// quantile_warp after its min / max / NaN pass: kmin, kmax are the warp-wide extreme order keys of
+// the list and nan whether it holds a NaN (all lanes agree).  Lists holding NaN are sorted exactly as
+// libstdc++ would, in `scratch` (n floats), by lane 0.
+__device__ float quantile_warp_core(const float* v, const LabelQ& lq, float p, int* hist, float* scratch, int lane,
+                                    int* status, uint32_t kmin, uint32_t kmax, bool nan) {
     const int n = lq.len;
-    if (lq.kind == 0) return v[0];
-    bool nan = false;
-    uint32_t kmin = 0xffffffffu, kmax = 0u;
-    for (int i = lane; i < n; i += 32) {
-        const float x = v[i];
-        nan |= x != x;
-        const uint32_t u = ord_key(x);
-        kmin = min(kmin, u);
-        kmax = max(kmax, u);
-    }
-    nan = __any_sync(FULL, nan);
-    kmin = __reduce_min_sync(FULL, kmin);
-    kmax = __reduce_max_sync(FULL, kmax);
     if (nan) {
         float r = 0.f;
         if (scratch == nullptr) {
@@ -292,6 +297,26 @@ __device__ float quantile_warp(const float* v, const LabelQ& lq, float p, int* h
     nxt = warp_min_u32(nxt);
     kb = le > lq.k ? ka : nxt;
     return interp(p, lq.prev_index, lq.step, key_float(ka), key_float(kb));
+}
+
+// The reference's percentile(v, n, p) (src/cusingler.cu:947-978) for one score list, by one warp.
+__device__ float quantile_warp(const float* v, const LabelQ& lq, float p, int* hist, float* scratch, int lane,
+                               int* status) {
+    const int n = lq.len;
+    if (lq.kind == 0) return v[0];
+    bool nan = false;
+    uint32_t kmin = 0xffffffffu, kmax = 0u;
+    for (int i = lane; i < n; i += 32) {
+        const float x = v[i];
+        nan |= x != x;
+        const uint32_t u = ord_key(x);
+        kmin = min(kmin, u);
+        kmax = max(kmax, u);
+    }
+    nan = __any_sync(FULL, nan);
+    kmin = __reduce_min_sync(FULL, kmin);
+    kmax = __reduce_max_sync(FULL, kmax);
+    return quantile_warp_core(v, lq, p, hist, scratch, lane, status, kmin, kmax, nan);
 }
 
 
