@@ -116,6 +116,8 @@ struct sgr_ctx {
     DevBuf<int32_t> d_blk_base;    // fine-tune lists: first 32-row block of each label
     DevBuf<int32_t> d_ell_off;     // fine-tune lists: start of each 32-row block in ref_sorted
     uint32_t R32 = 0;              // reference rows with each label's range padded to a multiple of 32
+    int pack_shift = 0;            // packed fine-tune row scan (0: not representable, plain scan)
+    int pack_scan = 1;             // tuning: use the packed scan when representable
     DevBuf<uint32_t> ref_sorted;       // thre-pool entries of each reference row, by value
     DevBuf<uint32_t> d_ctidx, d_ft_genes, d_ft_idx;
     DevBuf<int32_t> d_gene_thre;
@@ -481,6 +483,17 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
         }
     }
     blk_base[L] = (int32_t)ell_off.size() - 1;
+    // packed row scan: a run's kept count (<= the longest row) in the high bits, its e-sum
+    // (<= longest row x 2 Wt) below bit `shift`
+    {
+        int64_t max_row = 1;
+        for (uint32_t r = 0; r < ctx->R; ++r) max_row = std::max<int64_t>(max_row, fptr[r + 1] - fptr[r]);
+        int cbits = 0;
+        while ((int64_t(1) << cbits) <= max_row) ++cbits;
+        const int shift = 32 - cbits;
+        ctx->pack_shift = (shift > 0 && max_row * 2 * (int64_t)std::max<uint32_t>(ctx->Wt, 1) < (int64_t(1) << shift))
+                              ? shift : 0;
+    }
     ctx->d_blk_base.upload(blk_base, s);
     ctx->d_ell_off.upload(ell_off, s);
     DevBuf<int32_t> d_base, d_len;
@@ -897,6 +910,7 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     ctx->d_rounds.ensure(Q);
     FtPersistentArgs a{};
     a.ref_sorted = ctx->ref_sorted.p;
+    a.pack_shift = ctx->pack_scan ? ctx->pack_shift : 0;
     a.blk_base = ctx->d_blk_base.p;
     a.ell_off = ctx->d_ell_off.p;
     a.ctidx = ctx->d_ctidx.p;
@@ -1087,6 +1101,11 @@ sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value) {
     if (what == 2) {
         if (value < 1) return SGR_ERR_INVALID_ARGUMENT;
         ctx->score_chunk_bytes = (size_t)value << 20;
+        return SGR_OK;
+    }
+    if (what == 3) {
+        if (value != 0 && value != 1) return SGR_ERR_INVALID_ARGUMENT;
+        ctx->pack_scan = value;
         return SGR_OK;
     }
     return SGR_ERR_INVALID_ARGUMENT;

@@ -44,6 +44,9 @@ namespace {
 
 constexpr int SENT = INT32_MIN;  // "gene not in S"
 
+// Packed e-value of row_score's packed path: (1 << shift) + e at genes of S, 0 elsewhere.
+__device__ __forceinline__ int pack_e(int v, int shift) { return v >= 0 ? (int)((1u << shift) + (uint32_t)v) : 0; }
+
 // One warp per reference row: its thre-pool entries sorted by (value, gene), each packed as
 // gene | last << 31, where last marks the final entry of a run of equal values.  Entry j of row r is
 // written at ell_base[r] + (j / 4) * 128 + j % 4; entries k .. ell_len[r] - 1 are pad_gene | 1 << 31.
@@ -265,30 +268,58 @@ __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const 
     const int blk = a.blk_base[lab] + (j >> 5);
     const int beg = a.ell_off[blk], n4 = (a.ell_off[blk + 1] - beg) >> 7;
     const uint4* p = reinterpret_cast<const uint4*>(a.ref_sorted + beg) + (j & 31);
-    // Per entry: b, sum of the open run; at a run's last entry (flag bit 31) the run is closed with
-    // masks instead of a branch, since some lane of the warp closes a run at almost every step.
+    // Per entry: b, sum of the open run; at a run's last entry (flag bit 31) the run is closed.
     // Bounds (|S| <= Wt <= 40000, e <= 2|S|): sum, Y, z * sum / z < 2^32, b^3 < 2^63.
-    uint32_t b = 0, sum = 0, ka = 0, Y = 0;
+    uint32_t ka = 0, Y = 0;
     uint64_t X = 0, T = 0;
     uint4 nxt = n4 > 0 ? __ldg(p) : make_uint4(0u, 0u, 0u, 0u);
-    for (int t = 0; t < n4; ++t) {
-        const uint4 w4 = nxt;
-        if (t + 1 < n4) nxt = __ldg(p + 32 * (t + 1));
-        const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
+    if (a.pack_shift) {
+        // packed e-values: (1 << shift) + e at genes of S, 0 elsewhere, so one add per entry keeps
+        // the run's count (high bits) and e-sum (low bits); the host chose shift so that neither
+        // field of a run can overflow
+        const uint32_t* ep = reinterpret_cast<const uint32_t*>(eqv);
+        const int sh = a.pack_shift;
+        const uint32_t low = (1u << sh) - 1u;
+        uint32_t acc = 0;
+        for (int t = 0; t < n4; ++t) {
+            const uint4 w4 = nxt;
+            if (t + 1 < n4) nxt = __ldg(p + 32 * (t + 1));
+            const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const uint32_t ent = ws[u];
-            const int v = eqv[ent & 0xffffu];
-            b += v >= 0 ? 1u : 0u;
-            sum += (uint32_t)max(v, 0);
-            const uint32_t m = (uint32_t)((int32_t)ent >> 31);  // all ones at a run's last entry
-            const uint32_t bm = b & m, sm = sum & m;
-            X += (uint64_t)(2 * ka + bm) * sm;
-            Y += sm;
-            T += (uint64_t)bm * (bm * bm - 1u);
-            ka += bm;
-            b &= ~m;
-            sum &= ~m;
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t ent = ws[u];
+                acc += ep[ent & 0xffffu];
+                if ((int32_t)ent < 0) {  // last entry of its value run
+                    const uint32_t b = acc >> sh, sum = acc & low;
+                    X += (uint64_t)(2 * ka + b) * sum;
+                    Y += sum;
+                    T += (uint64_t)b * (b * b - 1u);
+                    ka += b;
+                    acc = 0;
+                }
+            }
+        }
+    } else {
+        uint32_t b = 0, sum = 0;
+        for (int t = 0; t < n4; ++t) {
+            const uint4 w4 = nxt;
+            if (t + 1 < n4) nxt = __ldg(p + 32 * (t + 1));
+            const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t ent = ws[u];
+                const int v = eqv[ent & 0xffffu];
+                b += v >= 0 ? 1u : 0u;
+                sum += (uint32_t)max(v, 0);
+                if ((int32_t)ent < 0) {  // last entry of its value run
+                    X += (uint64_t)(2 * ka + b) * sum;
+                    Y += sum;
+                    T += (uint64_t)b * (b * b - 1u);
+                    ka += b;
+                    b = 0;
+                    sum = 0;
+                }
+            }
         }
     }
     const int64_t kr = ka;
@@ -394,6 +425,8 @@ __global__ void __launch_bounds__(NW * 32) ft_persistent_kernel(FtPersistentArgs
                 continue;
             }
             cta_query_ranks<NW>(a, cell, nS, bits, eqv, qkeys, &sh.kq, &sh.nq, &sh.rq);
+            if (a.pack_shift)
+                for (int g = tid; g <= Wt; g += NW * 32) eqv[g] = pack_e(eqv[g], a.pack_shift);
             if (tid == 0) label_offsets(a, top, ntop, off);
             __syncthreads();
             const int total = off[ntop];
@@ -507,8 +540,12 @@ __global__ void __launch_bounds__(256) split_scan_kernel(FtPersistentArgs a, FtS
     uint8_t* top = reinterpret_cast<uint8_t*>(off + 260);
     const int* geqv = sp.eqv + (size_t)i * a.Wt;
     const int ntop = sp.ntop[i];
-    for (int g = threadIdx.x; g < a.Wt; g += 256) eqv[g] = geqv[g];
-    if (threadIdx.x == 0) eqv[a.Wt] = SENT;
+    if (a.pack_shift) {
+        for (int g = threadIdx.x; g < a.Wt; g += 256) eqv[g] = pack_e(geqv[g], a.pack_shift);
+    } else {
+        for (int g = threadIdx.x; g < a.Wt; g += 256) eqv[g] = geqv[g];
+    }
+    if (threadIdx.x == 0) eqv[a.Wt] = a.pack_shift ? 0 : SENT;
     for (int t = threadIdx.x; t <= ntop; t += 256) off[t] = sp.off[(size_t)i * 257 + t];
     for (int t = threadIdx.x; t < ntop; t += 256) top[t] = sp.top[(size_t)i * 256 + t];
     __syncthreads();

@@ -173,6 +173,7 @@ struct FtPersistentArgs {
     int64_t scratch_per_cta;
     int max_rcand, max_label, capq;
     int* status;
+    int pack_shift;               // > 0: row scan on packed e-values (count << shift | e-sum); 0: plain
 };
 
 // Split path for heavy cells: state arrays of H cells (device), one round per launch_split_round.

@@ -136,7 +136,10 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
 /* Launch-shape choices.  what 0: warps per CTA of the persistent fine-tune kernel (8 or 32);
  * what 1: candidate count from which a cell's fine-tune rounds are spread over the whole GPU
  * instead of one CTA (>= 2; large values disable the split path); what 2: MiB of score-step
- * correlations per block of queries (small blocks are read back from L2 by the selection). */
+ * correlations per block of queries (small blocks are read back from L2 by the selection); what 3:
+ * 1 (default) lets the fine-tune row scan keep each value run's count and e-sum in one packed
+ * 32-bit word when the trained reference allows it, 0 always uses the two-register scan.
+ * No choice changes any result. */
 sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value);
 sgr_status sgr_reset_timings(sgr_ctx* ctx);
 sgr_status sgr_get_timings(const sgr_ctx* ctx, sgr_timings* out);

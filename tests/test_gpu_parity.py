@@ -95,3 +95,16 @@ def test_annotate_matches_steps():
     assert np.nanmax(np.abs(scores - fp["scores"])) < 1e-5
     assert (first != fp["first"]).sum() == 0
     assert (final != fp["final"]).sum() <= 1
+
+
+@pytest.mark.parametrize("kind", ["tiny", "families"])
+@pytest.mark.parametrize("packed", [0, 1])
+def test_final_labels_both_row_scans(kind, packed):
+    """The fine-tune row scan on packed (count, e-sum) words and on two registers give the oracle's
+    final labels and round counts."""
+    a, prob = annotator(kind, abi.MODE_EXACT)
+    a.set_tuning(3, packed)
+    res = H.oracle_run(kind, 1)
+    final, rounds = a.finetune(prob.qry, res["flags"].astype(np.uint8))
+    assert np.array_equal(final, res["final"])
+    assert np.array_equal(rounds, res["rounds"])
