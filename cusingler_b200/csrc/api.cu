@@ -138,6 +138,7 @@ struct sgr_ctx {
     DevBuf<int64_t> sp_nq;
     DevBuf<double> sp_rq;
     DevBuf<float> sp_scores, sp_nan;
+    DevBuf<unsigned long long> sp_rows;
     DevBuf<int32_t> ft_order;
     DevBuf<int> ft_order_n;
     DevBuf<int32_t> d_final, d_rounds;
@@ -999,26 +1000,69 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
         ctx->sp_scores.ensure((size_t)H * ctx->R32);
         ctx->sp_nan.ensure((size_t)H * 8 * max_label);
         SGR_CUDA(cudaMemsetAsync(ctx->sp_state.p, 0, H * sizeof(int), s));
+        ctx->sp_rows.ensure(1);
+        SGR_CUDA(cudaMemsetAsync(ctx->sp_rows.p, 0, sizeof(unsigned long long), s));
         FtSplit sp{ctx->sp_cells.p, ctx->sp_top.p, ctx->sp_ntop.p, ctx->sp_rounds.p, ctx->sp_times.p,
                    ctx->sp_state.p, ctx->sp_nS.p, ctx->sp_kq.p, ctx->sp_nq.p, ctx->sp_rq.p, ctx->sp_total.p,
-                   ctx->sp_off.p, ctx->sp_eqv.p, ctx->sp_scores.p, ctx->sp_nan.p, (int)ctx->R32};
+                   ctx->sp_off.p, ctx->sp_eqv.p, ctx->sp_scores.p, ctx->sp_nan.p, (int)ctx->R32, ctx->sp_rows.p};
         const int max_chunks = (int)((ctx->R32 + 255) / 256);
-        std::vector<int> state(H), total(H);
-        // each round drops at least one candidate, so L + 2 rounds finish every cell
-        for (uint32_t round = 0;; ++round) {
-            if (round > L + 3) fail(SGR_ERR_STATE, "fine-tune split path did not converge");
-            launch_split_round(a, sp, H, max_chunks, s);
-            SGR_CUDA(cudaMemcpyAsync(state.data(), ctx->sp_state.p, H * sizeof(int), cudaMemcpyDeviceToHost, s));
-            SGR_CUDA(cudaMemcpyAsync(total.data(), ctx->sp_total.p, H * sizeof(int), cudaMemcpyDeviceToHost, s));
-            SGR_CUDA(cudaStreamSynchronize(s));
-            ctx->prof.acc.ft_split_rounds++;
-            bool all = true;
-            for (int i = 0; i < H; ++i) {
-                all &= state[i] == 2;
-                ctx->prof.acc.ft_split_rows += (uint64_t)total[i];
+        split_round_setup(a);
+        // Rounds run kRoundsPerGraph at a time from one CUDA graph (rounds of finished cells do
+        // nothing), with one host check of the cells' states per graph launch; a stream that
+        // cannot be captured runs the same rounds as plain launches.
+        constexpr int kRoundsPerGraph = 4;
+        cudaGraphExec_t exec = nullptr;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const uint64_t before = launch_count();
+            cudaGraph_t graph = nullptr;
+            try {
+                for (int r = 0; r < kRoundsPerGraph; ++r) launch_split_round(a, sp, H, max_chunks, s);
+            } catch (...) {
+                cudaStreamEndCapture(s, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                cudaGetLastError();
+                throw;
             }
+            if (cudaStreamEndCapture(s, &graph) == cudaSuccess && graph) {
+                if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) exec = nullptr;
+                cudaGraphDestroy(graph);
+            }
+            // launches recorded into the graph are counted when the graph runs
+            count_launch(before - launch_count());
+        }
+        cudaGetLastError();
+        std::vector<int> state(H);
+        // each round drops at least one candidate, so L + 2 rounds finish every cell
+        uint32_t rounds_run = 0;
+        for (;;) {
+            if (rounds_run > L + 3) {
+                if (exec) cudaGraphExecDestroy(exec);
+                fail(SGR_ERR_STATE, "fine-tune split path did not converge");
+            }
+            if (exec) {
+                const cudaError_t e = cudaGraphLaunch(exec, s);
+                if (e != cudaSuccess) {
+                    cudaGraphExecDestroy(exec);
+                    SGR_CUDA(e);
+                }
+                count_launch(3 * kRoundsPerGraph);
+                rounds_run += kRoundsPerGraph;
+            } else {
+                launch_split_round(a, sp, H, max_chunks, s);
+                rounds_run += 1;
+            }
+            SGR_CUDA(cudaMemcpyAsync(state.data(), ctx->sp_state.p, H * sizeof(int), cudaMemcpyDeviceToHost, s));
+            SGR_CUDA(cudaStreamSynchronize(s));
+            bool all = true;
+            for (int i = 0; i < H; ++i) all &= state[i] == 2;
             if (all) break;
         }
+        if (exec) cudaGraphExecDestroy(exec);
+        unsigned long long rows = 0;
+        SGR_CUDA(cudaMemcpyAsync(&rows, ctx->sp_rows.p, sizeof(rows), cudaMemcpyDeviceToHost, s));
+        SGR_CUDA(cudaStreamSynchronize(s));
+        ctx->prof.acc.ft_split_rounds += rounds_run;
+        ctx->prof.acc.ft_split_rows += rows;
     }
     ctx->prof.end(sp_ft, s);
     if (!final_labels) return;  // caller reads ctx->d_final / d_rounds itself

@@ -525,6 +525,7 @@ __global__ void __launch_bounds__(256) split_prepare_kernel(FtPersistentArgs a, 
         sp.nq[i] = s_nq;
         sp.rq[i] = s_rq;
         sp.total[i] = sp.off[(size_t)i * 257 + ntop];
+        atomicAdd(sp.rows_scored, (unsigned long long)sp.total[i]);
     }
 }
 
@@ -584,13 +585,18 @@ size_t split_prepare_smem(int Wt, int capq) {
            sizeof(int) * 16;
 }
 
-void launch_split_round(const FtPersistentArgs& a, const FtSplit& sp, int H, int max_chunks, cudaStream_t s) {
+void split_round_setup(const FtPersistentArgs& a) {
     const size_t sm1 = split_prepare_smem(a.Wt, a.capq);
     SGR_CUDA(cudaFuncSetAttribute(split_prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+    const size_t sm2 = sizeof(int) * (((a.Wt + 4) & ~3) + 260) + 256;
+    SGR_CUDA(cudaFuncSetAttribute(split_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+}
+
+void launch_split_round(const FtPersistentArgs& a, const FtSplit& sp, int H, int max_chunks, cudaStream_t s) {
+    const size_t sm1 = split_prepare_smem(a.Wt, a.capq);
     split_prepare_kernel<<<H, 256, sm1, s>>>(a, sp);
     SGR_LAUNCH_CHECK();
     const size_t sm2 = sizeof(int) * (((a.Wt + 4) & ~3) + 260) + 256;
-    SGR_CUDA(cudaFuncSetAttribute(split_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
     split_scan_kernel<<<dim3(max_chunks, H), 256, sm2, s>>>(a, sp);
     SGR_LAUNCH_CHECK();
     split_decide_kernel<<<H, 256, 0, s>>>(a, sp);

@@ -194,8 +194,12 @@ struct FtSplit {
     float* scores;          // H x max_rcand
     float* nan_scratch;     // H x 8 x max_label
     int max_rcand;
+    unsigned long long* rows_scored;  // device counter: reference rows scored, summed over rounds
 };
 
+// Function attributes of the split-round kernels; call once before launch_split_round (and before
+// capturing rounds into a CUDA graph).
+void split_round_setup(const FtPersistentArgs& a);
 void launch_split_round(const FtPersistentArgs& a, const FtSplit& sp, int H, int max_chunks, cudaStream_t s);
 
 size_t ft_persistent_smem(int Wt, int capq, int nw);
