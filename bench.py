@@ -165,7 +165,8 @@ def main():
     ap.add_argument("--mode", default="exact", choices=["exact", "fp32ref"])
     ap.add_argument("--cpu-sample", type=int, default=96)
     ap.add_argument("--form", default="both", choices=["plain", "learned", "both"])
-    ap.add_argument("--mlp-train-cells", type=int, default=60000)
+    ap.add_argument("--mlp-train-cells", type=int, default=200000)
+    ap.add_argument("--mlp-epochs", type=int, default=40)
     ap.add_argument("--min-confidence", type=float, default=0.98)
     ap.add_argument("--check-fraction", type=float, default=0.01)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -231,8 +232,8 @@ def main():
         train_q = synth.generate(synth.make_world(wl, 0), args.mlp_train_cells, 2 + 1000 * rank)
         tf, tfin, tsc = ann.annotate(train_q, with_scores=True)
         t1 = time.perf_counter()
-        loss = ann.mlp_train(tsc, tfin, epochs=20, batch=4096, lr=1e-3, weight_decay=0.01, seed=rank)
-        mlp_info = {"train_cells": args.mlp_train_cells, "label_s": t1 - t0,
+        loss = ann.mlp_train(tsc, tfin, epochs=args.mlp_epochs, batch=4096, lr=1e-3, weight_decay=0.01, seed=rank)
+        mlp_info = {"train_cells": args.mlp_train_cells, "epochs": args.mlp_epochs, "label_s": t1 - t0,
                     "train_s": time.perf_counter() - t1, "final_loss": loss,
                     "min_confidence": args.min_confidence, "check_fraction": args.check_fraction}
 
@@ -243,6 +244,14 @@ def main():
         f, fin, st = ann.annotate_learned(csr, min_confidence=args.min_confidence,
                                           check_fraction=args.check_fraction)
         return f, fin, st
+
+    # autotuner: launch shapes timed on a sample of the batch, outside the timed region, per form
+    tune_sample = qry.rows(0, min(qry.n_rows, 20000))
+    tuning = {}
+
+    def tune(learned):
+        tuning["learned" if learned else "plain"] = ann.autotune(
+            tune_sample, learned=learned, min_confidence=args.min_confidence, check_fraction=args.check_fraction)
 
     def timed(fn, csr, steps):
         for _ in range(args.warmup):
@@ -264,12 +273,14 @@ def main():
     form_lines = {}
     ms_plain = tm_plain = clk_plain = None
     if args.form in ("plain", "both") or not use_learned:
+        tune(False)
         ms_plain, tm_plain, clk_plain, out = timed(run_plain, csr_dev, args.steps)
         plain_final = out[1]
         form_lines["plain"] = {"value": world_size * qry.n_rows / (ms_plain / 1000.0), "ms_per_step": ms_plain}
     else:
         plain_final = ann.annotate(csr_dev)[1]
     if use_learned:
+        tune(True)
         ms_l, tm_l, clk_l, out = timed(run_learned, csr_dev, args.steps)
         agree = float((out[1] == plain_final).mean())
         form_lines["learned"] = {"value": world_size * qry.n_rows / (ms_l / 1000.0), "ms_per_step": ms_l,
@@ -282,6 +293,12 @@ def main():
         ms, tm, clk = ms_plain, tm_plain, clk_plain
         fn_chosen = run_plain
     value = world_size * qry.n_rows / (ms / 1000.0)
+
+    t = tuning.get(chosen)
+    if t:  # the chosen form's launch shapes for the e2e leg
+        ann.set_tuning(0, t["ft_warps"])
+        ann.set_tuning(1, t["ft_heavy"])
+        ann.set_tuning(2, t["score_chunk_mb"])
 
     # e2e: host (pinned) inputs through the same call, upload inside the timed region
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
@@ -350,6 +367,7 @@ def main():
             "gpu_launches": int(tm["launches"] / steps * steps),
             "roofline": dominant, "rooflines": [roof_corr, roof_rank, roof_sel],
             "stages_ms": stages, "ref_prep_s": ref_prep_s, "forms": form_lines, "mlp": mlp_info,
+            "tuning": tuning,
             "ft_rounds_per_cell": tm["ft_cell_rounds"] / max(1, tm["cells"]),
             "clocks": clk, "cpu_baseline": cpu,
         }

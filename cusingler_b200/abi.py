@@ -28,7 +28,7 @@ SYMBOLS = [
     "sgr_finetune", "sgr_annotate", "sgr_get_info", "sgr_get_u32", "sgr_debug_ranks", "sgr_debug_scores",
     "sgr_debug_stl_sort", "sgr_debug_stl_minmax", "sgr_set_stream", "sgr_set_profiling", "sgr_reset_timings",
     "sgr_get_timings", "sgr_select_labels_noalloc", "sgr_mlp_train", "sgr_mlp_predict", "sgr_mlp_params",
-    "sgr_mlp_load", "sgr_mlp_debug_grads", "sgr_annotate_learned", "sgr_set_tuning",
+    "sgr_mlp_load", "sgr_mlp_debug_grads", "sgr_annotate_learned", "sgr_set_tuning", "sgr_autotune",
 ]
 
 
@@ -51,6 +51,14 @@ class SgrTimings(C.Structure):
                 ("ft_cell_rounds", C.c_uint64), ("mlp_ms", C.c_double), ("select_launches", C.c_uint64),
                 ("select_bytes", C.c_uint64), ("ft_queue_cells", C.c_uint64), ("ft_split_cells", C.c_uint64),
                 ("ft_split_rounds", C.c_uint64), ("ft_split_rows", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class SgrTuning(C.Structure):
+    _fields_ = [("ft_warps", C.c_int32), ("ft_heavy", C.c_int32), ("score_chunk_mb", C.c_int32),
+                ("trials", C.c_int32), ("best_ms", C.c_double), ("worst_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -106,6 +114,7 @@ def lib():
             "sgr_set_stream": (C.c_int, [vp, vp]),
             "sgr_set_profiling": (C.c_int, [vp, C.c_int]),
             "sgr_set_tuning": (C.c_int, [vp, C.c_int, C.c_int]),
+            "sgr_autotune": (C.c_int, [vp, C.POINTER(SgrCsr), f32, f32, i32, i32, f32, f32, C.POINTER(SgrTuning)]),
             "sgr_reset_timings": (C.c_int, [vp]),
             "sgr_get_timings": (C.c_int, [vp, C.POINTER(SgrTimings)]),
             "sgr_select_labels_noalloc": (C.c_int, [vp, C.c_int64, u32, vp, u32, f32, f32, vp, vp, vp, vp]),
@@ -273,6 +282,15 @@ class Annotator:
     def set_stream(self, stream_ptr):
         """Run on a caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream); None = own."""
         self._check(self.L.sgr_set_stream(self.h, stream_ptr))
+
+    def autotune(self, sample, learned=False, quantile=0.8, thre=0.05, times=0, min_confidence=0.98,
+                 check_fraction=0.01) -> dict:
+        """Time every launch-shape candidate on `sample` and keep the fastest (see sgr_autotune)."""
+        csr, keep = self._csr(sample)
+        out = SgrTuning()
+        self._check(self.L.sgr_autotune(self.h, C.byref(csr), quantile, thre, times, 1 if learned else 0,
+                                        min_confidence, check_fraction, C.byref(out)))
+        return out.as_dict()
 
     def set_tuning(self, what: int, value: int):
         self._check(self.L.sgr_set_tuning(self.h, what, value))

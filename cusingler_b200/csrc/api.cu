@@ -1130,6 +1130,70 @@ sgr_status sgr_set_stream(sgr_ctx* ctx, void* stream) {
     return SGR_OK;
 }
 
+sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, float finetune_thre,
+                        int32_t finetune_times, int32_t learned, float min_confidence, float check_fraction,
+                        sgr_tuning* out) {
+    if (!ctx || !sample || !out) return SGR_ERR_INVALID_ARGUMENT;
+    if (ctx->device < 0) return SGR_ERR_STATE;
+    const uint32_t Q = sample->n_rows;
+    std::vector<int32_t> first(std::max<uint32_t>(Q, 1)), fin(first.size()), first0, fin0;
+    sgr_learned_stats st{};
+    auto run = [&]() -> sgr_status {
+        return learned ? sgr_annotate_learned(ctx, sample, quantile, finetune_thre, finetune_times, min_confidence,
+                                              check_fraction, first.data(), fin.data(), &st)
+                       : sgr_annotate(ctx, sample, quantile, finetune_thre, finetune_times, first.data(), fin.data(),
+                                      nullptr);
+    };
+    const int warps[] = {8, 32};
+    const int heavy[] = {4, 6, 9, 16, 1 << 30};
+    const int chunk_mb[] = {256, 1024};
+    const int keep_w = ctx->ft_warps, keep_h = ctx->ft_heavy;
+    const size_t keep_c = ctx->score_chunk_bytes;
+    sgr_tuning best{};
+    best.best_ms = 1e300;
+    // one untimed pass grows every buffer to the sample's size
+    sgr_status stt = run();
+    if (stt != SGR_OK) return stt;
+    first0 = first;
+    fin0 = fin;
+    for (int w : warps)
+        for (int h : heavy)
+            for (int c : chunk_mb) {
+                ctx->ft_warps = w;
+                ctx->ft_heavy = h;
+                ctx->score_chunk_bytes = (size_t)c << 20;
+                const auto t0 = std::chrono::steady_clock::now();
+                stt = run();
+                const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                if (stt != SGR_OK) {
+                    ctx->ft_warps = keep_w;
+                    ctx->ft_heavy = keep_h;
+                    ctx->score_chunk_bytes = keep_c;
+                    return stt;
+                }
+                if (first != first0 || fin != fin0) {
+                    ctx->ft_warps = keep_w;
+                    ctx->ft_heavy = keep_h;
+                    ctx->score_chunk_bytes = keep_c;
+                    ctx->err = "autotune: launch shapes disagree on the labels";
+                    return SGR_ERR_STATE;
+                }
+                best.trials++;
+                best.worst_ms = std::max(best.worst_ms, ms);
+                if (ms < best.best_ms) {
+                    best.best_ms = ms;
+                    best.ft_warps = w;
+                    best.ft_heavy = h;
+                    best.score_chunk_mb = c;
+                }
+            }
+    ctx->ft_warps = best.ft_warps;
+    ctx->ft_heavy = best.ft_heavy;
+    ctx->score_chunk_bytes = (size_t)best.score_chunk_mb << 20;
+    *out = best;
+    return SGR_OK;
+}
+
 sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value) {
     if (!ctx) return SGR_ERR_INVALID_ARGUMENT;
     if (what == 0) {

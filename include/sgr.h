@@ -142,6 +142,24 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
  * No choice changes any result. */
 sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value);
 sgr_status sgr_reset_timings(sgr_ctx* ctx);
+
+/* Autotuner (no counterpart in the reference): runs the annotation of `sample` (host or device
+ * CSR) once per candidate launch shape -- fine-tune warps per CTA {8, 32} x split-path threshold
+ * {4, 6, 9, 16, off} x score block {256, 1024} MiB -- keeps the fastest by wall time, and leaves
+ * it set in the context.  learned = 1 tunes the learned form (sgr_annotate_learned with
+ * min_confidence / check_fraction), 0 the plain form.  Every candidate must give the same first and
+ * final labels (SGR_ERR_STATE otherwise).  The trials count in sgr_timings. */
+typedef struct sgr_tuning {
+    int32_t ft_warps;
+    int32_t ft_heavy;       /* 1 << 30 when the split path is off */
+    int32_t score_chunk_mb;
+    int32_t trials;
+    double best_ms;         /* wall time of the chosen candidate on the sample */
+    double worst_ms;        /* slowest candidate */
+} sgr_tuning;
+sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, float finetune_thre,
+                        int32_t finetune_times, int32_t learned, float min_confidence, float check_fraction,
+                        sgr_tuning* out);
 sgr_status sgr_get_timings(const sgr_ctx* ctx, sgr_timings* out);
 
 /* ---- Learned proposal ------------------------------------------------------------------------ */

@@ -169,3 +169,18 @@ def test_dropin_run_matches_oracle():
     assert [r[0] for r in res] == cells
     assert [r[1] for r in res] == [prob.label_names[i] for i in o["first"]]
     assert [r[2] for r in res] == [prob.label_names[i] for i in o["final"]]
+
+
+def test_autotune_keeps_results():
+    """The autotuner times every launch-shape candidate, leaves the fastest set, and the annotation
+    afterwards still equals the oracle's."""
+    prob = H.problem("families")
+    a = abi.Annotator(gpuid=0)
+    a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
+    t = a.autotune(prob.qry)
+    assert t["trials"] == 20
+    assert t["ft_warps"] in (8, 32) and t["ft_heavy"] in (4, 6, 9, 16, 1 << 30)
+    assert t["score_chunk_mb"] in (256, 1024) and 0 < t["best_ms"] <= t["worst_ms"]
+    first, final = a.annotate(prob.qry)
+    o = H.oracle_run("families", 1)
+    assert np.array_equal(first, o["first"]) and np.array_equal(final, o["final"])
