@@ -570,7 +570,7 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
     for (uint32_t l = 0; l < L; ++l) max_len = std::max(max_len, ctx->mk.ctidx[2 * l + 1]);
     float* scratch = nullptr;
     if (any_nan_ref) {
-        scratch = ctx->sel_scratch.ensure((size_t)select_blocks_with_scratch() * 8 * max_len);
+        scratch = ctx->sel_scratch.ensure((size_t)select_warps_with_scratch() * max_len);
     }
     ctx->label_scores.ensure((size_t)Q * L);
     ctx->first.ensure(Q);
@@ -836,7 +836,7 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
                            ctx->ft_rd.p, ctx->ft_qf.p, ctx->ft_rf.p, ctx->ft_qr.p, ctx->ft_rr.p, ctx->ft_qn.p,
                            ctx->ft_rn.p, ctx->ft_scores.p, s);
             const double t_corr = pc.lap();
-            float* scratch = ctx->sel_scratch.ensure((size_t)select_blocks_with_scratch() * 8 * max_label);
+            float* scratch = ctx->sel_scratch.ensure((size_t)select_warps_with_scratch() * max_label);
             launch_ft_select(ctx->ft_groups.p, ctx->ft_sel_items.p, (uint32_t)si.size(), ctx->ft_lq.p, p,
                              ctx->ft_scores.p, ctx->ft_label_scores.p, scratch, max_label, ctx->status.p, s);
             std::vector<float> ls(out_off);

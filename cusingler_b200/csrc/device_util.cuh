@@ -160,7 +160,15 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
     auto bin_of = [&](float x) { return min(255, (int)((x - fmin) * scale)); };
     for (int b = lane; b < 256; b += 32) hist[b] = 0;
     __syncwarp();
-    for (int i = lane; i < n; i += 32) atomicAdd(&hist[bin_of(v[i])], 1);
+    int i = lane;
+    for (; i + 96 < n; i += 128) {  // four independent loads in flight per lane
+        const float x0 = v[i], x1 = v[i + 32], x2 = v[i + 64], x3 = v[i + 96];
+        atomicAdd(&hist[bin_of(x0)], 1);
+        atomicAdd(&hist[bin_of(x1)], 1);
+        atomicAdd(&hist[bin_of(x2)], 1);
+        atomicAdd(&hist[bin_of(x3)], 1);
+    }
+    for (; i < n; i += 32) atomicAdd(&hist[bin_of(v[i])], 1);
     __syncwarp();
     int c[8], s = 0;
 #pragma unroll
@@ -208,19 +216,16 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
     __syncwarp();
     uint32_t* buf = reinterpret_cast<uint32_t*>(hist);
     int w = 0;
-    for (int base = 0; base < n; base += 32) {
-        const int i = base + lane;
-        bool in = false;
-        uint32_t u = 0;
-        if (i < n) {
-            const float x = v[i];
-            const int b = bin_of(x);
-            in = b == bin || b == nb;
-            u = ord_key(x);
-        }
-        const unsigned m = __ballot_sync(FULL, in);
-        if (in) buf[w + __popc(m & ((1u << lane) - 1u))] = u;
-        w += __popc(m);
+    const unsigned lt = (1u << lane) - 1u;
+    for (int base = 0; base < n; base += 64) {  // two 32-value chunks per step
+        const int i0 = base + lane, i1 = base + 32 + lane;
+        const float x0 = i0 < n ? v[i0] : 0.f, x1 = i1 < n ? v[i1] : 0.f;
+        const int b0 = bin_of(x0), b1 = bin_of(x1);
+        const bool in0 = i0 < n && (b0 == bin || b0 == nb), in1 = i1 < n && (b1 == bin || b1 == nb);
+        const unsigned m0 = __ballot_sync(FULL, in0), m1 = __ballot_sync(FULL, in1);
+        if (in0) buf[w + __popc(m0 & lt)] = ord_key(x0);
+        if (in1) buf[w + __popc(m0) + __popc(m1 & lt)] = ord_key(x1);
+        w += __popc(m0) + __popc(m1);
     }
     int np = 1;
     while (np < total) np <<= 1;
@@ -305,17 +310,27 @@ __device__ float quantile_warp(const float* v, const LabelQ& lq, float p, int* h
     const int n = lq.len;
     if (lq.kind == 0) return v[0];
     bool nan = false;
-    uint32_t kmin = 0xffffffffu, kmax = 0u;
-    for (int i = lane; i < n; i += 32) {
+    uint32_t mn0 = 0xffffffffu, mn1 = 0xffffffffu, mx0 = 0u, mx1 = 0u;
+    int i = lane;
+    for (; i + 32 < n; i += 64) {  // two independent chains per lane
+        const float x0 = v[i], x1 = v[i + 32];
+        nan |= (x0 != x0) | (x1 != x1);
+        const uint32_t u0 = ord_key(x0), u1 = ord_key(x1);
+        mn0 = min(mn0, u0);
+        mx0 = max(mx0, u0);
+        mn1 = min(mn1, u1);
+        mx1 = max(mx1, u1);
+    }
+    if (i < n) {
         const float x = v[i];
         nan |= x != x;
         const uint32_t u = ord_key(x);
-        kmin = min(kmin, u);
-        kmax = max(kmax, u);
+        mn0 = min(mn0, u);
+        mx0 = max(mx0, u);
     }
     nan = __any_sync(FULL, nan);
-    kmin = __reduce_min_sync(FULL, kmin);
-    kmax = __reduce_max_sync(FULL, kmax);
+    const uint32_t kmin = __reduce_min_sync(FULL, min(mn0, mn1));
+    const uint32_t kmax = __reduce_max_sync(FULL, max(mx0, mx1));
     return quantile_warp_core(v, lq, p, hist, scratch, lane, status, kmin, kmax, nan);
 }
 

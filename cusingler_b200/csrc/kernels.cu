@@ -381,18 +381,18 @@ __global__ void __launch_bounds__(256) corr_simt_kernel(const int8_t* A, const i
 // STAGE: the block first copies the query's score row (row_len floats) into shared memory with
 // 16-byte loads, and warps take labels from `lorder` (longest first) through a shared counter; every
 // selection pass then reads shared memory instead of global memory.
-template <bool STAGE>
-__global__ void __launch_bounds__(256) select_first_kernel(const float* scores, int64_t ld, int nq, int L,
+template <bool STAGE, int NW = STAGE ? 16 : 8>
+__global__ void __launch_bounds__(NW * 32) select_first_kernel(const float* scores, int64_t ld, int nq, int L,
                                                            const LabelQ* lq, float p, float thre, const int64_t* qn2,
                                                            float* label_scores, int32_t* first, uint8_t* flags,
                                                            float* scratch, int64_t spw, int* status, int row_len,
                                                            const int32_t* lorder) {
     extern __shared__ __align__(16) float srow[];
     __shared__ float ls[256];
-    __shared__ int hist[8][256];
+    __shared__ int hist[NW][256];
     __shared__ int s_mx, s_next;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float* my_scratch = scratch ? scratch + (size_t)(blockIdx.x * 8 + warp) * spw : nullptr;
+    float* my_scratch = scratch ? scratch + (size_t)(blockIdx.x * NW + warp) * spw : nullptr;
     const bool vec = STAGE && (ld % 4) == 0 && (reinterpret_cast<uintptr_t>(scores) & 15) == 0;
     for (int q = blockIdx.x; q < nq; q += gridDim.x) {
         const float* row = scores + (size_t)q * ld;
@@ -402,10 +402,10 @@ __global__ void __launch_bounds__(256) select_first_kernel(const float* scores, 
                 if (vec) {
                     const float4* src = reinterpret_cast<const float4*>(row);
                     float4* dst = reinterpret_cast<float4*>(srow);
-                    for (int i = threadIdx.x; i < row_len / 4; i += 256) dst[i] = __ldcs(src + i);
-                    for (int i = (row_len & ~3) + threadIdx.x; i < row_len; i += 256) srow[i] = __ldcs(row + i);
+                    for (int i = threadIdx.x; i < row_len / 4; i += NW * 32) dst[i] = __ldcs(src + i);
+                    for (int i = (row_len & ~3) + threadIdx.x; i < row_len; i += NW * 32) srow[i] = __ldcs(row + i);
                 } else {
-                    for (int i = threadIdx.x; i < row_len; i += 256) srow[i] = __ldcs(row + i);
+                    for (int i = threadIdx.x; i < row_len; i += NW * 32) srow[i] = __ldcs(row + i);
                 }
             }
             if (threadIdx.x == 0) s_next = 0;
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(256) select_first_kernel(const float* scores, 
                 if (lane == 0) ls[l] = r;
             }
         } else {
-            for (int l = warp; l < L; l += 8) {
+            for (int l = warp; l < L; l += NW) {
                 const LabelQ d = lq[l];
                 float r;
                 if (qnan) r = __int_as_float(0x7fffffff);
@@ -626,10 +626,10 @@ void launch_select_first(const float* scores, int64_t ld, int nq, int L, const L
         SGR_CUDA(cudaFuncSetAttribute(select_first_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)stage_bytes));
         int per_sm = 0;
-        SGR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, select_first_kernel<true>, 256, stage_bytes));
-        per_sm = std::max(1, std::min(per_sm, 2));  // scratch is sized for two blocks per SM
+        SGR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, select_first_kernel<true>, 512, stage_bytes));
+        per_sm = std::max(1, std::min(per_sm, 2));  // scratch is sized for two 16-warp blocks per SM
         const unsigned blocks = (unsigned)std::min<long>(nq, (long)sm_count() * per_sm);
-        select_first_kernel<true><<<blocks, 256, stage_bytes, s>>>(scores, ld, nq, L, lq, p, thre, qn2, label_scores,
+        select_first_kernel<true><<<blocks, 512, stage_bytes, s>>>(scores, ld, nq, L, lq, p, thre, qn2, label_scores,
                                                                    first, flags, scratch, spw, status, row_len,
                                                                    lorder);
     } else {

@@ -20,7 +20,9 @@ void count_launch(uint64_t n = 1);
 
 // Grid caps of the selection kernels; their scratch (NaN-bearing lists) is sized per warp of the
 // capped grid.
-inline int select_blocks_with_scratch() { return device_sm_count() * 2; }
+// Warps of the score-step selection that may use NaN-list scratch at once: two blocks per SM of at
+// most 16 warps.
+inline int select_warps_with_scratch() { return device_sm_count() * 2 * 16; }
 
 // ---- gather + rank ----------------------------------------------------------------------------
 //
