@@ -11,16 +11,20 @@
 //             reciprocal, so the score of a constant row is NaN as in the reference.
 //
 // Operands are the rank kernel's int8 rows [H | L | S] (3 * Kp bytes, Kp a multiple of 128), so one
-// TMA tensor map per operand covers all three limb planes and the K loop runs over 3 * Kp bytes; the
-// MMA warp sends each third of the K loop to its own accumulator (3 x 128 TMEM columns).
+// TMA tensor map per operand covers all three limb planes.  Per tile the K loop runs plane by plane
+// in the order H, S, L into three TMEM accumulators of BN = 160 columns (P1, P3, P2; 480 of 512
+// columns).  A 128 x 160 tile (rather than 128 x 128) reads fewer operand bytes from shared memory
+// per MMA cycle, which bounds the M = 128 int8 MMA.
 //
-// Structure: persistent kernel, one CTA per SM, 256 threads:
-//   warp 0      TMA producer (128 x 128-byte boxes, 128B swizzle, STAGES-deep ring)
-//   warp 1      TMEM allocator and single-thread tcgen05.mma issuer (M = 128, N = 128, K = 32)
+// Structure: persistent kernel, one CTA per SM, 384 threads:
+//   warp 0      TMA producer (128 x 128-byte A boxes, 160 x 128-byte B boxes, 128B swizzle,
+//               STAGES-deep ring)
+//   warp 1      TMEM allocator and single-thread tcgen05.mma issuer (M = 128, N = 160, K = 32)
 //   warps 4..11 epilogue, two warps per TMEM lane quadrant (warp % 4), one column half each:
-//               tcgen05.ld 32x32b, exact recombination, scores into a 128 x 128 staging tile in
-//               shared memory, TMEM released, then row-contiguous 16-byte stores from the staging
-//               tile, which overlap the next tile's MMAs
+//               tcgen05.ld 32x32b of P1 and P3 into T = 127 P1 + P3 (registers), release of those
+//               two accumulators (the next tile's H and S planes may start), then P2, the exact
+//               recombination, scores into a 128 x 160 staging tile in shared memory, release of
+//               P2, and row-contiguous 16-byte stores from the staging tile
 // No TMA multicast is used.  Every mbarrier wait is bounded: on timeout the kernel records
 // SGR_TC_TIMEOUT in *status, drains its own TMA copies (bounded), frees TMEM and returns.
 
@@ -36,9 +40,11 @@ namespace sgr {
 namespace {
 
 constexpr int BM = 128;
-constexpr int BN = 128;
+constexpr int BN = 160;  // 3 x 160 accumulator columns fit TMEM's 512
+constexpr int HALF = BN / 2;       // columns per epilogue warp
+constexpr int CH = HALF / 16;      // 16-column TMEM chunks per epilogue warp
 constexpr int BK = 128;  // bytes of K per stage (one 128-byte swizzle row)
-constexpr int STAGES = 5;
+constexpr int STAGES = 4;
 constexpr int A_BYTES = BM * BK;
 constexpr int B_BYTES = BN * BK;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
@@ -147,7 +153,8 @@ struct __align__(8) TcShared {
     uint64_t full[STAGES];
     uint64_t empty[STAGES];
     uint64_t tmem_full;
-    uint64_t tmem_empty;
+    uint64_t tmem_empty;    // accumulator regions of P1 and P3 released by the epilogue
+    uint64_t tmem_empty_c;  // accumulator region of P2 released
     uint64_t drain;
     uint32_t tmem_base;
     int abort_flag;
@@ -175,6 +182,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         mbar_init(smem_u32(&sh.tmem_full), 1);
         mbar_init(smem_u32(&sh.tmem_empty), EPI_WARPS);
+        mbar_init(smem_u32(&sh.tmem_empty_c), EPI_WARPS);
         mbar_init(smem_u32(&sh.drain), 1);
         sh.abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -208,8 +216,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const uint32_t b_dst = a_dst + A_BYTES;
                     const uint32_t fb = smem_u32(&sh.full[s]);
                     mbar_expect_tx(fb, STAGE_BYTES);
-                    tma_load_2d(a_dst, &tmA, kb * BK, m0, fb);
-                    tma_load_2d(b_dst, &tmB, kb * BK, n0, fb);
+                    // planes in the order H, S, L (the MMA's accumulator order)
+                    const int grp = kb / seg_blocks, seg = grp == 0 ? 0 : (grp == 1 ? 2 : 1);
+                    const int kx = (seg * seg_blocks + kb % seg_blocks) * BK;
+                    tma_load_2d(a_dst, &tmA, kx, m0, fb);
+                    tma_load_2d(b_dst, &tmB, kx, n0, fb);
                 }
             }
             if (!ok) {
@@ -244,10 +255,19 @@ __global__ void __launch_bounds__(THREADS, 1)
                         break;
                     }
                     tc_fence_after();
-                    const int seg = kb / seg_blocks;
+                    // groups of k-blocks: H plane -> P1 (region 0), S plane -> P3 (region 1),
+                    // L plane -> P2 (region 2), which may still be read by the previous epilogue
+                    const int grp = kb / seg_blocks;
+                    if (kb == 2 * seg_blocks) {
+                        if (!mbar_wait(smem_u32(&sh.tmem_empty_c), (tile_iter & 1) ^ 1, abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                    }
                     const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
                     const uint64_t da = smem_desc(a_addr), db = smem_desc(a_addr + A_BYTES);
-                    const uint32_t tc = tmem + seg * BN;
+                    const uint32_t tc = tmem + grp * BN;
                     const bool first = (kb % seg_blocks) == 0;
 #pragma unroll
                     for (int k = 0; k < BK / 32; ++k)
@@ -284,10 +304,10 @@ __global__ void __launch_bounds__(THREADS, 1)
             // norms of this tile's rows and columns, loaded while the accumulator is still being computed
             const int q = m0 + row;
             const double rqv = q < nq ? rq[q] : 0.0;  // NaN when the query row is constant
-            double rrv[4];
+            double rrv[CH];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int r = n0 + half * 64 + c * 16 + lane;
+            for (int c = 0; c < CH; ++c) {
+                const int r = n0 + half * HALF + c * 16 + lane;
                 rrv[c] = (lane < 16 && r < R) ? rr[r] : 0.0;  // NaN for a constant reference row
             }
             const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh.tmem_full), tile_iter & 1, abort_flag));
@@ -301,46 +321,49 @@ __global__ void __launch_bounds__(THREADS, 1)
             tc_fence_after();
             const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
             float4* srow = staging + row * (BN / 4);
-            // TMEM reads run one 16-column chunk ahead of the arithmetic
-            uint32_t acc[2][3][16];
-            tmem_ld16(lane_base + half * 64, acc[0][0]);
-            tmem_ld16(lane_base + BN + half * 64, acc[0][1]);
-            tmem_ld16(lane_base + 2 * BN + half * 64, acc[0][2]);
+            // phase 1: T = 127 P1 + P3 for this warp's columns, then P1 and P3 are released
+            int T[CH][16];
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                uint32_t pa[16], pb[16];
+                tmem_ld16(lane_base + half * HALF + c * 16, pa);
+                tmem_ld16(lane_base + BN + half * HALF + c * 16, pb);
+                tmem_wait_ld();
+#pragma unroll
+                for (int j = 0; j < 16; ++j) T[c][j] = 127 * (int)pa[j] + (int)pb[j];
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh.tmem_empty));
+            // phase 2: P2, reads one chunk ahead of the arithmetic
+            uint32_t p2[2][16];
+            tmem_ld16(lane_base + 2 * BN + half * HALF, p2[0]);
             tmem_wait_ld();
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int col0 = half * 64 + c * 16;
-                if (c + 1 < 4) {
-                    tmem_ld16(lane_base + col0 + 16, acc[(c + 1) & 1][0]);
-                    tmem_ld16(lane_base + BN + col0 + 16, acc[(c + 1) & 1][1]);
-                    tmem_ld16(lane_base + 2 * BN + col0 + 16, acc[(c + 1) & 1][2]);
-                }
-                const uint32_t* p1 = acc[c & 1][0];
-                const uint32_t* p2 = acc[c & 1][1];
-                const uint32_t* p3 = acc[c & 1][2];
+            for (int c = 0; c < CH; ++c) {
+                const int col0 = half * HALF + c * 16;
+                if (c + 1 < CH) tmem_ld16(lane_base + 2 * BN + col0 + 16, p2[(c + 1) & 1]);
                 float v[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    // |N| < 2^53: the int64 value converts to double exactly
-                    const int64_t N = 128ll * (127ll * (int)p1[j] + (int)p3[j]) - 127ll * (int)p2[j];
+                    const int64_t N = 128ll * T[c][j] - 127ll * (int)p2[c & 1][j];
                     const double rrj = __shfl_sync(0xffffffffu, rrv[c], j);
                     v[j] = (float)(((double)N * rqv) * rrj);
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
                     srow[((col0 >> 2) + u) ^ (row & 7)] = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
-                if (c + 1 < 4) tmem_wait_ld();
+                if (c + 1 < CH) tmem_wait_ld();
             }
-            // all of this warp's TMEM reads are done: release its share of the accumulator
+            // all of this warp's TMEM reads are done: release its share of P2
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&sh.tmem_empty));
-            const int sub = lane >> 4, c4 = half * 16 + (lane & 15);
-            const int col = n0 + 4 * c4;
+            if (lane == 0) mbar_arrive(smem_u32(&sh.tmem_empty_c));
+            constexpr int F4 = HALF / 4;  // 16-byte chunks per row of this warp
 #pragma unroll 4
-            for (int i = 0; i < 16; ++i) {
-                const int rr_ = 32 * quarter + 2 * i + sub;
-                const int qq = m0 + rr_;
+            for (int it = lane; it < 32 * F4; it += 32) {
+                const int rr_ = 32 * quarter + it / F4, c4 = half * F4 + it % F4;
+                const int qq = m0 + rr_, col = n0 + 4 * c4;
                 if (qq >= nq || col >= R) continue;
                 const float4 val = staging[rr_ * (BN / 4) + (c4 ^ (rr_ & 7))];
                 float* dst = out + (size_t)qq * ld + col;
@@ -380,11 +403,11 @@ EncodeTiled encode_fn() {
 }
 
 // Tensor map of a [rows x (3 * Kp)] int8 limb matrix, 128 x 128-byte boxes, 128B swizzle.
-CUtensorMap limb_map(const int8_t* base, int rows, int Kp) {
+CUtensorMap limb_map(const int8_t* base, int rows, int Kp, int box_rows) {
     CUtensorMap m;
     cuuint64_t dims[2] = {(cuuint64_t)(3 * Kp), (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)(3 * Kp)};
-    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(base), dims, strides, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -402,7 +425,7 @@ void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, con
     if (nq <= 0 || R <= 0) return;
     if (Kp % BK != 0 || (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15))
         fail(SGR_ERR_INVALID_ARGUMENT, "tensor-core correlation: misaligned operands");
-    const CUtensorMap ta = limb_map(A, nq, Kp), tb = limb_map(B, R, Kp);
+    const CUtensorMap ta = limb_map(A, nq, Kp, BM), tb = limb_map(B, R, Kp, BN);
     const size_t smem = corr_tc_smem();
     SGR_CUDA(cudaFuncSetAttribute(corr_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long tiles = (long)((nq + BM - 1) / BM) * ((R + BN - 1) / BN);
