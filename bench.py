@@ -245,8 +245,10 @@ def main():
                                           check_fraction=args.check_fraction)
         return f, fin, st
 
-    # autotuner: launch shapes timed on a sample of the batch, outside the timed region, per form
-    tune_sample = qry.rows(0, min(qry.n_rows, 20000))
+    # autotuner: launch shapes timed per form, outside the timed region, on a separate seeded query
+    # sample of the same workload (large enough that the learned form routes a representative set
+    # of cells to the fine-tune)
+    tune_sample = synth.generate(synth.make_world(wl, 0), min(qry.n_rows, 50000), 3 + 1000 * rank)
     tuning = {}
 
     def tune(learned):
@@ -319,6 +321,34 @@ def main():
     h2d = qry.data.nbytes + qry.indices.nbytes + 4 * (qry.n_rows + 1)
     d2h = 2 * 4 * qry.n_rows
 
+    # FP16-operand correlation variant beside the exact INT8 form: score step only, same batch
+    fp16 = None
+    if mode == abi.MODE_EXACT and world_size == 1:
+        def score_ms():
+            ann.score_first(csr_dev)
+            barrier()
+            ann.reset_timings()
+            ann.set_profiling(True)
+            for _ in range(args.steps):
+                out = ann.score_first(csr_dev)
+            barrier()
+            ann.set_profiling(False)
+            t = ann.timings()
+            return t["corr_ms"] / args.steps, t["total_ms"] / args.steps, out
+        corr_exact, step_exact, (f_e, s_e, _) = score_ms()
+        ann.set_tuning(4, 1)
+        corr_f16, step_f16, (f_h, s_h, _) = score_ms()
+        sub = qry.rows(0, min(qry.n_rows, 2000))
+        raw_f16 = ann.debug_scores(sub)
+        ann.set_tuning(4, 0)
+        raw_exact = ann.debug_scores(sub)
+        fp16 = {"corr_ms": corr_f16, "corr_ms_exact_int8": corr_exact, "score_step_ms": step_f16,
+                "score_step_ms_exact_int8": step_exact,
+                "max_abs_err_label_scores": float(np.nanmax(np.abs(s_h.astype(np.float64) - s_e))),
+                "max_abs_err_scores_2000_cells": float(np.nanmax(np.abs(raw_f16.astype(np.float64) - raw_exact))),
+                "first_label_agreement": float((f_h == f_e).mean()),
+                "note": "FP16 ranks (exact for G <= 2048), FP32 accumulation; error against the exact FP64 scores"}
+
     hbm, bf16, src = peaks()
     steps = args.steps
     stages = {k: tm[k] / steps for k in ("rank_ms", "corr_ms", "select_ms", "finetune_ms", "mlp_ms")}
@@ -369,7 +399,7 @@ def main():
             "gpu_launches": int(tm["launches"] / steps * steps),
             "roofline": dominant, "rooflines": [roof_corr, roof_rank, roof_sel],
             "stages_ms": stages, "ref_prep_s": ref_prep_s, "forms": form_lines, "mlp": mlp_info,
-            "tuning": tuning,
+            "tuning": tuning, "fp16_variant": fp16,
             "ft_rounds_per_cell": tm["ft_cell_rounds"] / max(1, tm["cells"]),
             "clocks": clk, "cpu_baseline": cpu,
         }

@@ -90,6 +90,8 @@ struct sgr_ctx {
     int cores = 1;
     cudaStream_t stream = nullptr;      // the stream work runs on
     cudaStream_t own_stream = nullptr;  // created with the context
+    cudaStream_t side = nullptr;        // fine-tune split path, concurrent with the work queue
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     Profiler prof;
     sgr_mode mode = SGR_MODE_EXACT;
     std::string err;
@@ -123,6 +125,9 @@ struct sgr_ctx {
     DevBuf<int32_t> d_gene_thre;
     DevBuf<LabelQ> d_lq_label;
     DevBuf<int> next_cell;
+    int corr_f16 = 0;              // tuning: score-step correlation on FP16 operands (not exact)
+    DevBuf<uint16_t> ref_f16;      // reference ranks as IEEE half rows [R][Kp]
+    bool ref_f16_ready = false;
     DevBuf<int32_t> d_lorder;  // label ids by reference-cell count, longest first (score-step selection)
     DevBuf<RankItem> rank_overflow;  // rows ranked by the rank kernel's large-buffer tier
     DevBuf<int> rank_n_overflow;
@@ -242,6 +247,7 @@ sgr_status guarded(sgr_ctx* ctx, F&& f) {
     } catch (const Error& e) {
         ctx->err = e.what();
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+        if (ctx->side) cudaStreamSynchronize(ctx->side);
         cudaGetLastError();
         ctx->prof.spans.clear();
         ctx->prof.used = 0;
@@ -412,6 +418,7 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     Markers& mk = ctx->mk;
     ctx->R = ref->n_rows;
     ctx->ref_cols = ref->n_cols;
+    ctx->ref_f16_ready = false;
     ctx->G = (int)mk.common.size();
     ctx->Kp = round_up(std::max(ctx->G, 1), 128);
     ctx->Wt = (uint32_t)mk.thre.size();
@@ -526,7 +533,31 @@ bool exact_simt() {
 }
 
 // Score-step correlation of nq query rows (LIMBS at A, norms at offset q0) with every reference row.
+// Reference ranks as IEEE half rows for the FP16 correlation variant (ranked on first use).
+void ensure_ref_f16(sgr_ctx* ctx) {
+    if (ctx->ref_f16_ready) return;
+    if (ctx->G > 2048) fail(SGR_ERR_UNSUPPORTED, "FP16 correlation variant needs at most 2048 marker genes");
+    ctx->ref_f16.ensure((size_t)ctx->R * ctx->Kp);
+    DevBuf<int64_t> n2;
+    DevBuf<double> rinv;
+    DevBuf<float> f32;
+    n2.ensure(ctx->R);
+    rinv.ensure(ctx->R);
+    f32.ensure(ctx->R);
+    DevCsr rm{ctx->ref_data.p, ctx->ref_indices.p, ctx->ref_indptr.p, ctx->R, ctx->ref_cols, -1};
+    RankGroup g{ctx->ref_map_common.p, ctx->G, ctx->Kp, ctx->ref_f16.p, n2.p, rinv.p, f32.p};
+    rank_rows(ctx, rm, g, RANK_F16, NORM_NONE);
+    SGR_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->ref_f16_ready = true;
+}
+
 void correlate(sgr_ctx* ctx, bool fp32, const int8_t* A, int nq, uint32_t q0, float* out, int64_t ld) {
+    if (ctx->corr_f16 && !fp32) {
+        launch_corr_tc(A, reinterpret_cast<const int8_t*>(ctx->ref_f16.p), nq, (int)ctx->R, ctx->Kp,
+                       ctx->q_rinv.p + q0, ctx->ref_rinv.p, ctx->q_n2.p + q0, ctx->ref_n2.p, out, ld, ctx->status.p,
+                       ctx->stream, true);
+        return;
+    }
     if (fp32 || exact_simt())
         launch_corr_simt(fp32, A, ctx->ref_limbs.p, nq, (int)ctx->R, ctx->G, ctx->Kp, ctx->q_f32.p + q0,
                          ctx->ref_f32.p, ctx->q_rinv.p + q0, ctx->ref_rinv.p, ctx->q_n2.p + q0, ctx->ref_n2.p, out,
@@ -545,11 +576,13 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
     ctx->q_n2.ensure(Q);
     ctx->q_rinv.ensure(Q);
     ctx->q_f32.ensure(Q);
+    const bool f16 = ctx->corr_f16 && !fp32;
+    if (f16) ensure_ref_f16(ctx);
     RankGroup g{ctx->qry_map_common.p, ctx->G, ctx->Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p};
     DevCsr qq = q;
     const uint64_t l0 = launch_count();
     int sp = ctx->prof.begin(ST_RANK, s);
-    rank_rows(ctx, qq, g, RANK_LIMBS, fp32 ? NORM_SEQ : NORM_NONE);
+    rank_rows(ctx, qq, g, f16 ? RANK_F16 : RANK_LIMBS, fp32 ? NORM_SEQ : NORM_NONE);
     ctx->prof.end(sp, s);
     ctx->prof.acc.rank_launches += launch_count() - l0;
 
@@ -582,7 +615,7 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
         const int nq = (int)std::min(chunk, Q - q0);
         const uint64_t c0 = launch_count();
         sp = ctx->prof.begin(ST_CORR, s);
-        correlate(ctx, fp32, ctx->q_limbs.p + (size_t)q0 * 3 * ctx->Kp, nq, q0, ctx->scores.p, R);
+        correlate(ctx, fp32, ctx->q_limbs.p + (size_t)q0 * (f16 ? 2 : 3) * ctx->Kp, nq, q0, ctx->scores.p, R);
         ctx->prof.end(sp, s);
         ctx->prof.acc.corr_launches += launch_count() - c0;
         sp = ctx->prof.begin(ST_SELECT, s);
@@ -874,6 +907,16 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
     }
 }
 
+// The context's second stream (and its fork / join events), created on first use.
+cudaStream_t side_stream(sgr_ctx* ctx) {
+    if (!ctx->side) {
+        SGR_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+        SGR_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+        SGR_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+    }
+    return ctx->side;
+}
+
 // Exact-mode fine-tune: the persistent kernel over a device work queue.  `flags_dev` is the
 // Q x L candidate-flag matrix in device memory.
 void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev, float p, float thre, int times,
@@ -980,10 +1023,37 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     a.max_label = (int)max_label;
     a.capq = capq;
     a.status = ctx->status.p;
+    // Heavy cells take the split path on a second stream, concurrently with the work-queue kernel:
+    // the two write disjoint cells, and the split rounds fill the SMs that the queue's last cells
+    // leave idle.  Its buffers are sized first (a reallocation would synchronise the device).
+    cudaStream_t ss = s;
+    if (!heavy_cells.empty()) {
+        const size_t Hm = std::min<size_t>(1024, heavy_cells.size());
+        ctx->sp_cells.ensure(Hm);
+        ctx->sp_top.ensure(Hm * 256);
+        ctx->sp_ntop.ensure(Hm);
+        ctx->sp_rounds.ensure(Hm);
+        ctx->sp_times.ensure(Hm);
+        ctx->sp_state.ensure(Hm);
+        ctx->sp_nS.ensure(Hm);
+        ctx->sp_kq.ensure(Hm);
+        ctx->sp_total.ensure(Hm);
+        ctx->sp_off.ensure(Hm * 257);
+        ctx->sp_eqv.ensure(Hm * std::max<uint32_t>(Wt, 1));
+        ctx->sp_nq.ensure(Hm);
+        ctx->sp_rq.ensure(Hm);
+        ctx->sp_scores.ensure(Hm * ctx->R32);
+        ctx->sp_nan.ensure(Hm * 8 * max_label);
+        ctx->sp_rows.ensure(1);
+        ss = side_stream(ctx);
+        SGR_CUDA(cudaEventRecord(ctx->ev_fork, s));
+        SGR_CUDA(cudaStreamWaitEvent(ss, ctx->ev_fork, 0));
+    }
     launch_ft_persistent(a, grid, smem, nw, s);
     // heavy cells: rounds spread over the whole GPU, in batches
     for (size_t h0 = 0; h0 < heavy_cells.size(); h0 += 1024) {
         const int H = (int)std::min<size_t>(1024, heavy_cells.size() - h0);
+        cudaStream_t s = ss;  // the split path's stream
         ctx->sp_cells.upload(heavy_cells.data() + h0, H, s);
         ctx->sp_top.ensure((size_t)H * 256);
         ctx->sp_ntop.ensure(H);
@@ -1064,6 +1134,10 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
         ctx->prof.acc.ft_split_rounds += rounds_run;
         ctx->prof.acc.ft_split_rows += rows;
     }
+    if (ss != s) {  // join the split path's stream
+        SGR_CUDA(cudaEventRecord(ctx->ev_join, ss));
+        SGR_CUDA(cudaStreamWaitEvent(s, ctx->ev_join, 0));
+    }
     ctx->prof.end(sp_ft, s);
     if (!final_labels) return;  // caller reads ctx->d_final / d_rounds itself
     SGR_CUDA(cudaMemcpyAsync(final_labels, ctx->d_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -1117,9 +1191,14 @@ sgr_status sgr_destroy(sgr_ctx* ctx) {
     }
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    cudaStream_t s = ctx->own_stream;
+    if (ctx->side) cudaStreamSynchronize(ctx->side);
+    cudaStream_t s = ctx->own_stream, side = ctx->side;
+    cudaEvent_t e1 = ctx->ev_fork, e2 = ctx->ev_join;
     delete ctx;  // DevBuf destructors free device memory
     if (s) cudaStreamDestroy(s);
+    if (side) cudaStreamDestroy(side);
+    if (e1) cudaEventDestroy(e1);
+    if (e2) cudaEventDestroy(e2);
     return SGR_OK;
 }
 
@@ -1209,6 +1288,12 @@ sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value) {
     if (what == 2) {
         if (value < 1) return SGR_ERR_INVALID_ARGUMENT;
         ctx->score_chunk_bytes = (size_t)value << 20;
+        return SGR_OK;
+    }
+    if (what == 4) {
+        if (value != 0 && value != 1) return SGR_ERR_INVALID_ARGUMENT;
+        if (value && ctx->mode != SGR_MODE_EXACT) return SGR_ERR_STATE;
+        ctx->corr_f16 = value;
         return SGR_OK;
     }
     if (what == 3) {
@@ -1399,8 +1484,10 @@ sgr_status sgr_debug_scores(sgr_ctx* ctx, const sgr_csr* qry, float* out) {
         ctx->q_n2.ensure(Q);
         ctx->q_rinv.ensure(Q);
         ctx->q_f32.ensure(Q);
+        const bool f16 = ctx->corr_f16 && !fp32;
+        if (f16) ensure_ref_f16(ctx);
         RankGroup g{ctx->qry_map_common.p, ctx->G, ctx->Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p};
-        rank_rows(ctx, q, g, RANK_LIMBS, fp32 ? NORM_SEQ : NORM_NONE);
+        rank_rows(ctx, q, g, f16 ? RANK_F16 : RANK_LIMBS, fp32 ? NORM_SEQ : NORM_NONE);
         DevBuf<float> sc;
         sc.ensure((size_t)Q * R);
         correlate(ctx, fp32, ctx->q_limbs.p, (int)Q, 0, sc.p, R);

@@ -25,6 +25,8 @@
 //               two accumulators (the next tile's H and S planes may start), then P2, the exact
 //               recombination, scores into a 128 x 160 staging tile in shared memory, release of
 //               P2, and row-contiguous 16-byte stores from the staging tile
+// A second instantiation (F16) is the FP16-operand variant benchmarked beside the exact one: d as
+// IEEE half (exact for |d| <= 2048), one kind::f16 accumulator with FP32 sums (not exact).
 // No TMA multicast is used.  Every mbarrier wait is bounded: on timeout the kernel records
 // SGR_TC_TIMEOUT in *status, drains its own TMA copies (bounded), frees TMEM and returns.
 
@@ -113,6 +115,19 @@ __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
     return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
+// kind::f16 instruction descriptor: F32 accumulator, F16 A and B, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
+    return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_c, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_c),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
 __device__ __forceinline__ void umma_i8(uint32_t tmem_c, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -160,6 +175,9 @@ struct __align__(8) TcShared {
     int abort_flag;
 };
 
+// F16: the FP16-operand variant -- one plane of d as half (2 * Kp bytes per row), kind::f16 with
+// FP32 accumulation into one accumulator, score = float((acc * 1/sqrt(n_q)) * 1/sqrt(n_r)).
+template <bool F16>
 __global__ void __launch_bounds__(THREADS, 1)
     corr_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nq, int R,
                    int Kp, const double* __restrict__ rq, const double* __restrict__ rr,
@@ -173,7 +191,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tiles_n = (R + BN - 1) / BN, tiles_m = (nq + BM - 1) / BM;
     const int n_tiles = tiles_m * tiles_n;
-    const int kblocks = 3 * Kp / BK, seg_blocks = Kp / BK;
+    const int kblocks = (F16 ? 2 : 3) * Kp / BK, seg_blocks = F16 ? kblocks : Kp / BK;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -217,8 +235,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const uint32_t fb = smem_u32(&sh.full[s]);
                     mbar_expect_tx(fb, STAGE_BYTES);
                     // planes in the order H, S, L (the MMA's accumulator order)
-                    const int grp = kb / seg_blocks, seg = grp == 0 ? 0 : (grp == 1 ? 2 : 1);
-                    const int kx = (seg * seg_blocks + kb % seg_blocks) * BK;
+                    const int grp = kb / seg_blocks, seg = F16 ? 0 : (grp == 0 ? 0 : (grp == 1 ? 2 : 1));
+                    const int kx = F16 ? kb * BK : (seg * seg_blocks + kb % seg_blocks) * BK;
                     tma_load_2d(a_dst, &tmA, kx, m0, fb);
                     tma_load_2d(b_dst, &tmB, kx, n0, fb);
                 }
@@ -238,7 +256,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     } else if (warp == 1) {
         // ---- MMA issuer ----------------------------------------------------------------------
         if (lane == 0) {
-            constexpr uint32_t idesc = idesc_i8(BM, BN);
+            constexpr uint32_t idesc = F16 ? idesc_f16(BM, BN) : idesc_i8(BM, BN);
             uint32_t it = 0, tile_iter = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++tile_iter) {
@@ -257,8 +275,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                     tc_fence_after();
                     // groups of k-blocks: H plane -> P1 (region 0), S plane -> P3 (region 1),
                     // L plane -> P2 (region 2), which may still be read by the previous epilogue
-                    const int grp = kb / seg_blocks;
-                    if (kb == 2 * seg_blocks) {
+                    const int grp = F16 ? 2 : kb / seg_blocks;  // the F16 accumulator is released with P2's barrier
+                    if (kb == (F16 ? 0 : 2 * seg_blocks)) {
                         if (!mbar_wait(smem_u32(&sh.tmem_empty_c), (tile_iter & 1) ^ 1, abort_flag)) {
                             ok = false;
                             break;
@@ -267,11 +285,15 @@ __global__ void __launch_bounds__(THREADS, 1)
                     }
                     const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
                     const uint64_t da = smem_desc(a_addr), db = smem_desc(a_addr + A_BYTES);
-                    const uint32_t tc = tmem + grp * BN;
+                    const uint32_t tc = tmem + (F16 ? 0 : grp * BN);
                     const bool first = (kb % seg_blocks) == 0;
 #pragma unroll
-                    for (int k = 0; k < BK / 32; ++k)
-                        umma_i8(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (first && k == 0) ? 0u : 1u);
+                    for (int k = 0; k < BK / 32; ++k) {  // 32 bytes of K per MMA (32 int8 or 16 half)
+                        if (F16)
+                            umma_f16(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (first && k == 0) ? 0u : 1u);
+                        else
+                            umma_i8(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (first && k == 0) ? 0u : 1u);
+                    }
                     umma_commit(smem_u32(&sh.empty[s]));
                 }
                 if (!ok) break;
@@ -325,6 +347,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             int T[CH][16];
 #pragma unroll
             for (int c = 0; c < CH; ++c) {
+                if (F16) break;
                 uint32_t pa[16], pb[16];
                 tmem_ld16(lane_base + half * HALF + c * 16, pa);
                 tmem_ld16(lane_base + BN + half * HALF + c * 16, pb);
@@ -335,20 +358,22 @@ __global__ void __launch_bounds__(THREADS, 1)
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&sh.tmem_empty));
-            // phase 2: P2, reads one chunk ahead of the arithmetic
+            // phase 2: P2 (the F16 accumulator), reads one chunk ahead of the arithmetic
+            const uint32_t base2 = lane_base + (F16 ? 0 : 2 * BN);
             uint32_t p2[2][16];
-            tmem_ld16(lane_base + 2 * BN + half * HALF, p2[0]);
+            tmem_ld16(base2 + half * HALF, p2[0]);
             tmem_wait_ld();
 #pragma unroll
             for (int c = 0; c < CH; ++c) {
                 const int col0 = half * HALF + c * 16;
-                if (c + 1 < CH) tmem_ld16(lane_base + 2 * BN + col0 + 16, p2[(c + 1) & 1]);
+                if (c + 1 < CH) tmem_ld16(base2 + col0 + 16, p2[(c + 1) & 1]);
                 float v[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    const int64_t N = 128ll * T[c][j] - 127ll * (int)p2[c & 1][j];
+                    const double N = F16 ? (double)__uint_as_float(p2[c & 1][j])
+                                         : (double)(128ll * T[c][j] - 127ll * (int)p2[c & 1][j]);
                     const double rrj = __shfl_sync(0xffffffffu, rrv[c], j);
-                    v[j] = (float)(((double)N * rqv) * rrj);
+                    v[j] = (float)((N * rqv) * rrj);
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
@@ -402,11 +427,11 @@ EncodeTiled encode_fn() {
     return fn;
 }
 
-// Tensor map of a [rows x (3 * Kp)] int8 limb matrix, 128 x 128-byte boxes, 128B swizzle.
-CUtensorMap limb_map(const int8_t* base, int rows, int Kp, int box_rows) {
+// Tensor map of a [rows x row_bytes] operand matrix, box_rows x 128-byte boxes, 128B swizzle.
+CUtensorMap limb_map(const int8_t* base, int rows, int row_bytes, int box_rows) {
     CUtensorMap m;
-    cuuint64_t dims[2] = {(cuuint64_t)(3 * Kp), (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)(3 * Kp)};
+    cuuint64_t dims[2] = {(cuuint64_t)row_bytes, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)row_bytes};
     cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(base), dims, strides, box, estr,
@@ -421,16 +446,19 @@ CUtensorMap limb_map(const int8_t* base, int rows, int Kp, int box_rows) {
 size_t corr_tc_smem() { return (size_t)STAGES * STAGE_BYTES + STAGING_BYTES + 1024; }
 
 void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
-                    const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s) {
+                    const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s,
+                    bool f16) {
     if (nq <= 0 || R <= 0) return;
     if (Kp % BK != 0 || (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15))
         fail(SGR_ERR_INVALID_ARGUMENT, "tensor-core correlation: misaligned operands");
-    const CUtensorMap ta = limb_map(A, nq, Kp, BM), tb = limb_map(B, R, Kp, BN);
+    const int row_bytes = (f16 ? 2 : 3) * Kp;
+    const CUtensorMap ta = limb_map(A, nq, row_bytes, BM), tb = limb_map(B, R, row_bytes, BN);
     const size_t smem = corr_tc_smem();
-    SGR_CUDA(cudaFuncSetAttribute(corr_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto kern = f16 ? corr_tc_kernel<true> : corr_tc_kernel<false>;
+    SGR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long tiles = (long)((nq + BM - 1) / BM) * ((R + BN - 1) / BN);
     const int grid = (int)std::min<long>(tiles, device_sm_count());
-    corr_tc_kernel<<<grid, THREADS, smem, s>>>(ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status);
+    kern<<<grid, THREADS, smem, s>>>(ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status);
     SGR_LAUNCH_CHECK();
     count_launch();
 }

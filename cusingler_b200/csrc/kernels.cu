@@ -18,6 +18,8 @@
 #include <cstdio>
 #include <type_traits>
 
+#include <cuda_fp16.h>
+
 #include "kernels.cuh"
 #include "sgr_internal.h"
 #include "stl_order.h"
@@ -31,6 +33,7 @@ __device__ __forceinline__ int stage_d(const unsigned char* stage, int mode, int
         const int8_t* s = reinterpret_cast<const int8_t*>(stage);
         return 128 * (int)s[p] + (int)s[Kp + p];
     }
+    if (mode == RANK_F16) return __half2int_rn(reinterpret_cast<const __half*>(stage)[p]);
     return reinterpret_cast<const int16_t*>(stage)[p];
 }
 
@@ -42,6 +45,8 @@ __device__ __forceinline__ void stage_put(unsigned char* stage, int mode, int Kp
         st[p] = (int8_t)h;
         st[Kp + p] = (int8_t)l;
         st[2 * Kp + p] = (int8_t)s;
+    } else if (mode == RANK_F16) {
+        reinterpret_cast<__half*>(stage)[p] = __int2half_rn(d);
     } else {
         reinterpret_cast<int16_t*>(stage)[p] = (int16_t)d;
     }
@@ -126,6 +131,10 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
                     st[plane * wpp + w] = left >= 4 ? full : left <= 0 ? 0u : full & ((1u << (8 * left)) - 1u);
                 }
             }
+        } else if (a.out_mode == RANK_F16) {
+            __half* st = reinterpret_cast<__half*>(stage);
+            const __half h0 = __int2half_rn(d0), z = __int2half_rn(0);
+            for (int p = lane; p < Kp; p += 32) st[p] = p < G ? h0 : z;
         } else {
             int16_t* st = reinterpret_cast<int16_t*>(stage);
             for (int p = lane; p < Kp; p += 32) st[p] = p < G ? (int16_t)d0 : (int16_t)0;

@@ -45,7 +45,9 @@ struct RankItem {
     uint32_t pad;
 };
 
-enum RankOut { RANK_LIMBS = 0, RANK_D16 = 1 };
+// LIMBS: int8 planes H | L | S (3 * Kp bytes per row); D16: int16 d; F16: d as IEEE half (exact for
+// |d| <= 2048), the operand of the FP16 correlation variant.
+enum RankOut { RANK_LIMBS = 0, RANK_D16 = 1, RANK_F16 = 2 };
 enum F32Norm { NORM_NONE = 0, NORM_SEQ = 1, NORM_TREE128 = 2 };
 
 struct RankLaunch {
@@ -146,7 +148,8 @@ void launch_ft_select(const FtGroup* groups, const FtSelItem* items, uint32_t n_
 // Exact score-step correlation on the tensor cores (corr_tc.cu): A/B are LIMBS rows of 3 * Kp bytes.
 size_t corr_tc_smem();
 void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
-                    const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s);
+                    const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s,
+                    bool f16 = false);
 
 // Persistent exact fine-tune (finetune.cu).
 struct FtPersistentArgs {

@@ -139,7 +139,10 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
  * correlations per block of queries (small blocks are read back from L2 by the selection); what 3:
  * 1 (default) lets the fine-tune row scan keep each value run's count and e-sum in one packed
  * 32-bit word when the trained reference allows it, 0 always uses the two-register scan.
- * No choice changes any result. */
+ * No choice above changes any result.  what 4 (exact mode only; no counterpart in the reference):
+ * 1 runs the score-step correlation on FP16 operands with FP32 accumulation (one tensor-core
+ * product instead of three INT8 products; scores are not exact, their error against the exact
+ * scores is reported by the benchmark), 0 (default) the exact INT8 form. */
 sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value);
 sgr_status sgr_reset_timings(sgr_ctx* ctx);
 

@@ -108,3 +108,23 @@ def test_final_labels_both_row_scans(kind, packed):
     final, rounds = a.finetune(prob.qry, res["flags"].astype(np.uint8))
     assert np.array_equal(final, res["final"])
     assert np.array_equal(rounds, res["rounds"])
+
+
+@pytest.mark.parametrize("kind", ["tiny", "small"])
+def test_fp16_variant_close_to_exact(kind):
+    """The FP16-operand correlation variant (FP32 accumulation, not exact): every score within 1e-4
+    of the exact score (a bound of K x 2^-24 relative to the Cauchy-Schwarz bound of the sum), NaN
+    where the exact score is NaN, and first labels that differ only at near-ties."""
+    a, prob = annotator(kind, abi.MODE_EXACT)
+    raw_exact = a.debug_scores(prob.qry)
+    f_exact, s_exact, _ = a.score_first(prob.qry)
+    a.set_tuning(4, 1)
+    raw_f16 = a.debug_scores(prob.qry)
+    f16, s16, _ = a.score_first(prob.qry)
+    a.set_tuning(4, 0)
+    assert np.array_equal(np.isnan(raw_exact), np.isnan(raw_f16))
+    assert np.nanmax(np.abs(raw_f16.astype(np.float64) - raw_exact)) < 1e-4
+    assert np.nanmax(np.abs(s16.astype(np.float64) - s_exact)) < 1e-4
+    assert (f16 == f_exact).mean() >= 0.99
+    # back on the exact form, bit-exact again
+    assert H.ulp_diff(a.debug_scores(prob.qry), raw_exact).max() == 0
