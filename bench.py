@@ -40,6 +40,16 @@ FALLBACK_HBM_GBS = 6650.0
 FALLBACK_BF16_TFLOPS = 1590.0
 
 
+# DRAM bytes per query row of each score-step kernel, from one ncu capture of the 8,192-query case
+# (profiles/corr_tc_mid_8192q.md, select_first_mid_8192q.md, rank_kernel_mid_8192q.md: read +
+# write); a launch's traffic is this times its query rows (each row's traffic is the same).
+TRAFFIC_PER_QUERY = {
+    "corr": (1.183566e9 + 0.650477e9) / 8192,
+    "select": (0.655499e9 + 5.373952e6) / 8192,
+    "rank": (0.098896e9 + 7.392512e6) / 8192,
+}
+
+
 def peaks():
     try:
         with open(PEAKS_PATH) as f:
@@ -170,6 +180,9 @@ def main():
     ap.add_argument("--min-confidence", type=float, default=0.98)
     ap.add_argument("--check-fraction", type=float, default=0.01)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ft-heavy", type=int, default=0,
+                    help="pin the fine-tune split threshold and skip the autotuner (profiling runs)")
+    ap.add_argument("--ft-warps", type=int, default=8, help="with --ft-heavy: warps per work-queue CTA")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -252,6 +265,12 @@ def main():
     tuning = {}
 
     def tune(learned):
+        if args.ft_heavy:
+            ann.set_tuning(0, args.ft_warps)
+            ann.set_tuning(1, args.ft_heavy)
+            tuning["learned" if learned else "plain"] = {"pinned": True, "ft_warps": args.ft_warps,
+                                                          "ft_heavy": args.ft_heavy, "score_chunk_mb": 1024}
+            return
         tuning["learned" if learned else "plain"] = ann.autotune(
             tune_sample, learned=learned, min_confidence=args.min_confidence, check_fraction=args.check_fraction)
 
@@ -357,20 +376,23 @@ def main():
     rank_launch_ms = tm["rank_ms"] / max(1, tm["rank_launches"])
     rank_bytes_launch = tm["rank_bytes"] / max(1, tm["rank_launches"])
     int8_peak = 2 * bf16  # dense int8 = 2x dense bf16 on B200; no int8 figure is measured
+    rows_corr = qry.n_rows / max(1, tm["corr_launches"] / steps)
+    rows_rank = qry.n_rows / max(1, tm["rank_launches"] / steps)
+    rows_sel = qry.n_rows / max(1, tm["select_launches"] / steps)
     roof_corr = {"kernel": "score-step correlation", "bound": "tensor",
                  "achieved": corr_ops_launch / (corr_launch_ms / 1000) / 1e12, "peak": int8_peak,
-                 "unit": "TFLOP/s", "traffic": None,
+                 "unit": "TFLOP/s", "traffic": TRAFFIC_PER_QUERY["corr"] * rows_corr,
                  "peak_note": f"int8 dense = 2 x {src} bf16 cuBLAS ({bf16} TFLOP/s)"}
     roof_corr["frac"] = roof_corr["achieved"] / roof_corr["peak"]
     roof_rank = {"kernel": "gather + rank", "bound": "hbm",
                  "achieved": rank_bytes_launch / (rank_launch_ms / 1000) / 1e9, "peak": hbm, "unit": "GB/s",
-                 "traffic": None, "peak_note": f"{src} copy bandwidth"}
+                 "traffic": TRAFFIC_PER_QUERY["rank"] * rows_rank, "peak_note": f"{src} copy bandwidth"}
     roof_rank["frac"] = roof_rank["achieved"] / roof_rank["peak"]
     sel_launch_ms = tm["select_ms"] / max(1, tm["select_launches"])
     sel_bytes_launch = tm["select_bytes"] / max(1, tm["select_launches"])
     roof_sel = {"kernel": "per-label quantile select", "bound": "hbm",
                 "achieved": sel_bytes_launch / (sel_launch_ms / 1000) / 1e9, "peak": hbm, "unit": "GB/s",
-                "traffic": None, "peak_note": f"{src} copy bandwidth"}
+                "traffic": TRAFFIC_PER_QUERY["select"] * rows_sel, "peak_note": f"{src} copy bandwidth"}
     roof_sel["frac"] = roof_sel["achieved"] / roof_sel["peak"]
     # the dominant kernel with a roofline of its own: fine-tune is reported in stages_ms (it is bound by
     # issue and L1 gathers over L2-resident data, not by HBM or the tensor pipe)
