@@ -125,6 +125,7 @@ struct sgr_ctx {
     DevBuf<int32_t> d_gene_thre;
     DevBuf<LabelQ> d_lq_label;
     DevBuf<int> next_cell;
+    DevBuf<uint8_t> ft_row_mask;   // rows of the listed cells (learned form's fine-tune)
     int corr_f16 = 0;              // tuning: score-step correlation on FP16 operands (not exact)
     DevBuf<uint16_t> ref_f16;      // reference ranks as IEEE half rows [R][Kp]
     bool ref_f16_ready = false;
@@ -379,17 +380,17 @@ void rank_rows(sgr_ctx* ctx, const DevCsr& m, const RankGroup& grp, int out_mode
 
 // Compacts a device CSR to the columns with map >= 0 into (data, indices, indptr) buffers.
 void filter_csr(sgr_ctx* ctx, const DevCsr& m, const int32_t* map, DevBuf<float>& od, DevBuf<int32_t>& oi,
-                DevBuf<int32_t>& op) {
+                DevBuf<int32_t>& op, const uint8_t* row_mask = nullptr) {
     ctx->counts.ensure(m.n_rows + 1);
     op.ensure((size_t)m.n_rows + 1);
-    launch_filter_count(m.indptr, m.indices, m.n_rows, m.n_cols, map, ctx->counts.p, ctx->stream);
+    launch_filter_count(m.indptr, m.indices, m.n_rows, m.n_cols, map, ctx->counts.p, ctx->stream, row_mask);
     launch_exclusive_scan(ctx->counts.p, op.p, m.n_rows, nullptr, ctx->stream);
     int32_t total = 0;
     SGR_CUDA(cudaMemcpyAsync(&total, op.p + m.n_rows, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     SGR_CUDA(cudaStreamSynchronize(ctx->stream));
     od.ensure(std::max<int32_t>(total, 1));
     oi.ensure(std::max<int32_t>(total, 1));
-    launch_filter_fill(m.data, m.indptr, m.indices, m.n_rows, m.n_cols, map, op.p, od.p, oi.p, ctx->stream);
+    launch_filter_fill(m.data, m.indptr, m.indices, m.n_rows, m.n_cols, map, op.p, od.p, oi.p, ctx->stream, row_mask);
 }
 
 std::vector<int32_t> position_map(const std::vector<int32_t>& colmap, const std::vector<uint32_t>& genes,
@@ -926,7 +927,18 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     const Markers& mk = ctx->mk;
     const uint32_t Q = q.n_rows, L = mk.n_labels, Wt = ctx->Wt;
     const int sp_ft = ctx->prof.begin(ST_FT, s);
-    filter_csr(ctx, q, ctx->qry_map_thre.p, ctx->qf_data, ctx->qf_indices, ctx->qf_indptr);
+    // thre-pool rows of the cells to fine-tune (all cells, or only the listed ones)
+    const uint8_t* row_mask = nullptr;
+    if (cell_list) {
+        int n = 0;
+        SGR_CUDA(cudaMemcpyAsync(&n, n_list, sizeof(int), cudaMemcpyDeviceToHost, s));
+        SGR_CUDA(cudaStreamSynchronize(s));
+        uint8_t* mask = ctx->ft_row_mask.ensure(std::max<uint32_t>(Q, 1));
+        SGR_CUDA(cudaMemsetAsync(mask, 0, Q, s));
+        launch_mark_rows(cell_list, n, mask, s);
+        row_mask = mask;
+    }
+    filter_csr(ctx, q, ctx->qry_map_thre.p, ctx->qf_data, ctx->qf_indices, ctx->qf_indptr, row_mask);
     uint32_t max_label = 1;
     std::vector<LabelQ> lq(L);
     for (uint32_t l = 0; l < L; ++l) {

@@ -222,11 +222,16 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
 
 // ---- CSR compaction --------------------------------------------------------------------------
 
+// row_mask (optional): rows with mask 0 are left empty.
 __global__ void filter_count_kernel(const int32_t* indptr, const int32_t* indices, uint32_t n_rows, uint32_t n_cols,
-                                    const int32_t* map, int32_t* counts) {
+                                    const int32_t* map, int32_t* counts, const uint8_t* row_mask) {
     const int lane = threadIdx.x & 31;
     for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n_rows;
          row += (gridDim.x * blockDim.x) >> 5) {
+        if (row_mask && !row_mask[row]) {
+            if (lane == 0) counts[row] = 0;
+            continue;
+        }
         int cnt = 0;
         for (int i = indptr[row] + lane; i < indptr[row + 1]; i += 32) {
             const int c = indices[i];
@@ -239,10 +244,11 @@ __global__ void filter_count_kernel(const int32_t* indptr, const int32_t* indice
 
 __global__ void filter_fill_kernel(const float* data, const int32_t* indptr, const int32_t* indices, uint32_t n_rows,
                                    uint32_t n_cols, const int32_t* map, const int32_t* out_ptr, float* out_data,
-                                   int32_t* out_indices) {
+                                   int32_t* out_indices, const uint8_t* row_mask) {
     const int lane = threadIdx.x & 31;
     for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n_rows;
          row += (gridDim.x * blockDim.x) >> 5) {
+        if (row_mask && !row_mask[row]) continue;
         int base = out_ptr[row];
         const int beg = indptr[row], end = indptr[row + 1];
         for (int i0 = beg; i0 < end; i0 += 32) {
@@ -588,10 +594,23 @@ void launch_rank(const RankLaunch& a, cudaStream_t s) {
 }
 
 void launch_filter_count(const int32_t* indptr, const int32_t* indices, uint32_t n_rows, uint32_t n_cols,
-                         const int32_t* map, int32_t* counts, cudaStream_t s) {
+                         const int32_t* map, int32_t* counts, cudaStream_t s, const uint8_t* row_mask) {
     if (!n_rows) return;
     const unsigned blocks = std::min<unsigned>((n_rows + 7) / 8, sm_count() * 16);
-    filter_count_kernel<<<blocks, 256, 0, s>>>(indptr, indices, n_rows, n_cols, map, counts);
+    filter_count_kernel<<<blocks, 256, 0, s>>>(indptr, indices, n_rows, n_cols, map, counts, row_mask);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
+
+namespace {
+__global__ void mark_rows_kernel(const int32_t* list, int n, uint8_t* mask) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) mask[list[i]] = 1;
+}
+}  // namespace
+
+void launch_mark_rows(const int32_t* list, int n, uint8_t* mask, cudaStream_t s) {
+    if (n <= 0) return;
+    mark_rows_kernel<<<std::min((n + 255) / 256, sm_count() * 4), 256, 0, s>>>(list, n, mask);
     SGR_LAUNCH_CHECK();
     count_launch();
 }
@@ -604,11 +623,11 @@ void launch_exclusive_scan(const int32_t* in, int32_t* out, uint32_t n, int32_t*
 
 void launch_filter_fill(const float* data, const int32_t* indptr, const int32_t* indices, uint32_t n_rows,
                         uint32_t n_cols, const int32_t* map, const int32_t* out_ptr, float* out_data,
-                        int32_t* out_indices, cudaStream_t s) {
+                        int32_t* out_indices, cudaStream_t s, const uint8_t* row_mask) {
     if (!n_rows) return;
     const unsigned blocks = std::min<unsigned>((n_rows + 7) / 8, sm_count() * 16);
     filter_fill_kernel<<<blocks, 256, 0, s>>>(data, indptr, indices, n_rows, n_cols, map, out_ptr, out_data,
-                                              out_indices);
+                                              out_indices, row_mask);
     SGR_LAUNCH_CHECK();
     count_launch();
 }

@@ -76,11 +76,15 @@ void launch_rank(const RankLaunch& a, cudaStream_t s);
 
 // Compact a CSR to the columns with map[c] >= 0 (new column = map[c]); two passes.
 void launch_filter_count(const int32_t* indptr, const int32_t* indices, uint32_t n_rows, uint32_t n_cols,
-                         const int32_t* map, int32_t* counts, cudaStream_t s);
+                         const int32_t* map, int32_t* counts, cudaStream_t s,
+                         const uint8_t* row_mask = nullptr);
+// mask[list[i]] = 1 for i < n (list entries must be valid rows of mask).
+void launch_mark_rows(const int32_t* list, int n, uint8_t* mask, cudaStream_t s);
 void launch_exclusive_scan(const int32_t* in, int32_t* out, uint32_t n, int32_t* scratch, cudaStream_t s);
 void launch_filter_fill(const float* data, const int32_t* indptr, const int32_t* indices, uint32_t n_rows,
                         uint32_t n_cols, const int32_t* map, const int32_t* out_ptr, float* out_data,
-                        int32_t* out_indices, cudaStream_t s);
+                        int32_t* out_indices, cudaStream_t s,
+                        const uint8_t* row_mask = nullptr);
 
 // ---- score-step correlation on CUDA cores -------------------------------------------------------
 //
