@@ -8,7 +8,7 @@
 // forward and backward products); every product accumulates in FP32.  All kernels are hand-written:
 // a tiled CUDA-core GEMM with strided operands (the layers are at most 256 wide, far too small to
 // keep tensor cores busy), fused bias + GELU epilogues, softmax cross-entropy, bias reductions and
-// AdamW.
+// AdamW.  Inference (predict) runs the three products on the tensor cores instead.
 
 #include <cuda_bf16.h>
 
@@ -77,6 +77,87 @@ __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const TA
             C[m * ldc + n] = v;
         }
     }
+}
+
+// Inference product on the tensor cores (mma.sync m16n8k16, BF16 inputs, FP32 accumulation):
+// C[m][n] = act(sum_k A[m][k] W[n][k] + bias[n]) with A FP32 (row-major, lda) and W BF16 (row-major
+// [N][K], ldw).  Each A value is split into BF16 hi + lo (a - hi - lo is within 2^-16 |a|), so two
+// products per tile keep the FP32 activations' precision.  gelu: apply GELU after the bias.
+// Block tile 128 x 64 (8 warps, each 32 x 32), K in steps of 16; shared rows padded to 24 values so
+// the fragment loads are conflict-free.
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(256) gemm_tc_kernel(int M, int N, int K, const float* A, int64_t lda,
+                                                      const __nv_bfloat16* W, int64_t ldw, const float* bias,
+                                                      float* C, int64_t ldc, int gelu) {
+    constexpr int P = 24;  // padded row length (bf16 values)
+    __shared__ __align__(16) __nv_bfloat16 Ahi[128 * P], Alo[128 * P], Ws[64 * P];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;  // warp tile origin in the block tile
+    const int m0 = blockIdx.y * 128, n0 = blockIdx.x * 64;
+    float acc[2][4][4] = {};
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        for (int i = threadIdx.x; i < 128 * 16; i += 256) {
+            const int r = i >> 4, c = i & 15;
+            const int m = m0 + r, k = k0 + c;
+            const float a = (m < M && k < K) ? A[m * lda + k] : 0.f;
+            const __nv_bfloat16 hi = __float2bfloat16_rn(a);
+            Ahi[r * P + c] = hi;
+            Alo[r * P + c] = __float2bfloat16_rn(a - __bfloat162float(hi));
+        }
+        for (int i = threadIdx.x; i < 64 * 16; i += 256) {
+            const int r = i >> 4, c = i & 15;
+            const int n = n0 + r, k = k0 + c;
+            Ws[r * P + c] = (n < N && k < K) ? W[n * ldw + k] : __float2bfloat16_rn(0.f);
+        }
+        __syncthreads();
+        uint32_t bf[4][2];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const __nv_bfloat16* w = Ws + (wn + 8 * j + g) * P + 2 * t;
+            bf[j][0] = *reinterpret_cast<const uint32_t*>(w);
+            bf[j][1] = *reinterpret_cast<const uint32_t*>(w + 8);
+        }
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+            const __nv_bfloat16* As = part ? Alo : Ahi;
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const __nv_bfloat16* a = As + (wm + 16 * i + g) * P + 2 * t;
+                const uint32_t af[4] = {*reinterpret_cast<const uint32_t*>(a),
+                                        *reinterpret_cast<const uint32_t*>(a + 8 * P),
+                                        *reinterpret_cast<const uint32_t*>(a + 8),
+                                        *reinterpret_cast<const uint32_t*>(a + 8 * P + 8)};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], af, bf[j]);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int m = m0 + wm + 16 * i + g + (e >= 2 ? 8 : 0);
+                const int n = n0 + wn + 8 * j + 2 * t + (e & 1);
+                if (m >= M || n >= N) continue;
+                float v = acc[i][j][e] + bias[n];
+                if (gelu) v = 0.5f * v * (1.f + erff(v * 0.70710678118654752f));
+                C[m * ldc + n] = v;
+            }
 }
 
 // dZ = dH * GELU'(Z), GELU'(z) = Phi(z) + z phi(z)
@@ -359,11 +440,28 @@ void Mlp::features(const float* scores, int Q, float* X, uint8_t* bad, cudaStrea
     count_launch();
 }
 
+// Inference forward of B rows of X into logits on the tensor cores (no activations kept).
+void Mlp::forward_infer(const float* X, int B, cudaStream_t s) {
+    h1.ensure((size_t)B * H);
+    h2.ensure((size_t)B * H);
+    logits.ensure((size_t)B * L);
+    const __nv_bfloat16* W = wb.p;
+    auto run = [&](int N, int K, const float* A, const __nv_bfloat16* w, const float* b, float* C, int gelu) {
+        dim3 grid((N + 63) / 64, (B + 127) / 128);
+        gemm_tc_kernel<<<grid, 256, 0, s>>>(B, N, K, A, K, w, K, b, C, N, gelu);
+        SGR_LAUNCH_CHECK();
+        count_launch();
+    };
+    run(H, L, X, W + off_w1, w.p + off_b1, h1.p, 1);
+    run(H, H, h1.p, W + off_w2, w.p + off_b2, h2.p, 1);
+    run(L, H, h2.p, W + off_w3, w.p + off_b3, logits.p, 0);
+}
+
 void Mlp::predict(const float* X, int Q, int32_t* label, float* conf, cudaStream_t s) {
     const int chunk = 1 << 16;
     for (int q0 = 0; q0 < Q; q0 += chunk) {
         const int n = std::min(chunk, Q - q0);
-        forward(X + (size_t)q0 * L, n, s);
+        forward_infer(X + (size_t)q0 * L, n, s);
         predict_kernel<<<(n + 255) / 256, 256, 0, s>>>(logits.p, n, L, label + q0, conf + q0);
         SGR_LAUNCH_CHECK();
         count_launch();

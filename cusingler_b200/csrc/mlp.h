@@ -19,6 +19,8 @@ struct Mlp {
     void init(int L, int H, uint64_t seed, cudaStream_t s);
     void set_params(const float* host, cudaStream_t s);
     void forward(const float* X, int B, cudaStream_t s);
+    // Inference forward on the tensor cores (BF16 hi/lo split of the activations); logits only.
+    void forward_infer(const float* X, int B, cudaStream_t s);
     void backward(const float* X, const int32_t* y, int B, cudaStream_t s);
     void adamw(float lr, float b1, float b2, float eps, float wd, cudaStream_t s);
     void features(const float* scores, int Q, float* X, uint8_t* bad, cudaStream_t s);

@@ -32,6 +32,15 @@ def gelu_grad(z):
     return 0.5 * (1 + erf(z / np.sqrt(2))) + z * np.exp(-0.5 * z * z) / np.sqrt(2 * np.pi)
 
 
+def forward(params, L, H, X):
+    """Logits of the network in float64 with BF16-rounded weights."""
+    P = unpack(params, L, H)
+    W1, W2, W3 = (bf16(P[k].astype(np.float32)).astype(np.float64) for k in ("W1", "W2", "W3"))
+    h1 = gelu(X.astype(np.float64) @ W1.T + P["b1"])
+    h2 = gelu(h1 @ W2.T + P["b2"])
+    return h2 @ W3.T + P["b3"]
+
+
 def loss_and_grads(params, L, H, X, y):
     P = unpack(params, L, H)
     W1, W2, W3 = (bf16(P[k].astype(np.float32)).astype(np.float64) for k in ("W1", "W2", "W3"))

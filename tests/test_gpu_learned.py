@@ -35,6 +35,28 @@ def test_gradients_match_oracle():
     assert np.max(np.abs(g - ref_g)) < 1e-4 * np.max(np.abs(ref_g)) + 1e-7
 
 
+def test_inference_matches_oracle():
+    """mlp_predict (tensor-core inference, BF16 hi/lo split of the FP32 activations) against the
+    oracle's float64 forward: confidences within 1e-4, labels equal wherever the top two logits are
+    not within 1e-3 of each other."""
+    a, prob = _trained("tiny")
+    L = len(prob.label_names)
+    rng = np.random.default_rng(4)
+    scores = rng.uniform(0.0, 0.9, (3000, L)).astype(np.float32)
+    targets = rng.integers(0, L, 3000).astype(np.int32)
+    a.mlp_train(scores, targets, epochs=3, batch=256, seed=2)
+    lab, conf = a.mlp_predict(scores)
+    params, Lp, Hd = a.mlp_params()
+    X = np.maximum((scores - scores.max(1, keepdims=True)) * 20, -8).astype(np.float32)
+    logits = M.forward(params, Lp, Hd, X)
+    z = logits - logits.max(1, keepdims=True)
+    ref_conf = 1.0 / np.exp(z).sum(1)
+    assert np.max(np.abs(conf - ref_conf)) < 1e-4
+    top2 = np.sort(logits, 1)[:, -2:]
+    clear = (top2[:, 1] - top2[:, 0]) > 1e-3
+    assert np.array_equal(lab[clear], logits.argmax(1)[clear])
+
+
 def test_training_learns_and_confident_proposals_agree():
     a, prob = _trained("tiny")
     first, scores, flags = a.score_first(prob.qry)
