@@ -4,7 +4,8 @@
 // Reference kernels restated here (STOmics/cusingler src/cusingler.cu):
 //   csr2dense (204-281) + get_device_ref_lines (566-577) + csrFilter codes (src/io.cpp:470-523)
 //       -> rank_kernel: one warp per cell row gathers the row's marker entries straight from the
-//          CSR, sorts them in shared memory and writes tie-averaged doubled centred ranks.
+//          CSR, counts each entry's #less / #equal through 256 value buckets in shared memory and
+//          writes tie-averaged doubled centred ranks.
 //   rankdata_bin3 / rankdata_batch / rankdata (745-801, 601-625, 158-179)
 //       -> the same half-integer ranks 1 + #less + (#equal - 1)/2, as d = 2*rank - (G+1).
 //   spearman (918-945)        -> corr_simt_kernel (fp32ref: fma chain over genes in order).
@@ -52,11 +53,21 @@ __device__ __forceinline__ void stage_put(unsigned char* stage, int mode, int Kp
     }
 }
 
+// Bucket of a rank key's value on the map (x - fmin) * scale (0 for NaN and a zero scale).
+__device__ __forceinline__ int rank_bucket(uint64_t key, float fmin, float scale) {
+    const float t = (key_float((uint32_t)(key >> 32)) - fmin) * scale;
+    return t >= 0.f ? min(255, (int)t) : 0;
+}
+
 __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    // per warp: keys (cap x 8 B) | values by bucket (cap x 4 B) | bucket counts | bucket cursors | stage
     uint64_t* keys = reinterpret_cast<uint64_t*>(smem + (size_t)warp * warp_bytes);
-    unsigned char* stage = reinterpret_cast<unsigned char*>(keys + a.cap);
+    uint32_t* vals = reinterpret_cast<uint32_t*>(keys + a.cap);
+    int* hist = reinterpret_cast<int*>(vals + a.cap);
+    int* cursor = hist + 256;
+    unsigned char* stage = reinterpret_cast<unsigned char*>(cursor + 256);
     const uint32_t n_items = a.n_items_dev ? (uint32_t)*a.n_items_dev : a.n_items;
     for (uint32_t item = blockIdx.x * wpb + warp; item < n_items; item += gridDim.x * wpb) {
         RankItem it;
@@ -107,12 +118,44 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
             if (lane == 0) a.overflow[atomicAdd(a.n_overflow, 1)] = it;
             continue;
         }
-        if (fits && k > 1) {
-            int n = 1;
-            while (n < k) n <<= 1;
-            for (int i = k + lane; i < n; i += 32) keys[i] = ~0ull;
+        // bucket counting instead of a sort: 256 buckets over a linear map of [min, max] of the
+        // entries' value keys (monotone, so equal values share a bucket); every entry of a lower
+        // bucket is smaller, and the rest of #less / #equal is counted inside the entry's bucket
+        float fmin = 0.f, scale = 0.f;
+        if (fits && k > 0) {
+            uint32_t kmin = 0xffffffffu, kmax = 0u;
+            for (int j = lane; j < k; j += 32) {
+                const uint32_t u = (uint32_t)(keys[j] >> 32);
+                kmin = min(kmin, u);
+                kmax = max(kmax, u);
+            }
+            kmin = __reduce_min_sync(FULL, kmin);
+            kmax = __reduce_max_sync(FULL, kmax);
+            fmin = key_float(kmin);
+            const float span = key_float(kmax) - fmin;
+            scale = (span > 0.f && span < 1e30f) ? 256.0f / span : 0.f;
+            for (int b = lane; b < 256; b += 32) hist[b] = 0;
             __syncwarp();
-            warp_bitonic(keys, n, lane);
+            for (int j = lane; j < k; j += 32) atomicAdd(&hist[rank_bucket(keys[j], fmin, scale)], 1);
+            __syncwarp();
+            int c[8], sum = 0;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                c[t] = hist[8 * lane + t];
+                sum += c[t];
+            }
+            int acc = warp_incl_scan(sum, lane) - sum;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                cursor[8 * lane + t] = acc;
+                acc += c[t];
+            }
+            __syncwarp();
+            for (int j = lane; j < k; j += 32) {
+                const uint64_t key = keys[j];
+                vals[atomicAdd(&cursor[rank_bucket(key, fmin, scale)], 1)] = (uint32_t)(key >> 32);
+            }
+            __syncwarp();  // cursor[b] is now the end of bucket b
         }
 
         // 2) every position of the subset starts as an implicit zero: rank (G-k+1)/2, d = -k;
@@ -147,8 +190,15 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
             for (int j = lane; j < k; j += 32) {
                 const uint64_t key = keys[j];
                 const uint32_t hv = (uint32_t)(key >> 32);
-                const int lo = lower_hi(keys, k, hv), hi = upper_hi(keys, k, hv);
-                const int d = G - 2 * k + 2 * lo + (hi - lo);
+                const int b = rank_bucket(key, fmin, scale);
+                const int e = cursor[b];
+                int less = e - hist[b], eq = 0;  // entries of lower buckets, then this bucket's
+                for (int t = e - hist[b]; t < e; ++t) {
+                    const uint32_t u = vals[t];
+                    less += u < hv;
+                    eq += u == hv;
+                }
+                const int d = G - 2 * k + 2 * less + eq;
                 stage_put(stage, a.out_mode, Kp, (int)(uint32_t)key, d);
                 sq += (int64_t)d * d;
             }
@@ -557,7 +607,7 @@ int sm_count() { return device_sm_count(); }
 namespace {
 void launch_rank_tier(const RankLaunch& a, long max_blocks, cudaStream_t s) {
     const int stage_bytes = a.out_mode == RANK_LIMBS ? 3 * a.max_Kp : 2 * a.max_Kp;
-    const int warp_bytes = ((a.cap * 8 + stage_bytes) + 15) & ~15;
+    const int warp_bytes = ((a.cap * 12 + 2 * 256 * 4 + stage_bytes) + 15) & ~15;
     const int budget = 200 * 1024;
     int wpb = budget / warp_bytes;
     if (wpb > 8) wpb = 8;
