@@ -170,7 +170,8 @@ __device__ int cta_gene_set(const FtPersistentArgs& a, const uint8_t* top, int n
 // stored ones, SENT outside S.  CTA-wide (the ranking itself by warp 0); sets *kq, *nq, *rq.
 template <int NW>
 __device__ void cta_query_ranks(const FtPersistentArgs& a, int cell, int nS, const uint32_t* bits, int* eqv,
-                                uint64_t* qkeys, int* kq_out, int64_t* nq_out, double* rq_out) {
+                                uint64_t* qkeys, uint32_t* qvals, int* qhist, int* kq_out, int64_t* nq_out,
+                                double* rq_out) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int g = tid; g < a.Wt; g += NW * 32) eqv[g] = (bits[g >> 5] >> (g & 31)) & 1u ? 0 : SENT;
     if (tid == 0) eqv[a.Wt] = SENT;  // the pad entries' gene id
@@ -199,16 +200,55 @@ __device__ void cta_query_ranks(const FtPersistentArgs& a, int cell, int nS, con
         __syncwarp();
         int64_t sq = 0;
         if (k <= a.capq) {
-            int n = 1;
-            while (n < k) n <<= 1;
-            for (int i = k + lane; i < n; i += 32) qkeys[i] = ~0ull;
+            // #less / #equal through 256 value buckets (as in the score step's rank kernel)
+            int* cnt = qhist;
+            int* cursor = qhist + 256;
+            uint32_t kmin = 0xffffffffu, kmax = 0u;
+            for (int j = lane; j < k; j += 32) {
+                const uint32_t u = (uint32_t)(qkeys[j] >> 32);
+                kmin = min(kmin, u);
+                kmax = max(kmax, u);
+            }
+            kmin = __reduce_min_sync(FULL, kmin);
+            kmax = __reduce_max_sync(FULL, kmax);
+            const float fmin = key_float(kmin), span = key_float(kmax) - fmin;
+            const float scale = (span > 0.f && span < 1e30f) ? 256.0f / span : 0.f;
+            auto bucket = [&](uint32_t u) {
+                const float t = (key_float(u) - fmin) * scale;
+                return t >= 0.f ? min(255, (int)t) : 0;
+            };
+            for (int b = lane; b < 256; b += 32) cnt[b] = 0;
             __syncwarp();
-            if (k > 1) warp_bitonic(qkeys, n, lane);
+            for (int j = lane; j < k; j += 32) atomicAdd(&cnt[bucket((uint32_t)(qkeys[j] >> 32))], 1);
+            __syncwarp();
+            int c[8], sum = 0;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                c[t] = cnt[8 * lane + t];
+                sum += c[t];
+            }
+            int acc = warp_incl_scan(sum, lane) - sum;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                cursor[8 * lane + t] = acc;
+                acc += c[t];
+            }
+            __syncwarp();
+            for (int j = lane; j < k; j += 32) {
+                const uint32_t u = (uint32_t)(qkeys[j] >> 32);
+                qvals[atomicAdd(&cursor[bucket(u)], 1)] = u;
+            }
+            __syncwarp();
             for (int j = lane; j < k; j += 32) {
                 const uint64_t key = qkeys[j];
                 const uint32_t hv = (uint32_t)(key >> 32);
-                const int lo = lower_hi(qkeys, k, hv), hi = upper_hi(qkeys, k, hv);
-                const int e = nS - k + 2 * lo + (hi - lo);
+                const int b = bucket(hv), end_b = cursor[b];
+                int less = end_b - cnt[b], eq = 0;
+                for (int t = end_b - cnt[b]; t < end_b; ++t) {
+                    less += qvals[t] < hv;
+                    eq += qvals[t] == hv;
+                }
+                const int e = nS - k + 2 * less + eq;
                 eqv[(int)(uint32_t)key] = e;
                 sq += (int64_t)(e - k) * (e - k);
             }
@@ -385,7 +425,8 @@ __global__ void __launch_bounds__(NW * 32) ft_persistent_kernel(FtPersistentArgs
     int* eqv = reinterpret_cast<int*>(smem);                                     // Wt + 1
     uint32_t* bits = reinterpret_cast<uint32_t*>(eqv + ((Wt + 4) & ~3));         // nwords
     uint64_t* qkeys = reinterpret_cast<uint64_t*>(bits + ((nwords + 3) & ~3));   // capq (8-byte aligned)
-    int* hist = reinterpret_cast<int*>(qkeys + a.capq);                          // NW * 256
+    uint32_t* qvals = reinterpret_cast<uint32_t*>(qkeys + a.capq);                // capq
+    int* hist = reinterpret_cast<int*>(qvals + a.capq);                           // NW * 256 (>= 512)
     float* lsc = reinterpret_cast<float*>(hist + NW * 256);                      // 256
     int* off = reinterpret_cast<int*>(lsc + 256);                                // 257
     int* red = off + 257;                                                        // NW
@@ -424,7 +465,7 @@ __global__ void __launch_bounds__(NW * 32) ft_persistent_kernel(FtPersistentArgs
                 __syncthreads();
                 continue;
             }
-            cta_query_ranks<NW>(a, cell, nS, bits, eqv, qkeys, &sh.kq, &sh.nq, &sh.rq);
+            cta_query_ranks<NW>(a, cell, nS, bits, eqv, qkeys, qvals, hist, &sh.kq, &sh.nq, &sh.rq);
             if (a.pack_shift)
                 for (int g = tid; g <= Wt; g += NW * 32) eqv[g] = pack_e(eqv[g], a.pack_shift);
             if (tid == 0) label_offsets(a, top, ntop, off);
@@ -464,7 +505,9 @@ __global__ void __launch_bounds__(256) split_prepare_kernel(FtPersistentArgs a, 
     int* eqv = reinterpret_cast<int*>(smem);
     uint32_t* bits = reinterpret_cast<uint32_t*>(eqv + ((Wt + 4) & ~3));
     uint64_t* qkeys = reinterpret_cast<uint64_t*>(bits + ((nwords + 3) & ~3));
-    int* red = reinterpret_cast<int*>(qkeys + a.capq);
+    uint32_t* qvals = reinterpret_cast<uint32_t*>(qkeys + a.capq);
+    int* qhist = reinterpret_cast<int*>(qvals + a.capq);  // 512
+    int* red = qhist + 512;
     __shared__ int s_ntop, s_go;
     uint8_t* top = sp.top + (size_t)i * 256;
     const int cell = sp.cells[i];
@@ -515,7 +558,7 @@ __global__ void __launch_bounds__(256) split_prepare_kernel(FtPersistentArgs a, 
     __shared__ int s_kq;
     __shared__ int64_t s_nq;
     __shared__ double s_rq;
-    cta_query_ranks<NW>(a, cell, nS, bits, eqv, qkeys, &s_kq, &s_nq, &s_rq);
+    cta_query_ranks<NW>(a, cell, nS, bits, eqv, qkeys, qvals, qhist, &s_kq, &s_nq, &s_rq);
     int* geqv = sp.eqv + (size_t)i * Wt;
     for (int g = tid; g < Wt; g += NW * 32) geqv[g] = eqv[g];
     if (tid == 0) {
@@ -582,7 +625,7 @@ __global__ void __launch_bounds__(256) split_decide_kernel(FtPersistentArgs a, F
 size_t split_prepare_smem(int Wt, int capq) {
     const int nwords = (Wt + 31) / 32;
     return sizeof(int) * ((Wt + 4) & ~3) + sizeof(uint32_t) * ((nwords + 3) & ~3) + sizeof(uint64_t) * capq +
-           sizeof(int) * 16;
+           sizeof(uint32_t) * capq + sizeof(int) * (512 + 16);
 }
 
 void split_round_setup(const FtPersistentArgs& a) {
@@ -617,7 +660,7 @@ size_t ft_persistent_smem(int Wt, int capq, int nw) {
     size_t b = 0;
     b += sizeof(int) * ((Wt + 4) & ~3);
     b += sizeof(uint32_t) * ((nwords + 3) & ~3);
-    b += sizeof(uint64_t) * capq;
+    b += sizeof(uint64_t) * capq + sizeof(uint32_t) * capq;
     b += sizeof(int) * (size_t)nw * 256 + sizeof(float) * 256 + sizeof(int) * (257 + nw) + 512;
     return (b + 15) & ~size_t(15);
 }
