@@ -129,7 +129,9 @@ struct sgr_ctx {
     int corr_f16 = 0;              // tuning: score-step correlation on FP16 operands (not exact)
     DevBuf<uint16_t> ref_f16;      // reference ranks as IEEE half rows [R][Kp]
     bool ref_f16_ready = false;
-    DevBuf<int32_t> d_lorder;  // label ids by reference-cell count, longest first (score-step selection)
+    DevBuf<int32_t> d_lorder;
+    DevBuf<int32_t> d_lstart;     // first reference column of each label (L + 1 entries)
+    DevBuf<uint32_t> ext_min, ext_max;  // per (query, label) score extremes of a score block  // label ids by reference-cell count, longest first (score-step selection)
     DevBuf<RankItem> rank_overflow;  // rows ranked by the rank kernel's large-buffer tier
     DevBuf<int> rank_n_overflow;
     int ft_warps = 8;            // warps per CTA of the persistent fine-tune (8 or 32)
@@ -513,6 +515,12 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
                        std::min(pow2_at_least(std::max<int>(ctx->Wt, 32)), 8192), ctx->Wt, ctx->ref_sorted.p, s);
     SGR_CUDA(cudaStreamSynchronize(s));  // the row tables are freed on return
     ctx->d_ctidx.upload(mk.ctidx, s);
+    {
+        std::vector<int32_t> lstart(mk.n_labels + 1);
+        for (uint32_t l = 0; l < mk.n_labels; ++l) lstart[l] = (int32_t)mk.ctidx[2 * l];
+        lstart[mk.n_labels] = (int32_t)ctx->R;
+        ctx->d_lstart.upload(lstart, s);
+    }
     ctx->d_ft_genes.upload(mk.ft_genes.empty() ? std::vector<uint32_t>{0} : mk.ft_genes, s);
     ctx->d_ft_idx.upload(mk.ft_idx, s);
     std::vector<int32_t> gt(mk.n_labels + 1, 0);
@@ -552,11 +560,12 @@ void ensure_ref_f16(sgr_ctx* ctx) {
     ctx->ref_f16_ready = true;
 }
 
-void correlate(sgr_ctx* ctx, bool fp32, const int8_t* A, int nq, uint32_t q0, float* out, int64_t ld) {
+void correlate(sgr_ctx* ctx, bool fp32, const int8_t* A, int nq, uint32_t q0, float* out, int64_t ld,
+               LabelExtremes ext = LabelExtremes{}) {
     if (ctx->corr_f16 && !fp32) {
         launch_corr_tc(A, reinterpret_cast<const int8_t*>(ctx->ref_f16.p), nq, (int)ctx->R, ctx->Kp,
                        ctx->q_rinv.p + q0, ctx->ref_rinv.p, ctx->q_n2.p + q0, ctx->ref_n2.p, out, ld, ctx->status.p,
-                       ctx->stream, true);
+                       ctx->stream, true, ext);
         return;
     }
     if (fp32 || exact_simt())
@@ -565,7 +574,7 @@ void correlate(sgr_ctx* ctx, bool fp32, const int8_t* A, int nq, uint32_t q0, fl
                          ld, ctx->stream);
     else
         launch_corr_tc(A, ctx->ref_limbs.p, nq, (int)ctx->R, ctx->Kp, ctx->q_rinv.p + q0, ctx->ref_rinv.p,
-                       ctx->q_n2.p + q0, ctx->ref_n2.p, out, ld, ctx->status.p, ctx->stream);
+                       ctx->q_n2.p + q0, ctx->ref_n2.p, out, ld, ctx->status.p, ctx->stream, false, ext);
 }
 
 // Score-step device pass over the first nq rows of `q` (already device resident).
@@ -612,11 +621,24 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
     const uint32_t chunk =
         (uint32_t)std::max<size_t>(1, std::min<size_t>(Q, ctx->score_chunk_bytes / (4 * (size_t)R)));
     ctx->scores.ensure((size_t)chunk * R);
+    // the tensor-core correlation also writes each (query, label) list's extremes for the selection
+    const bool tc_ext = !fp32 && !exact_simt();
+    LabelExtremes ext{};
+    if (tc_ext) {
+        ext.lstart = ctx->d_lstart.p;
+        ext.L = (int)L;
+        ext.kmin = ctx->ext_min.ensure((size_t)chunk * L);
+        ext.kmax = ctx->ext_max.ensure((size_t)chunk * L);
+    }
     for (uint32_t q0 = 0; q0 < Q; q0 += chunk) {
         const int nq = (int)std::min(chunk, Q - q0);
         const uint64_t c0 = launch_count();
         sp = ctx->prof.begin(ST_CORR, s);
-        correlate(ctx, fp32, ctx->q_limbs.p + (size_t)q0 * (f16 ? 2 : 3) * ctx->Kp, nq, q0, ctx->scores.p, R);
+        if (tc_ext) {
+            SGR_CUDA(cudaMemsetAsync(ext.kmin, 0xff, (size_t)nq * L * sizeof(uint32_t), s));
+            SGR_CUDA(cudaMemsetAsync(ext.kmax, 0, (size_t)nq * L * sizeof(uint32_t), s));
+        }
+        correlate(ctx, fp32, ctx->q_limbs.p + (size_t)q0 * (f16 ? 2 : 3) * ctx->Kp, nq, q0, ctx->scores.p, R, ext);
         ctx->prof.end(sp, s);
         ctx->prof.acc.corr_launches += launch_count() - c0;
         sp = ctx->prof.begin(ST_SELECT, s);
@@ -624,7 +646,7 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
         ctx->prof.acc.select_bytes += 4ull * (uint64_t)nq * R;
         launch_select_first(ctx->scores.p, R, nq, (int)L, ctx->lq.p, p, thre, ctx->q_n2.p + q0,
                             ctx->label_scores.p + (size_t)q0 * L, ctx->first.p + q0, ctx->flags.p + (size_t)q0 * L,
-                            scratch, max_len, ctx->status.p, (int)R, ctx->d_lorder.p, s);
+                            scratch, max_len, ctx->status.p, (int)R, ctx->d_lorder.p, s, ext.kmin, ext.kmax);
         ctx->prof.end(sp, s);
     }
     ctx->prof.acc.cells += Q;

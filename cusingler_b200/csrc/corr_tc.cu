@@ -24,7 +24,8 @@
 //               tcgen05.ld 32x32b of P1 and P3 into T = 127 P1 + P3 (registers), release of those
 //               two accumulators (the next tile's H and S planes may start), then P2, the exact
 //               recombination, scores into a 128 x 160 staging tile in shared memory, release of
-//               P2, and row-contiguous 16-byte stores from the staging tile
+//               P2, and row-contiguous 16-byte stores from the staging tile; with LabelExtremes it
+//               also keeps each (query, label) list's min / max for the selection
 // A second instantiation (F16) is the FP16-operand variant benchmarked beside the exact one: d as
 // IEEE half (exact for |d| <= 2048), one kind::f16 accumulator with FP32 sums (not exact).
 // No TMA multicast is used.  Every mbarrier wait is bounded: on timeout the kernel records
@@ -164,6 +165,12 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
+// Order key of a float (unsigned compare = float compare for non-NaN values).
+__device__ __forceinline__ uint32_t ord_key(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
 struct __align__(8) TcShared {
     uint64_t full[STAGES];
     uint64_t empty[STAGES];
@@ -182,7 +189,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     corr_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nq, int R,
                    int Kp, const double* __restrict__ rq, const double* __restrict__ rr,
                    const int64_t* __restrict__ nq2, const int64_t* __restrict__ nr2, float* __restrict__ out,
-                   int64_t ld, int* status) {
+                   int64_t ld, int* status, LabelExtremes ext) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ TcShared sh;
     // stage buffers must start on a 1024-byte boundary (128B swizzle atoms)
@@ -358,6 +365,22 @@ __global__ void __launch_bounds__(THREADS, 1)
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&sh.tmem_empty));
+            // per-(query, label) extremes of this warp's columns, flushed at label ends (labels are
+            // column ranges, the same for every lane, so the flushes are warp-uniform)
+            int lab = 0, lab_end = 0;
+            float mnf = __int_as_float(0x7f800000), mxf = -__int_as_float(0x7f800000);
+            bool seen = false;
+            if (ext.kmin) {
+                const int cb = n0 + half * HALF;
+                int lo = 0, hi = ext.L - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (__ldg(ext.lstart + mid) <= cb) lo = mid;
+                    else hi = mid - 1;
+                }
+                lab = lo;
+                lab_end = __ldg(ext.lstart + lab + 1);
+            }
             // phase 2: P2 (the F16 accumulator), reads one chunk ahead of the arithmetic
             const uint32_t base2 = lane_base + (F16 ? 0 : 2 * BN);
             uint32_t p2[2][16];
@@ -378,12 +401,49 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
                     srow[((col0 >> 2) + u) ^ (row & 7)] = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+                if (ext.kmin && n0 + col0 + 16 <= min(lab_end, R)) {  // the chunk lies in one label
+                    float a0 = fminf(fminf(v[0], v[1]), fminf(v[2], v[3]));
+                    float b0 = fmaxf(fmaxf(v[0], v[1]), fmaxf(v[2], v[3]));
+#pragma unroll
+                    for (int j = 4; j < 16; j += 4) {
+                        a0 = fminf(a0, fminf(fminf(v[j], v[j + 1]), fminf(v[j + 2], v[j + 3])));
+                        b0 = fmaxf(b0, fmaxf(fmaxf(v[j], v[j + 1]), fmaxf(v[j + 2], v[j + 3])));
+                    }
+                    mnf = fminf(mnf, a0);
+                    mxf = fmaxf(mxf, b0);
+                    seen = true;
+                } else if (ext.kmin) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int col = n0 + col0 + j;
+                        if (col >= R) break;
+                        if (col >= lab_end) {  // label boundary
+                            if (seen && q < nq) {
+                                atomicMin(ext.kmin + (size_t)q * ext.L + lab, ord_key(mnf));
+                                atomicMax(ext.kmax + (size_t)q * ext.L + lab, ord_key(mxf));
+                            }
+                            mnf = __int_as_float(0x7f800000);
+                            mxf = -__int_as_float(0x7f800000);
+                            do {
+                                ++lab;
+                                lab_end = __ldg(ext.lstart + lab + 1);
+                            } while (col >= lab_end);
+                        }
+                        mnf = fminf(mnf, v[j]);
+                        mxf = fmaxf(mxf, v[j]);
+                        seen = true;
+                    }
+                }
                 if (c + 1 < CH) tmem_wait_ld();
             }
             // all of this warp's TMEM reads are done: release its share of P2
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&sh.tmem_empty_c));
+            if (ext.kmin && seen && q < nq) {
+                atomicMin(ext.kmin + (size_t)q * ext.L + lab, ord_key(mnf));
+                atomicMax(ext.kmax + (size_t)q * ext.L + lab, ord_key(mxf));
+            }
             constexpr int F4 = HALF / 4;  // 16-byte chunks per row of this warp
 #pragma unroll 4
             for (int it = lane; it < 32 * F4; it += 32) {
@@ -447,7 +507,7 @@ size_t corr_tc_smem() { return (size_t)STAGES * STAGE_BYTES + STAGING_BYTES + 10
 
 void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
                     const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s,
-                    bool f16) {
+                    bool f16, LabelExtremes ext) {
     if (nq <= 0 || R <= 0) return;
     if (Kp % BK != 0 || (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15))
         fail(SGR_ERR_INVALID_ARGUMENT, "tensor-core correlation: misaligned operands");
@@ -458,7 +518,7 @@ void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, con
     SGR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long tiles = (long)((nq + BM - 1) / BM) * ((R + BN - 1) / BN);
     const int grid = (int)std::min<long>(tiles, device_sm_count());
-    kern<<<grid, THREADS, smem, s>>>(ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status);
+    kern<<<grid, THREADS, smem, s>>>(ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status, ext);
     SGR_LAUNCH_CHECK();
     count_launch();
 }

@@ -451,7 +451,8 @@ __global__ void __launch_bounds__(NW * 32) select_first_kernel(const float* scor
                                                            const LabelQ* lq, float p, float thre, const int64_t* qn2,
                                                            float* label_scores, int32_t* first, uint8_t* flags,
                                                            float* scratch, int64_t spw, int* status, int row_len,
-                                                           const int32_t* lorder) {
+                                                           const int32_t* lorder, const uint32_t* ext_min,
+                                                           const uint32_t* ext_max) {
     extern __shared__ __align__(16) float srow[];
     __shared__ float ls[256];
     __shared__ int hist[NW][256];
@@ -485,6 +486,9 @@ __global__ void __launch_bounds__(NW * 32) select_first_kernel(const float* scor
                 const LabelQ d = lq[l];
                 float r;
                 if (qnan) r = __int_as_float(0x7fffffff);
+                else if (ext_min && !d.has_nan && d.kind != 0)  // extremes from the correlation epilogue
+                    r = quantile_warp_core(row + d.start, d, p, hist[warp], my_scratch, lane, status,
+                                           ext_min[(size_t)q * L + l], ext_max[(size_t)q * L + l], false);
                 else r = quantile_warp(row + d.start, d, p, hist[warp], my_scratch, lane, status);
                 if (lane == 0) ls[l] = r;
             }
@@ -697,7 +701,8 @@ void launch_corr_simt(bool fp32ref, const int8_t* A, const int8_t* B, int nq, in
 
 void launch_select_first(const float* scores, int64_t ld, int nq, int L, const LabelQ* lq, float p, float thre,
                          const int64_t* qn2, float* label_scores, int32_t* first, uint8_t* flags, float* scratch,
-                         int64_t spw, int* status, int row_len, const int32_t* lorder, cudaStream_t s) {
+                         int64_t spw, int* status, int row_len, const int32_t* lorder, cudaStream_t s,
+                         const uint32_t* ext_min, const uint32_t* ext_max) {
     if (nq <= 0) return;
     const size_t stage_bytes = (((size_t)std::max(row_len, 1) * 4 + 15) & ~size_t(15));
     if (lorder && stage_bytes <= 200 * 1024) {
@@ -709,12 +714,13 @@ void launch_select_first(const float* scores, int64_t ld, int nq, int L, const L
         const unsigned blocks = (unsigned)std::min<long>(nq, (long)sm_count() * per_sm);
         select_first_kernel<true><<<blocks, 512, stage_bytes, s>>>(scores, ld, nq, L, lq, p, thre, qn2, label_scores,
                                                                    first, flags, scratch, spw, status, row_len,
-                                                                   lorder);
+                                                                   lorder, ext_min, ext_max);
     } else {
         const unsigned blocks = scratch ? (unsigned)std::min<long>(nq, sm_count() * 2)
                                         : (unsigned)std::min<long>(nq, sm_count() * 8);
         select_first_kernel<false><<<blocks, 256, 0, s>>>(scores, ld, nq, L, lq, p, thre, qn2, label_scores, first,
-                                                          flags, scratch, spw, status, row_len, lorder);
+                                                          flags, scratch, spw, status, row_len, lorder, nullptr,
+                                                          nullptr);
     }
     SGR_LAUNCH_CHECK();
     count_launch();

@@ -109,10 +109,12 @@ struct LabelQ {
 
 // row_len: floats of a score row that the labels cover.  With `lorder` (label ids, longest first)
 // and rows of at most 200 KB, each block stages its row in shared memory before selecting.
+// ext_min / ext_max (optional, staged path): per (row, label) extreme order keys from the
+// correlation epilogue, used instead of a min / max pass for lists that cannot hold NaN.
 void launch_select_first(const float* scores, int64_t ld, int nq, int L, const LabelQ* lq, float p,
                          float thre, const int64_t* qn2, float* label_scores, int32_t* first, uint8_t* flags,
                          float* scratch, int64_t scratch_per_warp, int* status, int row_len, const int32_t* lorder,
-                         cudaStream_t s);
+                         cudaStream_t s, const uint32_t* ext_min = nullptr, const uint32_t* ext_max = nullptr);
 
 // ---- fine-tune ----------------------------------------------------------------------------------
 struct FtGroup {
@@ -151,9 +153,19 @@ void launch_ft_select(const FtGroup* groups, const FtSelItem* items, uint32_t n_
 
 // Exact score-step correlation on the tensor cores (corr_tc.cu): A/B are LIMBS rows of 3 * Kp bytes.
 size_t corr_tc_smem();
+// Per-(query, label) extremes written by the correlation epilogue for the selection: label l's
+// reference columns are [lstart[l], lstart[l+1]); kmin / kmax (Q x L order keys, preset to all ones /
+// zero) receive atomicMin / atomicMax of each list's scores.  kmin = nullptr: not written.
+struct LabelExtremes {
+    const int32_t* lstart = nullptr;
+    int L = 0;
+    uint32_t* kmin = nullptr;
+    uint32_t* kmax = nullptr;
+};
+
 void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
                     const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s,
-                    bool f16 = false);
+                    bool f16 = false, LabelExtremes ext = LabelExtremes{});
 
 // Persistent exact fine-tune (finetune.cu).
 struct FtPersistentArgs {
