@@ -142,16 +142,32 @@ __device__ int cta_gene_set(const FtPersistentArgs& a, const uint8_t* top, int n
     for (int w = tid; w < nwords; w += NW * 32) bits[w] = 0u;
     __syncthreads();
     const int gthre = a.gene_thre[ntop];
-    for (int pr = warp; pr < ntop * ntop; pr += NW) {
-        const int i = pr / ntop, j = pr % ntop;
-        if (i == j) continue;
-        const int li = top[i], lj = top[j];
-        const uint32_t pos = a.ft_idx[2 * ((size_t)li * a.L + lj)];
-        int len = (int)a.ft_idx[2 * ((size_t)li * a.L + lj) + 1];
-        if (len > gthre) len = gthre;
-        for (int e = lane; e < len; e += 32) {
-            const uint32_t g = a.ft_genes[pos + e];
-            atomicOr(&bits[g >> 5], 1u << (g & 31));
+    // a warp takes 32 ordered pairs at a time: each lane fetches one pair's list, then the warp
+    // walks the 32 lists together so that the gene loads of several pairs are in flight at once
+    for (int base = warp * 32; base < ntop * ntop; base += NW * 32) {
+        const int pr = base + lane;
+        uint32_t pos = 0;
+        int len = 0;
+        if (pr < ntop * ntop) {
+            const int i = pr / ntop, j = pr % ntop;
+            if (i != j) {
+                const size_t pi = (size_t)top[i] * a.L + top[j];
+                pos = a.ft_idx[2 * pi];
+                len = min((int)a.ft_idx[2 * pi + 1], gthre);
+            }
+        }
+        const int maxn = __reduce_max_sync(FULL, len);
+        for (int e0 = 0; e0 < maxn; e0 += 32) {
+#pragma unroll 8
+            for (int t = 0; t < 32; ++t) {
+                const uint32_t p = __shfl_sync(FULL, pos, t);
+                const int n = __shfl_sync(FULL, len, t);
+                const int e = e0 + lane;
+                if (e < n) {
+                    const uint32_t g = __ldg(a.ft_genes + p + e);
+                    atomicOr(&bits[g >> 5], 1u << (g & 31));
+                }
+            }
         }
     }
     __syncthreads();
