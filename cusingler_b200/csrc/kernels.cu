@@ -62,12 +62,11 @@ __device__ __forceinline__ int rank_bucket(uint64_t key, float fmin, float scale
 __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-    // per warp: keys (cap x 8 B) | values by bucket (cap x 4 B) | bucket counts | bucket cursors | stage
+    // per warp: keys (cap x 8 B) | values by bucket (cap x 4 B) | 256 bucket counts / ends | stage
     uint64_t* keys = reinterpret_cast<uint64_t*>(smem + (size_t)warp * warp_bytes);
     uint32_t* vals = reinterpret_cast<uint32_t*>(keys + a.cap);
     int* hist = reinterpret_cast<int*>(vals + a.cap);
-    int* cursor = hist + 256;
-    unsigned char* stage = reinterpret_cast<unsigned char*>(cursor + 256);
+    unsigned char* stage = reinterpret_cast<unsigned char*>(hist + 256);
     const uint32_t n_items = a.n_items_dev ? (uint32_t)*a.n_items_dev : a.n_items;
     for (uint32_t item = blockIdx.x * wpb + warp; item < n_items; item += gridDim.x * wpb) {
         RankItem it;
@@ -146,16 +145,16 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
             }
             int acc = warp_incl_scan(sum, lane) - sum;
 #pragma unroll
-            for (int t = 0; t < 8; ++t) {
-                cursor[8 * lane + t] = acc;
+            for (int t = 0; t < 8; ++t) {  // each lane rewrites only the counts it read
+                hist[8 * lane + t] = acc;
                 acc += c[t];
             }
             __syncwarp();
             for (int j = lane; j < k; j += 32) {
                 const uint64_t key = keys[j];
-                vals[atomicAdd(&cursor[rank_bucket(key, fmin, scale)], 1)] = (uint32_t)(key >> 32);
+                vals[atomicAdd(&hist[rank_bucket(key, fmin, scale)], 1)] = (uint32_t)(key >> 32);
             }
-            __syncwarp();  // cursor[b] is now the end of bucket b
+            __syncwarp();  // hist[b] is now the end of bucket b, and bucket b starts where b - 1 ends
         }
 
         // 2) every position of the subset starts as an implicit zero: rank (G-k+1)/2, d = -k;
@@ -191,9 +190,9 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
                 const uint64_t key = keys[j];
                 const uint32_t hv = (uint32_t)(key >> 32);
                 const int b = rank_bucket(key, fmin, scale);
-                const int e = cursor[b];
-                int less = e - hist[b], eq = 0;  // entries of lower buckets, then this bucket's
-                for (int t = e - hist[b]; t < e; ++t) {
+                const int e = hist[b], st = b > 0 ? hist[b - 1] : 0;
+                int less = st, eq = 0;  // entries of lower buckets, then this bucket's
+                for (int t = st; t < e; ++t) {
                     const uint32_t u = vals[t];
                     less += u < hv;
                     eq += u == hv;
@@ -611,7 +610,7 @@ int sm_count() { return device_sm_count(); }
 namespace {
 void launch_rank_tier(const RankLaunch& a, long max_blocks, cudaStream_t s) {
     const int stage_bytes = a.out_mode == RANK_LIMBS ? 3 * a.max_Kp : 2 * a.max_Kp;
-    const int warp_bytes = ((a.cap * 12 + 2 * 256 * 4 + stage_bytes) + 15) & ~15;
+    const int warp_bytes = ((a.cap * 12 + 256 * 4 + stage_bytes) + 15) & ~15;
     const int budget = 200 * 1024;
     int wpb = budget / warp_bytes;
     if (wpb > 8) wpb = 8;
@@ -629,7 +628,7 @@ void launch_rank_tier(const RankLaunch& a, long max_blocks, cudaStream_t s) {
 
 void launch_rank(const RankLaunch& a, cudaStream_t s) {
     if (a.n_items == 0) return;
-    constexpr int kSmallCap = 512;
+    constexpr int kSmallCap = 384;  // 3 CTAs of 8 warps per SM with a 1,152-column stage
     if (!a.overflow || a.cap <= kSmallCap) {
         RankLaunch b = a;
         b.overflow = nullptr;

@@ -64,7 +64,7 @@ struct RankLaunch {
     int max_Kp;                 // largest Kp over the groups (smem sizing)
     int cap;                    // sort capacity per warp (power of two)
     int* status;                // device flags: bit0 column out of range, bit1 NaN value
-    // Two-tier launch: when `overflow` is set, launch_rank ranks rows of at most `small_cap` entries
+    // Two-tier launch: when `overflow` is set, launch_rank ranks rows of at most 384 marker entries
     // with a small sort buffer (more warps per SM) and appends the other rows to `overflow`
     // (capacity n_items), which a second launch with `cap` ranks; `n_overflow` is one device int.
     RankItem* overflow = nullptr;
