@@ -124,6 +124,35 @@ def test_dense_rows_take_the_large_sort_tier(mode):
         assert np.array_equal(d_ref[i], orc.rank_row(0, i)), i
 
 
+def test_long_labels_ties_and_nan_lists():
+    """Long score lists in exact mode.  Five labels, four of them over 1,024 reference cells: one long
+    label holds an empty reference row (its lists hold NaN and are sorted exactly), one holds 1,000
+    copies of a single cell (the order statistic's value bin exceeds the 256-key buffer, so the radix
+    selection decides), two take the bucket selection with extremes from the correlation; one query
+    row is empty (a NaN row).  Scores, first labels, flags and final labels equal the oracle's."""
+    w, ref, qry = synth.custom_dataset(6000, 128, 3000, 5, 0.08, seed=36)
+    counts = np.bincount(ref.labels, minlength=5)
+    assert (counts >= 1024).sum() == 4
+
+    def rows_of(m):
+        return [list(zip(m.indices[m.indptr[i]:m.indptr[i + 1]], m.data[m.indptr[i]:m.indptr[i + 1]]))
+                for i in range(m.n_rows)]
+
+    rows_r = rows_of(ref)
+    by_label = [np.flatnonzero(ref.labels == l) for l in range(5)]
+    copies = by_label[0][:1000]
+    for i in copies[1:]:
+        rows_r[i] = list(rows_r[copies[0]])
+    rows_r[by_label[1][7]] = []
+    rows_q = rows_of(qry)
+    rows_q[5] = []
+    r = _csr_from_rows(rows_r, ref.n_cols)
+    q = _csr_from_rows(rows_q, qry.n_cols)
+    prob = O.Problem(r, q, synth.names("CT", 5), ref.labels, synth.names("G", ref.n_cols),
+                     synth.names("G", qry.n_cols))
+    _run_both(prob, abi.MODE_EXACT)
+
+
 def test_gene_intersection():
     ref, qry, L = H.dataset("tiny")
     rg = synth.names("G", ref.n_cols)
