@@ -473,6 +473,13 @@ __global__ void __launch_bounds__(NW * 32) select_first_kernel(const float* scor
                     for (int i = threadIdx.x; i < row_len; i += NW * 32) srow[i] = __ldcs(row + i);
                 }
             }
+            // the block's next row is brought into L2 while this one is selected, so that its staging
+            // loads hit L2 (16-byte aligned rows, ld % 4 == 0: the rounded-up size stays in the row)
+            if (vec && threadIdx.x == 0 && q + (int)gridDim.x < nq && qn2[q + gridDim.x] != 0) {
+                const float* nxt = scores + (size_t)(q + gridDim.x) * ld;
+                const uint32_t bytes = (uint32_t)(row_len * 4 + 15) & ~15u;
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(nxt), "r"(bytes) : "memory");
+            }
             if (threadIdx.x == 0) s_next = 0;
             __syncthreads();
             row = srow;
