@@ -130,6 +130,7 @@ struct sgr_ctx {
     DevBuf<uint16_t> ref_f16;      // reference ranks as IEEE half rows [R][Kp]
     bool ref_f16_ready = false;
     DevBuf<int32_t> d_lorder;
+    DevBuf<int32_t> scan_part;  // tile sums of the filter's exclusive scan
     DevBuf<int32_t> d_lstart;     // first reference column of each label (L + 1 entries)
     DevBuf<uint32_t> ext_min, ext_max;  // per (query, label) score extremes of a score block  // label ids by reference-cell count, longest first (score-step selection)
     DevBuf<RankItem> rank_overflow;  // rows ranked by the rank kernel's large-buffer tier
@@ -386,7 +387,8 @@ void filter_csr(sgr_ctx* ctx, const DevCsr& m, const int32_t* map, DevBuf<float>
     ctx->counts.ensure(m.n_rows + 1);
     op.ensure((size_t)m.n_rows + 1);
     launch_filter_count(m.indptr, m.indices, m.n_rows, m.n_cols, map, ctx->counts.p, ctx->stream, row_mask);
-    launch_exclusive_scan(ctx->counts.p, op.p, m.n_rows, nullptr, ctx->stream);
+    int32_t* scan_scratch = ctx->scan_part.ensure(2 * (((size_t)m.n_rows + 4095) / 4096) + 1);
+    launch_exclusive_scan(ctx->counts.p, op.p, m.n_rows, scan_scratch, ctx->stream);
     int32_t total = 0;
     SGR_CUDA(cudaMemcpyAsync(&total, op.p + m.n_rows, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     SGR_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -675,10 +675,72 @@ void launch_mark_rows(const int32_t* list, int n, uint8_t* mask, cudaStream_t s)
     count_launch();
 }
 
-void launch_exclusive_scan(const int32_t* in, int32_t* out, uint32_t n, int32_t*, cudaStream_t s) {
-    scan_kernel<<<1, 1024, 0, s>>>(in, out, n);
+namespace {
+constexpr uint32_t kScanTile = 4096;  // values per block of the tiled scan: 1024 threads x 4
+
+// Sum of each 4096-value tile.
+__global__ void __launch_bounds__(1024) tile_sum_kernel(const int32_t* in, uint32_t n, int32_t* part) {
+    __shared__ int32_t ws[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * 4;
+    int32_t v = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v += base + j < n ? in[base + j] : 0;
+    v = __reduce_add_sync(FULL, v);
+    if (lane == 0) ws[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        const int32_t t = __reduce_add_sync(FULL, ws[lane]);
+        if (lane == 0) part[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of each tile (4 consecutive values per thread) plus the tile's offset part_ex[b];
+// block 0 also writes the total out[n] = part_ex[nb].
+__global__ void __launch_bounds__(1024) tile_scan_kernel(const int32_t* in, int32_t* out, uint32_t n,
+                                                         const int32_t* part_ex, uint32_t nb) {
+    __shared__ int32_t ws[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * 4;
+    int32_t v[4], sum = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        v[j] = base + j < n ? in[base + j] : 0;
+        sum += v[j];
+    }
+    const int32_t x = warp_incl_scan(sum, lane);
+    if (lane == 31) ws[warp] = x;
+    __syncthreads();
+    if (warp == 0) ws[lane] = warp_incl_scan(ws[lane], lane);
+    __syncthreads();
+    int32_t e = part_ex[blockIdx.x] + (warp ? ws[warp - 1] : 0) + x - sum;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (base + j < n) out[base + j] = e;
+        e += v[j];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = part_ex[nb];
+}
+}  // namespace
+
+void launch_exclusive_scan(const int32_t* in, int32_t* out, uint32_t n, int32_t* scratch, cudaStream_t s) {
+    const uint32_t nb = (n + kScanTile - 1) / kScanTile;
+    if (nb <= 2 || scratch == nullptr) {  // one block walks the values
+        scan_kernel<<<1, 1024, 0, s>>>(in, out, n);
+        SGR_LAUNCH_CHECK();
+        count_launch();
+        return;
+    }
+    // tile sums, their scan (one block), then each tile's scan from its offset
+    int32_t* part = scratch;
+    int32_t* part_ex = scratch + nb;
+    tile_sum_kernel<<<nb, 1024, 0, s>>>(in, n, part);
     SGR_LAUNCH_CHECK();
-    count_launch();
+    scan_kernel<<<1, 1024, 0, s>>>(part, part_ex, nb);
+    SGR_LAUNCH_CHECK();
+    tile_scan_kernel<<<nb, 1024, 0, s>>>(in, out, n, part_ex, nb);
+    SGR_LAUNCH_CHECK();
+    count_launch(3);
 }
 
 void launch_filter_fill(const float* data, const int32_t* indptr, const int32_t* indices, uint32_t n_rows,

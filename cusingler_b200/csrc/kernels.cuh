@@ -80,6 +80,8 @@ void launch_filter_count(const int32_t* indptr, const int32_t* indices, uint32_t
                          const uint8_t* row_mask = nullptr);
 // mask[list[i]] = 1 for i < n (list entries must be valid rows of mask).
 void launch_mark_rows(const int32_t* list, int n, uint8_t* mask, cudaStream_t s);
+// out[i] = in[0] + ... + in[i-1] for i <= n.  scratch (optional): 2 * ceil(n / 4096) + 1 ints, which
+// lets blocks scan 4096-value tiles in parallel.
 void launch_exclusive_scan(const int32_t* in, int32_t* out, uint32_t n, int32_t* scratch, cudaStream_t s);
 void launch_filter_fill(const float* data, const int32_t* indptr, const int32_t* indices, uint32_t n_rows,
                         uint32_t n_cols, const int32_t* map, const int32_t* out_ptr, float* out_data,

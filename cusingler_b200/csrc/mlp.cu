@@ -6,9 +6,9 @@
 // -> L -> softmax.
 // Weights are kept as FP32 master copies (updated by AdamW) and BF16 working copies (used by the
 // forward and backward products); every product accumulates in FP32.  All kernels are hand-written:
-// a tiled CUDA-core GEMM with strided operands (the layers are at most 256 wide, far too small to
-// keep tensor cores busy), fused bias + GELU epilogues, softmax cross-entropy, bias reductions and
-// AdamW.  Inference (predict) runs the three products on the tensor cores instead.
+// a tiled CUDA-core GEMM with strided operands for training, fused bias + GELU epilogues, softmax
+// cross-entropy, bias reductions and AdamW.  Inference (predict) runs the three products on the
+// tensor cores instead.
 
 #include <cuda_bf16.h>
 
@@ -83,12 +83,10 @@ __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const TA
 // C[m][n] = act(sum_k A[m][k] W[n][k] + bias[n]) with A FP32 (row-major, lda) and W BF16 (row-major
 // [N][K], ldw).  Each A value is split into BF16 hi + lo (a - hi - lo is within 2^-16 |a|), so two
 // products per tile keep the FP32 activations' precision.  gelu: apply GELU after the bias.
-// Block tile 128 x 64 (8 warps, each 32 x 32), K in steps of 16; shared rows padded to 24 values so
-// the fragment loads are conflict-free.
-__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
-}
-
+// Block tile BM x BN with 8 warps in WARPS_M x WARPS_N, each warp 32 rows x BN / WARPS_N columns; one
+// block spans every output column of a 256-wide layer, so each A row is loaded and split once.  K in
+// steps of 64; shared rows padded to 72 values (36 words), so the fragment loads are conflict-free.
+// 16-byte loads when rows and K allow them, element loads otherwise (the first layer's K = labels).
 __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
     asm volatile(
         "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
@@ -97,50 +95,88 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-__global__ void __launch_bounds__(256) gemm_tc_kernel(int M, int N, int K, const float* A, int64_t lda,
-                                                      const __nv_bfloat16* W, int64_t ldw, const float* bias,
-                                                      float* C, int64_t ldc, int gelu) {
-    constexpr int P = 24;  // padded row length (bf16 values)
-    __shared__ __align__(16) __nv_bfloat16 Ahi[128 * P], Alo[128 * P], Ws[64 * P];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+__device__ __forceinline__ void split_store(__nv_bfloat16* hi, __nv_bfloat16* lo, float a) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(a);
+    *hi = h;
+    *lo = __float2bfloat16_rn(a - __bfloat162float(h));
+}
+
+template <int BN, int WARPS_N>
+__global__ void __launch_bounds__(256, 2) gemm_tc_kernel(int M, int N, int K, const float* A, int64_t lda,
+                                                         const __nv_bfloat16* W, int64_t ldw, const float* bias,
+                                                         float* C, int64_t ldc, int gelu) {
+    constexpr int WARPS_M = 8 / WARPS_N, BM = 32 * WARPS_M, WN = BN / WARPS_N, NT = WN / 8;
+    constexpr int BK = 64, P = BK + 8;
+    extern __shared__ __align__(16) __nv_bfloat16 sm[];
+    __nv_bfloat16* Ahi = sm;
+    __nv_bfloat16* Alo = Ahi + BM * P;
+    __nv_bfloat16* Ws = Alo + BM * P;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
-    const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;  // warp tile origin in the block tile
-    const int m0 = blockIdx.y * 128, n0 = blockIdx.x * 64;
-    float acc[2][4][4] = {};
-    for (int k0 = 0; k0 < K; k0 += 16) {
-        for (int i = threadIdx.x; i < 128 * 16; i += 256) {
-            const int r = i >> 4, c = i & 15;
-            const int m = m0 + r, k = k0 + c;
-            const float a = (m < M && k < K) ? A[m * lda + k] : 0.f;
-            const __nv_bfloat16 hi = __float2bfloat16_rn(a);
-            Ahi[r * P + c] = hi;
-            Alo[r * P + c] = __float2bfloat16_rn(a - __bfloat162float(hi));
+    const int wm = (warp / WARPS_N) * 32, wn = (warp % WARPS_N) * WN;
+    const int m0 = blockIdx.x * BM;
+    const bool vecA = (K % 4) == 0 && (lda % 4) == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0;
+    const bool vecW = (K % 8) == 0 && (ldw % 8) == 0 && (reinterpret_cast<uintptr_t>(W) & 15) == 0;
+    float acc[2][NT][4] = {};
+    for (int k0 = 0; k0 < K; k0 += BK) {
+        if (vecA) {
+            for (int i = tid; i < BM * (BK / 4); i += 256) {
+                const int r = i / (BK / 4), c = 4 * (i % (BK / 4));
+                const int m = m0 + r, k = k0 + c;
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (m < M && k < K) v = *reinterpret_cast<const float4*>(A + (int64_t)m * lda + k);
+                __nv_bfloat16* h = Ahi + r * P + c;
+                __nv_bfloat16* l = Alo + r * P + c;
+                split_store(h, l, v.x);
+                split_store(h + 1, l + 1, v.y);
+                split_store(h + 2, l + 2, v.z);
+                split_store(h + 3, l + 3, v.w);
+            }
+        } else {
+            for (int i = tid; i < BM * BK; i += 256) {
+                const int r = i / BK, c = i % BK;
+                const int m = m0 + r, k = k0 + c;
+                split_store(Ahi + r * P + c, Alo + r * P + c, (m < M && k < K) ? A[(int64_t)m * lda + k] : 0.f);
+            }
         }
-        for (int i = threadIdx.x; i < 64 * 16; i += 256) {
-            const int r = i >> 4, c = i & 15;
-            const int n = n0 + r, k = k0 + c;
-            Ws[r * P + c] = (n < N && k < K) ? W[n * ldw + k] : __float2bfloat16_rn(0.f);
+        if (vecW) {
+            for (int i = tid; i < BN * (BK / 8); i += 256) {
+                const int r = i / (BK / 8), c = 8 * (i % (BK / 8));
+                const int k = k0 + c;
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (r < N && k < K) v = *reinterpret_cast<const uint4*>(W + (int64_t)r * ldw + k);
+                *reinterpret_cast<uint4*>(Ws + r * P + c) = v;
+            }
+        } else {
+            for (int i = tid; i < BN * BK; i += 256) {
+                const int r = i / BK, c = i % BK;
+                const int k = k0 + c;
+                Ws[r * P + c] = (r < N && k < K) ? W[(int64_t)r * ldw + k] : __float2bfloat16_rn(0.f);
+            }
         }
         __syncthreads();
-        uint32_t bf[4][2];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const __nv_bfloat16* w = Ws + (wn + 8 * j + g) * P + 2 * t;
-            bf[j][0] = *reinterpret_cast<const uint32_t*>(w);
-            bf[j][1] = *reinterpret_cast<const uint32_t*>(w + 8);
-        }
+        for (int kk = 0; kk < BK; kk += 16) {
+            uint32_t bf[NT][2];
 #pragma unroll
-        for (int part = 0; part < 2; ++part) {
-            const __nv_bfloat16* As = part ? Alo : Ahi;
+            for (int j = 0; j < NT; ++j) {
+                const __nv_bfloat16* w = Ws + (wn + 8 * j + g) * P + kk + 2 * t;
+                bf[j][0] = *reinterpret_cast<const uint32_t*>(w);
+                bf[j][1] = *reinterpret_cast<const uint32_t*>(w + 8);
+            }
 #pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                const __nv_bfloat16* a = As + (wm + 16 * i + g) * P + 2 * t;
-                const uint32_t af[4] = {*reinterpret_cast<const uint32_t*>(a),
-                                        *reinterpret_cast<const uint32_t*>(a + 8 * P),
-                                        *reinterpret_cast<const uint32_t*>(a + 8),
-                                        *reinterpret_cast<const uint32_t*>(a + 8 * P + 8)};
+            for (int part = 0; part < 2; ++part) {
+                const __nv_bfloat16* As = part ? Alo : Ahi;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], af, bf[j]);
+                for (int i = 0; i < 2; ++i) {
+                    const __nv_bfloat16* a = As + (wm + 16 * i + g) * P + kk + 2 * t;
+                    const uint32_t af[4] = {*reinterpret_cast<const uint32_t*>(a),
+                                            *reinterpret_cast<const uint32_t*>(a + 8 * P),
+                                            *reinterpret_cast<const uint32_t*>(a + 8),
+                                            *reinterpret_cast<const uint32_t*>(a + 8 * P + 8)};
+#pragma unroll
+                    for (int j = 0; j < NT; ++j) mma_bf16(acc[i][j], af, bf[j]);
+                }
             }
         }
         __syncthreads();
@@ -148,16 +184,21 @@ __global__ void __launch_bounds__(256) gemm_tc_kernel(int M, int N, int K, const
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < NT; ++j)
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const int m = m0 + wm + 16 * i + g + (e >= 2 ? 8 : 0);
-                const int n = n0 + wn + 8 * j + 2 * t + (e & 1);
+                const int n = wn + 8 * j + 2 * t + (e & 1);
                 if (m >= M || n >= N) continue;
                 float v = acc[i][j][e] + bias[n];
                 if (gelu) v = 0.5f * v * (1.f + erff(v * 0.70710678118654752f));
-                C[m * ldc + n] = v;
+                C[(int64_t)m * ldc + n] = v;
             }
+}
+
+template <int BN, int WARPS_N>
+constexpr size_t gemm_tc_smem() {
+    return sizeof(__nv_bfloat16) * (2 * 32 * (8 / WARPS_N) + BN) * (64 + 8);
 }
 
 // dZ = dH * GELU'(Z), GELU'(z) = Phi(z) + z phi(z)
@@ -446,11 +487,28 @@ void Mlp::forward_infer(const float* X, int B, cudaStream_t s) {
     h2.ensure((size_t)B * H);
     logits.ensure((size_t)B * L);
     const __nv_bfloat16* W = wb.p;
+    // one block spans up to 256 output columns (64 rows x 256, or 256 rows x 32 for narrow layers);
+    // wider layers take several column blocks
     auto run = [&](int N, int K, const float* A, const __nv_bfloat16* w, const float* b, float* C, int gelu) {
-        dim3 grid((N + 63) / 64, (B + 127) / 128);
-        gemm_tc_kernel<<<grid, 256, 0, s>>>(B, N, K, A, K, w, K, b, C, N, gelu);
-        SGR_LAUNCH_CHECK();
-        count_launch();
+        if (N <= 32) {
+            constexpr size_t smem = gemm_tc_smem<32, 1>();
+            SGR_CUDA(cudaFuncSetAttribute(gemm_tc_kernel<32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+            gemm_tc_kernel<32, 1><<<(B + 255) / 256, 256, smem, s>>>(B, N, K, A, K, w, K, b, C, N, gelu);
+            SGR_LAUNCH_CHECK();
+            count_launch();
+            return;
+        }
+        constexpr size_t smem = gemm_tc_smem<256, 4>();
+        SGR_CUDA(cudaFuncSetAttribute(gemm_tc_kernel<256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        for (int n0 = 0; n0 < N; n0 += 256) {
+            gemm_tc_kernel<256, 4><<<(B + 63) / 64, 256, smem, s>>>(B, std::min(256, N - n0), K, A, K,
+                                                                     w + (size_t)n0 * K, K, b + n0, C + n0, N,
+                                                                     gelu);
+            SGR_LAUNCH_CHECK();
+            count_launch();
+        }
     };
     run(H, L, X, W + off_w1, w.p + off_b1, h1.p, 1);
     run(H, H, h1.p, W + off_w2, w.p + off_b2, h2.p, 1);

@@ -153,6 +153,16 @@ def test_long_labels_ties_and_nan_lists():
     _run_both(prob, abi.MODE_EXACT)
 
 
+def test_many_query_rows_tiled_scan():
+    """9,000 query rows: the thre-pool compaction's exclusive scan over the rows' counts runs as
+    4,096-row tiles in parallel (three tiles); scores, labels, flags and fine-tune rounds equal
+    the oracle's."""
+    w, ref, qry = synth.custom_dataset(600, 9000, 3000, 7, 0.08, seed=13)
+    prob = O.Problem(ref, qry, synth.names("CT", 7), ref.labels, synth.names("G", ref.n_cols),
+                     synth.names("G", qry.n_cols))
+    _run_both(prob, abi.MODE_EXACT)
+
+
 def test_gene_intersection():
     ref, qry, L = H.dataset("tiny")
     rg = synth.names("G", ref.n_cols)
