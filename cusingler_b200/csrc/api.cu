@@ -92,6 +92,8 @@ struct sgr_ctx {
     cudaStream_t own_stream = nullptr;  // created with the context
     cudaStream_t side = nullptr;        // fine-tune split path, concurrent with the work queue
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_state[2] = {nullptr, nullptr};  // split path: cell states copied to h_state
+    int32_t* h_state = nullptr;                     // pinned, two buffers of 1,024 cell states
     Profiler prof;
     sgr_mode mode = SGR_MODE_EXACT;
     std::string err;
@@ -932,12 +934,16 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
     }
 }
 
-// The context's second stream (and its fork / join events), created on first use.
+// The context's second stream (its fork / join events and the split path's state buffers), created
+// on first use.
 cudaStream_t side_stream(sgr_ctx* ctx) {
     if (!ctx->side) {
         SGR_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
         SGR_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
         SGR_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+        SGR_CUDA(cudaEventCreateWithFlags(&ctx->ev_state[0], cudaEventDisableTiming));
+        SGR_CUDA(cudaEventCreateWithFlags(&ctx->ev_state[1], cudaEventDisableTiming));
+        SGR_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->h_state), 2 * 1024 * sizeof(int32_t)));
     }
     return ctx->side;
 }
@@ -1137,14 +1143,12 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
             count_launch(before - launch_count());
         }
         cudaGetLastError();
-        std::vector<int> state(H);
-        // each round drops at least one candidate, so L + 2 rounds finish every cell
-        uint32_t rounds_run = 0;
-        for (;;) {
-            if (rounds_run > L + 3) {
-                if (exec) cudaGraphExecDestroy(exec);
-                fail(SGR_ERR_STATE, "fine-tune split path did not converge");
-            }
+        // Launches are pipelined: launch k + 1 is queued before the cells' states after launch k are
+        // read (copied asynchronously into pinned memory), so the device never waits for the host;
+        // the launch queued after the last cell finished runs rounds that do nothing.  Each round
+        // drops at least one candidate, so L + 2 rounds finish every cell.
+        uint32_t rounds_run = 0, rounds_at[2] = {0, 0};
+        for (int launched = 0;; ++launched) {
             if (exec) {
                 const cudaError_t e = cudaGraphLaunch(exec, s);
                 if (e != cudaSuccess) {
@@ -1157,11 +1161,22 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
                 launch_split_round(a, sp, H, max_chunks, s);
                 rounds_run += 1;
             }
-            SGR_CUDA(cudaMemcpyAsync(state.data(), ctx->sp_state.p, H * sizeof(int), cudaMemcpyDeviceToHost, s));
-            SGR_CUDA(cudaStreamSynchronize(s));
+            const int cur = launched & 1;
+            rounds_at[cur] = rounds_run;
+            SGR_CUDA(cudaMemcpyAsync(ctx->h_state + cur * 1024, ctx->sp_state.p, H * sizeof(int),
+                                     cudaMemcpyDeviceToHost, s));
+            SGR_CUDA(cudaEventRecord(ctx->ev_state[cur], s));
+            if (launched == 0) continue;
+            const int prev = cur ^ 1;
+            SGR_CUDA(cudaEventSynchronize(ctx->ev_state[prev]));
+            const int32_t* state = ctx->h_state + prev * 1024;
             bool all = true;
             for (int i = 0; i < H; ++i) all &= state[i] == 2;
             if (all) break;
+            if (rounds_at[prev] > L + 3) {
+                if (exec) cudaGraphExecDestroy(exec);
+                fail(SGR_ERR_STATE, "fine-tune split path did not converge");
+            }
         }
         if (exec) cudaGraphExecDestroy(exec);
         unsigned long long rows = 0;
@@ -1229,12 +1244,16 @@ sgr_status sgr_destroy(sgr_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->side) cudaStreamSynchronize(ctx->side);
     cudaStream_t s = ctx->own_stream, side = ctx->side;
-    cudaEvent_t e1 = ctx->ev_fork, e2 = ctx->ev_join;
+    cudaEvent_t e1 = ctx->ev_fork, e2 = ctx->ev_join, e3 = ctx->ev_state[0], e4 = ctx->ev_state[1];
+    int32_t* hs = ctx->h_state;
     delete ctx;  // DevBuf destructors free device memory
     if (s) cudaStreamDestroy(s);
     if (side) cudaStreamDestroy(side);
     if (e1) cudaEventDestroy(e1);
     if (e2) cudaEventDestroy(e2);
+    if (e3) cudaEventDestroy(e3);
+    if (e4) cudaEventDestroy(e4);
+    if (hs) cudaFreeHost(hs);
     return SGR_OK;
 }
 
