@@ -44,9 +44,9 @@ FALLBACK_BF16_TFLOPS = 1590.0
 # (profiles/corr_tc_mid_8192q.md, select_first_mid_8192q.md, rank_kernel_mid_8192q.md: read +
 # write); a launch's traffic is this times its query rows (each row's traffic is the same).
 TRAFFIC_PER_QUERY = {
-    "corr": (1.135093e9 + 0.632601e9) / 8192,
-    "select": (0.657565e9 + 4.414976e6) / 8192,
-    "rank": (0.098435e9 + 9.91616e6) / 8192,
+    "corr": (1.170260e9 + 0.632710e9) / 8192,
+    "select": (0.657572e9 + 4.554752e6) / 8192,
+    "rank": (0.098440e9 + 6.304e6) / 8192,
 }
 
 
