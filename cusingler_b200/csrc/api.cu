@@ -93,6 +93,8 @@ struct sgr_ctx {
     cudaStream_t side = nullptr;        // fine-tune split path, concurrent with the work queue
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_state[2] = {nullptr, nullptr};  // split path: cell states copied to h_state
+    cudaStream_t copy = nullptr;                    // host query rows, copied chunk by chunk
+    std::vector<cudaEvent_t> up_ev;                 // one per copied chunk
     int32_t* h_state = nullptr;                     // pinned, two buffers of 1,024 cell states
     Profiler prof;
     sgr_mode mode = SGR_MODE_EXACT;
@@ -254,6 +256,7 @@ sgr_status guarded(sgr_ctx* ctx, F&& f) {
         ctx->err = e.what();
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         if (ctx->side) cudaStreamSynchronize(ctx->side);
+        if (ctx->copy) cudaStreamSynchronize(ctx->copy);  // no copy may read caller memory after return
         cudaGetLastError();
         ctx->prof.spans.clear();
         ctx->prof.used = 0;
@@ -339,7 +342,9 @@ struct DevCsr {
     int64_t nnz;  // -1 when unknown (device input)
 };
 
-DevCsr query_on_device(sgr_ctx* ctx, const sgr_csr* q) {
+// defer_rows (host input): only indptr is copied here and the value / index buffers are sized;
+// score_device copies the rows chunk by chunk, overlapped with the scoring of earlier chunks.
+DevCsr query_on_device(sgr_ctx* ctx, const sgr_csr* q, bool defer_rows = false) {
     check_csr_shape(q, "query");
     if (q->on_device) {
         int32_t nnz = 0;
@@ -351,6 +356,12 @@ DevCsr query_on_device(sgr_ctx* ctx, const sgr_csr* q) {
     }
     validate_host_csr(q, "query");
     const size_t nnz = (size_t)q->indptr[q->n_rows];
+    if (defer_rows) {
+        ctx->q_data.ensure(std::max<size_t>(nnz, 1));
+        ctx->q_indices.ensure(std::max<size_t>(nnz, 1));
+        ctx->q_indptr.upload(q->indptr, (size_t)q->n_rows + 1, ctx->stream);
+        return {ctx->q_data.p, ctx->q_indices.p, ctx->q_indptr.p, q->n_rows, q->n_cols, (int64_t)nnz};
+    }
     int sp = ctx->prof.begin(ST_H2D, ctx->stream);
     ctx->q_data.upload(q->data, nnz, ctx->stream);
     ctx->q_indices.upload(q->indices, nnz, ctx->stream);
@@ -381,6 +392,61 @@ void rank_rows(sgr_ctx* ctx, const DevCsr& m, const RankGroup& grp, int out_mode
     a.overflow = ctx->rank_overflow.ensure(std::max<uint32_t>(m.n_rows, 1));
     a.n_overflow = ctx->rank_n_overflow.ensure(1);
     launch_rank(a, ctx->stream);
+}
+
+// Gather + rank of rows [r0, r0 + n) of a device CSR; `group` (device) holds the outputs of row r0.
+void rank_range(sgr_ctx* ctx, const DevCsr& m, const RankGroup* group, int G, int Kp, uint32_t r0, uint32_t n,
+                int out_mode, int norm_mode) {
+    RankLaunch a{};
+    a.data = m.data;
+    a.indices = m.indices;
+    a.indptr = m.indptr;
+    a.n_cols = m.n_cols;
+    a.items = nullptr;
+    a.row0 = r0;
+    a.n_items = n;
+    a.groups = group;
+    a.out_mode = out_mode;
+    a.norm_mode = norm_mode;
+    a.max_Kp = Kp;
+    a.cap = sort_cap(G);
+    a.status = ctx->status.p;
+    a.overflow = ctx->rank_overflow.ensure(std::max<uint32_t>(n, 1));
+    a.n_overflow = ctx->rank_n_overflow.ensure(1);
+    launch_rank(a, ctx->stream);
+}
+
+// The context's copy stream, created on first use.
+cudaStream_t copy_stream(sgr_ctx* ctx) {
+    if (!ctx->copy) SGR_CUDA(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+    return ctx->copy;
+}
+
+// Copies the values and indices of a host query's rows into the device CSR buffers on the copy
+// stream, one row chunk at a time; ctx->up_ev[c] is recorded after chunk c.
+void copy_row_chunks(sgr_ctx* ctx, const sgr_csr* h, const DevCsr& q, uint32_t chunk, uint32_t n_chunks) {
+    cudaStream_t cs = copy_stream(ctx);
+    while (ctx->up_ev.size() < n_chunks) {
+        cudaEvent_t e;
+        SGR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->up_ev.push_back(e);
+    }
+    // the buffers may still be read by work queued earlier on the compute stream
+    SGR_CUDA(cudaEventRecord(ctx->up_ev[0], ctx->stream));
+    SGR_CUDA(cudaStreamWaitEvent(cs, ctx->up_ev[0], 0));
+    const int sp = ctx->prof.begin(ST_H2D, cs);
+    for (uint32_t c = 0; c < n_chunks; ++c) {
+        const uint32_t r0 = c * chunk, r1 = std::min(q.n_rows, r0 + chunk);
+        const size_t b = (size_t)h->indptr[r0], e = (size_t)h->indptr[r1];
+        if (e > b) {
+            SGR_CUDA(cudaMemcpyAsync(ctx->q_data.p + b, h->data + b, (e - b) * sizeof(float),
+                                     cudaMemcpyHostToDevice, cs));
+            SGR_CUDA(cudaMemcpyAsync(ctx->q_indices.p + b, h->indices + b, (e - b) * sizeof(int32_t),
+                                     cudaMemcpyHostToDevice, cs));
+        }
+        if (c + 1 == n_chunks) ctx->prof.end(sp, cs);
+        SGR_CUDA(cudaEventRecord(ctx->up_ev[c], cs));
+    }
 }
 
 // Compacts a device CSR to the columns with map >= 0 into (data, indices, indptr) buffers.
@@ -581,8 +647,10 @@ void correlate(sgr_ctx* ctx, bool fp32, const int8_t* A, int nq, uint32_t q0, fl
                        ctx->q_n2.p + q0, ctx->ref_n2.p, out, ld, ctx->status.p, ctx->stream, false, ext);
 }
 
-// Score-step device pass over the first nq rows of `q` (already device resident).
-void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
+// Score-step device pass over the rows of `q`.  host: the caller's host CSR when q's rows are not yet
+// on the device (query_on_device with defer_rows); they are copied chunk by chunk on the copy stream
+// and each chunk is ranked and scored once its rows have arrived.
+void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const sgr_csr* host = nullptr) {
     cudaStream_t s = ctx->stream;
     const uint32_t Q = q.n_rows, R = ctx->R, L = ctx->mk.n_labels;
     const bool fp32 = ctx->mode == SGR_MODE_FP32REF;
@@ -592,13 +660,31 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
     ctx->q_f32.ensure(Q);
     const bool f16 = ctx->corr_f16 && !fp32;
     if (f16) ensure_ref_f16(ctx);
-    RankGroup g{ctx->qry_map_common.p, ctx->G, ctx->Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p};
-    DevCsr qq = q;
-    const uint64_t l0 = launch_count();
-    int sp = ctx->prof.begin(ST_RANK, s);
-    rank_rows(ctx, qq, g, f16 ? RANK_F16 : RANK_LIMBS, fp32 ? NORM_SEQ : NORM_NONE);
-    ctx->prof.end(sp, s);
-    ctx->prof.acc.rank_launches += launch_count() - l0;
+    const uint32_t chunk =
+        (uint32_t)std::max<size_t>(1, std::min<size_t>(Q, ctx->score_chunk_bytes / (4 * (size_t)R)));
+    const uint32_t n_chunks = (Q + chunk - 1) / chunk;
+    // Rows already on the device are ranked in one launch.  Host rows are ranked chunk by chunk as
+    // they arrive: one rank group per chunk, each writing its own rows' limbs and norms.
+    const size_t row_bytes = (size_t)(f16 ? 2 : 3) * ctx->Kp;
+    const uint32_t n_groups = host ? n_chunks : 1;
+    std::vector<RankGroup> groups(n_groups);
+    for (uint32_t c = 0; c < n_groups; ++c) {
+        const size_t r0 = (size_t)c * chunk;
+        groups[c] = RankGroup{ctx->qry_map_common.p, ctx->G,          ctx->Kp,
+                              ctx->q_limbs.p + r0 * row_bytes, ctx->q_n2.p + r0, ctx->q_rinv.p + r0,
+                              ctx->q_f32.p + r0};
+    }
+    ctx->rank_groups.upload(groups, s);
+    const int rank_out = f16 ? RANK_F16 : RANK_LIMBS, rank_norm = fp32 ? NORM_SEQ : NORM_NONE;
+    if (host) {
+        copy_row_chunks(ctx, host, q, chunk, n_chunks);
+    } else {
+        const uint64_t l0 = launch_count();
+        const int sp = ctx->prof.begin(ST_RANK, s);
+        rank_range(ctx, q, ctx->rank_groups.p, ctx->G, ctx->Kp, 0, Q, rank_out, rank_norm);
+        ctx->prof.end(sp, s);
+        ctx->prof.acc.rank_launches += launch_count() - l0;
+    }
 
     std::vector<LabelQ> lq(L);
     bool any_nan_ref = false;
@@ -622,8 +708,6 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
     ctx->label_scores.ensure((size_t)Q * L);
     ctx->first.ensure(Q);
     ctx->flags.ensure((size_t)Q * L);
-    const uint32_t chunk =
-        (uint32_t)std::max<size_t>(1, std::min<size_t>(Q, ctx->score_chunk_bytes / (4 * (size_t)R)));
     ctx->scores.ensure((size_t)chunk * R);
     // the tensor-core correlation also writes each (query, label) list's extremes for the selection
     const bool tc_ext = !fp32 && !exact_simt();
@@ -634,8 +718,17 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre) {
         ext.kmin = ctx->ext_min.ensure((size_t)chunk * L);
         ext.kmax = ctx->ext_max.ensure((size_t)chunk * L);
     }
-    for (uint32_t q0 = 0; q0 < Q; q0 += chunk) {
+    for (uint32_t c = 0, q0 = 0; q0 < Q; ++c, q0 += chunk) {
         const int nq = (int)std::min(chunk, Q - q0);
+        int sp = -1;
+        if (host) {
+            SGR_CUDA(cudaStreamWaitEvent(s, ctx->up_ev[c], 0));
+            const uint64_t l0 = launch_count();
+            sp = ctx->prof.begin(ST_RANK, s);
+            rank_range(ctx, q, ctx->rank_groups.p + c, ctx->G, ctx->Kp, q0, (uint32_t)nq, rank_out, rank_norm);
+            ctx->prof.end(sp, s);
+            ctx->prof.acc.rank_launches += launch_count() - l0;
+        }
         const uint64_t c0 = launch_count();
         sp = ctx->prof.begin(ST_CORR, s);
         if (tc_ext) {
@@ -1246,7 +1339,12 @@ sgr_status sgr_destroy(sgr_ctx* ctx) {
     cudaStream_t s = ctx->own_stream, side = ctx->side;
     cudaEvent_t e1 = ctx->ev_fork, e2 = ctx->ev_join, e3 = ctx->ev_state[0], e4 = ctx->ev_state[1];
     int32_t* hs = ctx->h_state;
+    cudaStream_t cp = ctx->copy;
+    if (cp) cudaStreamSynchronize(cp);
+    std::vector<cudaEvent_t> up = ctx->up_ev;
     delete ctx;  // DevBuf destructors free device memory
+    if (cp) cudaStreamDestroy(cp);
+    for (cudaEvent_t e : up) cudaEventDestroy(e);
     if (s) cudaStreamDestroy(s);
     if (side) cudaStreamDestroy(side);
     if (e1) cudaEventDestroy(e1);
@@ -1398,9 +1496,9 @@ sgr_status sgr_score_first(sgr_ctx* ctx, const sgr_csr* qry, float quantile, flo
         if (!ctx->trained) fail(SGR_ERR_STATE, "score before train");
         if (!first_labels) fail(SGR_ERR_INVALID_ARGUMENT, "null first_labels");
         reset_status(ctx);
-        DevCsr q = query_on_device(ctx, qry);
+        DevCsr q = query_on_device(ctx, qry, true);
         if (q.n_rows == 0) return;
-        score_device(ctx, q, quantile, finetune_thre);
+        score_device(ctx, q, quantile, finetune_thre, qry->on_device ? nullptr : qry);
         const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
         cudaStream_t s = ctx->stream;
         SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -1436,9 +1534,9 @@ sgr_status sgr_annotate(sgr_ctx* ctx, const sgr_csr* qry, float quantile, float 
         if (!ctx->trained) fail(SGR_ERR_STATE, "annotate before train");
         if (!first_labels || !final_labels) fail(SGR_ERR_INVALID_ARGUMENT, "null output");
         reset_status(ctx);
-        DevCsr q = query_on_device(ctx, qry);
+        DevCsr q = query_on_device(ctx, qry, true);
         if (q.n_rows == 0) return;
-        score_device(ctx, q, quantile, finetune_thre);
+        score_device(ctx, q, quantile, finetune_thre, qry->on_device ? nullptr : qry);
         const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
         cudaStream_t s = ctx->stream;
         SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -1677,12 +1775,12 @@ sgr_status sgr_annotate_learned(sgr_ctx* ctx, const sgr_csr* qry, float quantile
         if (!ctx->mlp.ready || ctx->mlp.L != (int)ctx->mk.n_labels) fail(SGR_ERR_STATE, "no proposal network");
         if (!first_labels || !final_labels) fail(SGR_ERR_INVALID_ARGUMENT, "null output");
         reset_status(ctx);
-        DevCsr q = query_on_device(ctx, qry);
+        DevCsr q = query_on_device(ctx, qry, true);
         const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
         if (stats) *stats = sgr_learned_stats{};
         if (Q == 0) return;
         cudaStream_t s = ctx->stream;
-        score_device(ctx, q, quantile, finetune_thre);
+        score_device(ctx, q, quantile, finetune_thre, qry->on_device ? nullptr : qry);
         const int sp = ctx->prof.begin(ST_MLP, s);
         ctx->mlp_x.ensure((size_t)Q * L);
         ctx->mlp_bad.ensure(Q);

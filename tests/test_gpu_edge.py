@@ -163,6 +163,32 @@ def test_many_query_rows_tiled_scan():
     _run_both(prob, abi.MODE_EXACT)
 
 
+def test_host_rows_copied_in_chunks():
+    """A host query's rows are copied to the device one block of queries at a time, overlapped with
+    the scoring of the blocks before.  With 1 MiB score blocks the 9,000-row query takes about 21
+    blocks; scores, labels, flags and rounds equal the oracle's, through both the score-then-
+    fine-tune calls and the one-call annotation."""
+    w, ref, qry = synth.custom_dataset(600, 9000, 3000, 7, 0.08, seed=13)
+    prob = O.Problem(ref, qry, synth.names("CT", 7), ref.labels, synth.names("G", ref.n_cols),
+                     synth.names("G", qry.n_cols))
+    a = abi.Annotator(gpuid=0, mode=abi.MODE_EXACT)
+    a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
+    a.set_tuning(2, 1)
+    first, scores, flags = a.score_first(prob.qry)
+    final, rounds = a.finetune(prob.qry, flags)
+    orc = O.Oracle(prob)
+    orc.train()
+    of, os_, ofl, _ = orc.score(mode=1)
+    ofin, orounds = orc.finetune(mode=1)
+    assert H.ulp_diff(scores, os_).max() == 0
+    assert np.array_equal(first, of)
+    assert np.array_equal(flags, ofl.astype(np.uint8))
+    assert np.array_equal(final, ofin)
+    assert np.array_equal(rounds, orounds)
+    first2, final2 = a.annotate(prob.qry)
+    assert np.array_equal(first2, of) and np.array_equal(final2, ofin)
+
+
 def test_gene_intersection():
     ref, qry, L = H.dataset("tiny")
     rg = synth.names("G", ref.n_cols)
