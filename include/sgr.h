@@ -8,7 +8,9 @@
  *
  * Threading: one context is used by one host thread at a time.  Contexts are independent.
  * Memory: unless a sgr_csr says on_device = 1, every pointer is host memory; the library copies
- * what it needs and never keeps a caller pointer past the call.
+ * what it needs and never keeps a caller pointer past the call.  A host query's rows are copied one
+ * score block at a time on a stream of the context's own, overlapped with the scoring of the blocks
+ * before; from page-locked host memory the copies run at the link's speed.
  */
 #ifndef SGR_H_
 #define SGR_H_
@@ -109,7 +111,7 @@ sgr_status sgr_set_stream(sgr_ctx* ctx, void* stream);
 /* Per-stage device times of the calls since the last sgr_reset_timings, measured with CUDA events
  * on the context's stream while profiling is on (sgr_set_profiling(ctx, 1)). */
 typedef struct sgr_timings {
-    double h2d_ms;          /* query upload (host inputs only)                                 */
+    double h2d_ms;          /* query upload (host inputs only; overlaps the score step)        */
     double rank_ms;         /* score-step gather + rank of the query                            */
     double corr_ms;         /* score-step correlation                                            */
     double select_ms;       /* score-step quantile / argmax / flags                              */
