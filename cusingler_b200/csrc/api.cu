@@ -133,10 +133,10 @@ struct sgr_ctx {
     int corr_f16 = 0;              // tuning: score-step correlation on FP16 operands (not exact)
     DevBuf<uint16_t> ref_f16;      // reference ranks as IEEE half rows [R][Kp]
     bool ref_f16_ready = false;
-    DevBuf<int32_t> d_lorder;
-    DevBuf<int32_t> scan_part;  // tile sums of the filter's exclusive scan
+    DevBuf<int32_t> d_lorder;     // label ids by reference-cell count, longest first (score-step selection)
+    DevBuf<int32_t> scan_part;    // tile sums of the filter's exclusive scan
     DevBuf<int32_t> d_lstart;     // first reference column of each label (L + 1 entries)
-    DevBuf<uint32_t> ext_min, ext_max;  // per (query, label) score extremes of a score block  // label ids by reference-cell count, longest first (score-step selection)
+    DevBuf<uint32_t> ext_min, ext_max;  // per (query, label) score extremes of a score block
     DevBuf<RankItem> rank_overflow;  // rows ranked by the rank kernel's large-buffer tier
     DevBuf<int> rank_n_overflow;
     int ft_warps = 8;            // warps per CTA of the persistent fine-tune (8 or 32)
@@ -372,28 +372,6 @@ DevCsr query_on_device(sgr_ctx* ctx, const sgr_csr* q, bool defer_rows = false) 
 
 int sort_cap(int G) { return std::min(pow2_at_least(std::max(G, 32)), 4096); }
 
-// Gather + rank of rows [0, n) of a device CSR over one gene subset.
-void rank_rows(sgr_ctx* ctx, const DevCsr& m, const RankGroup& grp, int out_mode, int norm_mode) {
-    ctx->rank_groups.upload(&grp, 1, ctx->stream);
-    RankLaunch a{};
-    a.data = m.data;
-    a.indices = m.indices;
-    a.indptr = m.indptr;
-    a.n_cols = m.n_cols;
-    a.items = nullptr;
-    a.row0 = 0;
-    a.n_items = m.n_rows;
-    a.groups = ctx->rank_groups.p;
-    a.out_mode = out_mode;
-    a.norm_mode = norm_mode;
-    a.max_Kp = grp.Kp;
-    a.cap = sort_cap(grp.G);
-    a.status = ctx->status.p;
-    a.overflow = ctx->rank_overflow.ensure(std::max<uint32_t>(m.n_rows, 1));
-    a.n_overflow = ctx->rank_n_overflow.ensure(1);
-    launch_rank(a, ctx->stream);
-}
-
 // Gather + rank of rows [r0, r0 + n) of a device CSR; `group` (device) holds the outputs of row r0.
 void rank_range(sgr_ctx* ctx, const DevCsr& m, const RankGroup* group, int G, int Kp, uint32_t r0, uint32_t n,
                 int out_mode, int norm_mode) {
@@ -414,6 +392,12 @@ void rank_range(sgr_ctx* ctx, const DevCsr& m, const RankGroup* group, int G, in
     a.overflow = ctx->rank_overflow.ensure(std::max<uint32_t>(n, 1));
     a.n_overflow = ctx->rank_n_overflow.ensure(1);
     launch_rank(a, ctx->stream);
+}
+
+// Gather + rank of rows [0, n) of a device CSR over one gene subset.
+void rank_rows(sgr_ctx* ctx, const DevCsr& m, const RankGroup& grp, int out_mode, int norm_mode) {
+    ctx->rank_groups.upload(&grp, 1, ctx->stream);
+    rank_range(ctx, m, ctx->rank_groups.p, grp.G, grp.Kp, 0, m.n_rows, out_mode, norm_mode);
 }
 
 // The context's copy stream, created on first use.
