@@ -29,6 +29,7 @@ SYMBOLS = [
     "sgr_debug_stl_sort", "sgr_debug_stl_minmax", "sgr_set_stream", "sgr_set_profiling", "sgr_reset_timings",
     "sgr_get_timings", "sgr_select_labels_noalloc", "sgr_mlp_train", "sgr_mlp_predict", "sgr_mlp_params",
     "sgr_mlp_load", "sgr_mlp_debug_grads", "sgr_annotate_learned", "sgr_set_tuning", "sgr_autotune",
+    "sgr_annotate_stream",
 ]
 
 
@@ -50,7 +51,8 @@ class SgrTimings(C.Structure):
                 ("rank_bytes", C.c_uint64), ("corr_ops", C.c_uint64), ("cells", C.c_uint64),
                 ("ft_cell_rounds", C.c_uint64), ("mlp_ms", C.c_double), ("select_launches", C.c_uint64),
                 ("select_bytes", C.c_uint64), ("ft_queue_cells", C.c_uint64), ("ft_split_cells", C.c_uint64),
-                ("ft_split_rounds", C.c_uint64), ("ft_split_rows", C.c_uint64)]
+                ("ft_split_rounds", C.c_uint64), ("ft_split_rows", C.c_uint64), ("ft_cells", C.c_uint64),
+                ("ft_candidates", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -118,6 +120,8 @@ def lib():
             "sgr_reset_timings": (C.c_int, [vp]),
             "sgr_get_timings": (C.c_int, [vp, C.POINTER(SgrTimings)]),
             "sgr_select_labels_noalloc": (C.c_int, [vp, C.c_int64, u32, vp, u32, f32, f32, vp, vp, vp, vp]),
+            "sgr_annotate_stream": (C.c_int, [vp, vp, u32, f32, f32, i32, i32, f32, f32, vp, vp, vp,
+                                              C.POINTER(SgrLearnedStats)]),
             "sgr_mlp_train": (C.c_int, [vp, vp, vp, u32, C.POINTER(SgrMlpConfig), C.POINTER(f32)]),
             "sgr_mlp_predict": (C.c_int, [vp, vp, u32, vp, vp]),
             "sgr_mlp_params": (C.c_int, [vp, vp, C.c_uint64, C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_uint64)]),
@@ -278,6 +282,28 @@ class Annotator:
         self._check(self.L.sgr_annotate_learned(self.h, C.byref(csr), quantile, thre, times, min_confidence,
                                                 check_fraction, first.ctypes.data, final.ctypes.data, C.byref(st)))
         return first, final, st.as_dict()
+
+    def annotate_stream(self, batches, quantile=0.8, thre=0.05, times=0, learned=False, min_confidence=0.98,
+                        check_fraction=0.01):
+        """Annotate a sequence of host CSR batches (objects with n_rows, n_cols, data, indices, indptr,
+        or SgrCsr views of page-locked memory); batch i + 1 uploads while batch i runs.  Returns
+        (first, final, batch_ms, stats): labels of all rows in batch order, per-batch latency from
+        upload start to labels on the host, and the learned form's routing counts."""
+        views, keep = [], []
+        for b in batches:
+            c, k = self._csr(b)
+            views.append(c)
+            keep.append(k)
+        arr = (SgrCsr * max(1, len(views)))(*views)
+        n = sum(v.n_rows for v in views)
+        first = np.zeros(n, np.int32)
+        final = np.zeros(n, np.int32)
+        ms = np.zeros(len(views), np.float32)
+        st = SgrLearnedStats()
+        self._check(self.L.sgr_annotate_stream(self.h, C.cast(arr, C.c_void_p), len(views), quantile, thre, times,
+                                               1 if learned else 0, min_confidence, check_fraction,
+                                               first.ctypes.data, final.ctypes.data, ms.ctypes.data, C.byref(st)))
+        return first, final, ms, st.as_dict()
 
     def set_stream(self, stream_ptr):
         """Run on a caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream); None = own."""

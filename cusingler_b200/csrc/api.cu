@@ -39,6 +39,9 @@ struct Profiler {
     };
     std::vector<Span> spans;
     sgr_timings acc{};
+    // fine-tune rounds summed on the device (learned form), copied to pinned memory by the call
+    unsigned long long* h_rounds = nullptr;
+    bool rounds_pending = false;
 
     cudaEvent_t take() {
         if (used == pool.size()) {
@@ -60,6 +63,8 @@ struct Profiler {
     }
     // after the stream is synchronised
     void collect() {
+        if (rounds_pending && h_rounds) acc.ft_cell_rounds += *h_rounds;
+        rounds_pending = false;
         if (!on || spans.empty()) {
             spans.clear();
             used = 0;
@@ -80,6 +85,7 @@ struct Profiler {
     }
     ~Profiler() {
         for (auto e : pool) cudaEventDestroy(e);
+        if (h_rounds) cudaFreeHost(h_rounds);
     }
 };
 
@@ -155,6 +161,7 @@ struct sgr_ctx {
     DevBuf<int32_t> ft_order;
     DevBuf<int> ft_order_n;
     DevBuf<int32_t> d_final, d_rounds;
+    DevBuf<unsigned long long> d_round_sum;  // profiling: fine-tune rounds of the listed cells
     DevBuf<float> ft_scratch;
 
     // learned proposal
@@ -164,6 +171,12 @@ struct sgr_ctx {
     DevBuf<int32_t> mlp_y, mlp_idx, mlp_yb, prop, plain, route_final;
     DevBuf<float> mlp_xb, prop_conf, mlp_scores;
     DevBuf<int> n_plain;
+
+    // streamed query batches: two sets of CSR buffers (batch i + 1 uploads while batch i runs)
+    DevBuf<float> sq_data[2];
+    DevBuf<int32_t> sq_indices[2], sq_indptr[2];
+    cudaEvent_t sq_up_start[2] = {nullptr, nullptr}, sq_up_done[2] = {nullptr, nullptr};
+    cudaEvent_t sq_free[2] = {nullptr, nullptr}, sq_end = nullptr;
 
     // per-call query buffers
     DevBuf<float> q_data;
@@ -260,6 +273,7 @@ sgr_status guarded(sgr_ctx* ctx, F&& f) {
         cudaGetLastError();
         ctx->prof.spans.clear();
         ctx->prof.used = 0;
+        ctx->prof.rounds_pending = false;
         return e.code;
     } catch (const std::bad_alloc&) {
         ctx->err = "host allocation failed";
@@ -282,39 +296,6 @@ void validate_host_csr(const sgr_csr* m, const char* what) {
     for (uint32_t r = 0; r < m->n_rows; ++r)
         if (m->indptr[r + 1] < m->indptr[r])
             fail(SGR_ERR_INVALID_ARGUMENT, std::string(what) + ": indptr decreases at row " + std::to_string(r));
-}
-
-// LabelQ of a score list of `len` values at `start` for quantile p: the reference's float index
-// grid i * step with step = 1/(len-1), lower_bound of p (src/cusingler.cu:947-978).
-LabelQ make_lq(int start, int len, float p) {
-    LabelQ q{};
-    q.start = start;
-    q.len = len;
-    if (len <= 1) {
-        q.kind = 0;
-        return q;
-    }
-    const float step = 1.0 / (len - 1);
-    q.step = step;
-    const float first = 0 * step, last = (len - 1) * step;
-    if (p <= first) {
-        q.kind = 1;
-        return q;
-    }
-    if (last <= p) {
-        q.kind = 2;
-        return q;
-    }
-    int lo = 0, hi = len;
-    while (lo < hi) {
-        int mid = (lo + hi) / 2;
-        if (mid * step < p) lo = mid + 1;
-        else hi = mid;
-    }
-    q.kind = 3;
-    q.k = lo;
-    q.prev_index = (lo - 1) * step;
-    return q;
 }
 
 void check_status(sgr_ctx* ctx) {
@@ -807,9 +788,14 @@ void finetune_device(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags, float 
     DevCsr rf{ctx->reff_data.p, ctx->reff_indices.p, ctx->reff_indptr.p, ctx->R, std::max<uint32_t>(Wt, 1), -1};
 
     std::vector<CellState> st(Q);
-    for (uint32_t i = 0; i < Q; ++i)
+    for (uint32_t i = 0; i < Q; ++i) {
         for (uint32_t l = 0; l < L; ++l)
             if (flags[(size_t)i * L + l]) st[i].top.push_back((uint8_t)l);
+        if (st[i].top.size() >= 2 && times >= 0) {
+            ctx->prof.acc.ft_cells++;
+            ctx->prof.acc.ft_candidates += st[i].top.size();
+        }
+    }
 
     uint32_t max_label = 1;
     for (uint32_t l = 0; l < L; ++l) max_label = std::max(max_label, mk.ctidx[2 * l + 1]);
@@ -1034,6 +1020,8 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     const Markers& mk = ctx->mk;
     const uint32_t Q = q.n_rows, L = mk.n_labels, Wt = ctx->Wt;
     const int sp_ft = ctx->prof.begin(ST_FT, s);
+    const int32_t* listed = cell_list;  // the caller's cells (cell_list is replaced by the queue order)
+    const int* n_listed = n_list;
     // thre-pool rows of the cells to fine-tune (all cells, or only the listed ones)
     const uint8_t* row_mask = nullptr;
     if (cell_list) {
@@ -1121,6 +1109,10 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
             const int32_t c = cell_list ? list[i] : i;
             if (ncand[i] >= ctx->ft_heavy) heavy.push_back(c);
             else order.push_back(c);
+            if (ncand[i] >= 2) {  // a cell with two or more candidates runs at least one round
+                ctx->prof.acc.ft_cells++;
+                ctx->prof.acc.ft_candidates += (uint64_t)ncand[i];
+            }
         }
         int n_order = (int)order.size();
         ctx->prof.acc.ft_queue_cells += (uint64_t)n_order;
@@ -1267,7 +1259,18 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
         SGR_CUDA(cudaStreamWaitEvent(s, ctx->ev_join, 0));
     }
     ctx->prof.end(sp_ft, s);
-    if (!final_labels) return;  // caller reads ctx->d_final / d_rounds itself
+    if (!final_labels) {  // caller reads ctx->d_final / d_rounds itself
+        if (ctx->prof.on && listed) {  // rounds of the listed cells, summed on the device
+            if (!ctx->prof.h_rounds)
+                SGR_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->prof.h_rounds), sizeof(unsigned long long)));
+            unsigned long long* d = ctx->d_round_sum.ensure(1);
+            SGR_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), s));
+            launch_sum_listed(listed, n_listed, ctx->d_rounds.p, d, s);
+            SGR_CUDA(cudaMemcpyAsync(ctx->prof.h_rounds, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+            ctx->prof.rounds_pending = true;
+        }
+        return;
+    }
     SGR_CUDA(cudaMemcpyAsync(final_labels, ctx->d_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     std::vector<int32_t> rounds(Q);
     SGR_CUDA(cudaMemcpyAsync(rounds.data(), ctx->d_rounds.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -1275,6 +1278,164 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     for (uint32_t i = 0; i < Q; ++i) {
         if (rounds_out) rounds_out[i] = rounds[i];
         ctx->prof.acc.ft_cell_rounds += rounds[i];
+    }
+}
+
+// Plain form (score step, then the fine-tune) of a query whose rows are on the device, or are copied
+// block by block from `host` during the score step.  Results land in host arrays.
+void annotate_plain(sgr_ctx* ctx, const DevCsr& q, const sgr_csr* host, float quantile, float finetune_thre,
+                    int32_t finetune_times, int32_t* first_labels, int32_t* final_labels, float* label_scores) {
+    score_device(ctx, q, quantile, finetune_thre, host);
+    const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
+    cudaStream_t s = ctx->stream;
+    SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    if (label_scores)
+        SGR_CUDA(cudaMemcpyAsync(label_scores, ctx->label_scores.p, (size_t)Q * L * sizeof(float),
+                                 cudaMemcpyDeviceToHost, s));
+    if (ctx->mode == SGR_MODE_EXACT) {
+        finetune_persistent(ctx, q, ctx->flags.p, quantile, finetune_thre, finetune_times, final_labels, nullptr);
+    } else {
+        std::vector<uint8_t> fl((size_t)Q * L);
+        SGR_CUDA(cudaMemcpyAsync(fl.data(), ctx->flags.p, fl.size(), cudaMemcpyDeviceToHost, s));
+        check_status(ctx);
+        finetune_device(ctx, q, fl.data(), quantile, finetune_thre, finetune_times, final_labels, nullptr);
+    }
+}
+
+// Learned form (score step, proposal network, the plain fine-tune for routed cells) of a query whose
+// rows are on the device, or are copied block by block from `host` during the score step.
+void annotate_learned(sgr_ctx* ctx, const DevCsr& q, const sgr_csr* host, float quantile, float finetune_thre,
+                      int32_t finetune_times, float min_confidence, float check_fraction, int32_t* first_labels,
+                      int32_t* final_labels, sgr_learned_stats* stats, uint64_t row0 = 0) {
+    const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
+    cudaStream_t s = ctx->stream;
+    score_device(ctx, q, quantile, finetune_thre, host);
+    const int sp = ctx->prof.begin(ST_MLP, s);
+    ctx->mlp_x.ensure((size_t)Q * L);
+    ctx->mlp_bad.ensure(Q);
+    ctx->prop.ensure(Q);
+    ctx->prop_conf.ensure(Q);
+    ctx->route_final.ensure(Q);
+    ctx->plain.ensure(Q);
+    ctx->role.ensure(Q);
+    ctx->n_plain.ensure(1);
+    ctx->mlp.features(ctx->label_scores.p, (int)Q, ctx->mlp_x.p, ctx->mlp_bad.p, s);
+    ctx->mlp.predict(ctx->mlp_x.p, (int)Q, ctx->prop.p, ctx->prop_conf.p, s);
+    SGR_CUDA(cudaMemsetAsync(ctx->n_plain.p, 0, sizeof(int), s));
+    const uint32_t per10k = (uint32_t)std::lround(std::min(std::max(check_fraction, 0.f), 1.f) * 10000.f);
+    launch_learned_route((int)Q, (int)L, ctx->flags.p, ctx->mlp_bad.p, ctx->prop.p, ctx->prop_conf.p,
+                         min_confidence, per10k, 0x243F6A8885A308D3ull, row0, ctx->route_final.p, ctx->plain.p,
+                         ctx->n_plain.p, ctx->role.p, s);
+    ctx->prof.end(sp, s);
+    finetune_persistent(ctx, q, ctx->flags.p, quantile, finetune_thre, finetune_times, nullptr, nullptr,
+                        ctx->plain.p, ctx->n_plain.p);
+    std::vector<int32_t> rf(Q), ff(Q);
+    std::vector<uint8_t> role(Q);
+    SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SGR_CUDA(cudaMemcpyAsync(rf.data(), ctx->route_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SGR_CUDA(cudaMemcpyAsync(ff.data(), ctx->d_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SGR_CUDA(cudaMemcpyAsync(role.data(), ctx->role.p, Q, cudaMemcpyDeviceToHost, s));
+    check_status(ctx);
+    sgr_learned_stats st{};
+    st.cells = Q;
+    for (uint32_t i = 0; i < Q; ++i) {
+        if (role[i] == 0) {
+            final_labels[i] = rf[i];
+            st.decided++;
+        } else {
+            final_labels[i] = ff[i];
+            st.finetuned++;
+            if (role[i] == 2) {
+                st.checked++;
+                st.check_agree += rf[i] == ff[i];
+            }
+        }
+    }
+    if (stats) *stats = st;
+}
+
+// Streamed annotation of host query batches: batch i + 1's rows are uploaded on the copy stream into
+// the other of two CSR buffer sets while batch i is annotated on the compute stream.  batch_ms[i]
+// (may be NULL) receives the time from the start of batch i's upload to its labels on the host.
+void annotate_stream(sgr_ctx* ctx, const sgr_csr* batches, uint32_t n_batches, float quantile, float thre,
+                     int32_t times, bool learned, float min_confidence, float check_fraction, int32_t* first_labels,
+                     int32_t* final_labels, float* batch_ms, sgr_learned_stats* stats) {
+    size_t max_nnz = 1, max_rows = 1;
+    for (uint32_t b = 0; b < n_batches; ++b) {
+        const sgr_csr* m = batches + b;
+        check_csr_shape(m, "query batch");
+        if (m->on_device) fail(SGR_ERR_INVALID_ARGUMENT, "streamed query batches are host CSRs");
+        validate_host_csr(m, "query batch");
+        max_nnz = std::max<size_t>(max_nnz, (size_t)m->indptr[m->n_rows]);
+        max_rows = std::max<size_t>(max_rows, (size_t)m->n_rows + 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+        ctx->sq_data[i].ensure(max_nnz);
+        ctx->sq_indices[i].ensure(max_nnz);
+        ctx->sq_indptr[i].ensure(max_rows);
+        if (!ctx->sq_up_start[i]) {
+            SGR_CUDA(cudaEventCreate(&ctx->sq_up_start[i]));
+            SGR_CUDA(cudaEventCreateWithFlags(&ctx->sq_up_done[i], cudaEventDisableTiming));
+            SGR_CUDA(cudaEventCreateWithFlags(&ctx->sq_free[i], cudaEventDisableTiming));
+        }
+    }
+    if (!ctx->sq_end) SGR_CUDA(cudaEventCreate(&ctx->sq_end));
+    cudaStream_t s = ctx->stream, cs = copy_stream(ctx);
+    // both buffer sets are free once the work queued so far on the compute stream is done
+    for (int i = 0; i < 2; ++i) SGR_CUDA(cudaEventRecord(ctx->sq_free[i], s));
+    auto upload = [&](uint32_t b) {
+        const int k = b & 1;
+        const sgr_csr* m = batches + b;
+        const size_t nnz = (size_t)m->indptr[m->n_rows];
+        SGR_CUDA(cudaStreamWaitEvent(cs, ctx->sq_free[k], 0));
+        SGR_CUDA(cudaEventRecord(ctx->sq_up_start[k], cs));
+        const int sp = ctx->prof.begin(ST_H2D, cs);
+        SGR_CUDA(cudaMemcpyAsync(ctx->sq_indptr[k].p, m->indptr, ((size_t)m->n_rows + 1) * sizeof(int32_t),
+                                 cudaMemcpyHostToDevice, cs));
+        if (nnz) {
+            SGR_CUDA(cudaMemcpyAsync(ctx->sq_data[k].p, m->data, nnz * sizeof(float), cudaMemcpyHostToDevice, cs));
+            SGR_CUDA(cudaMemcpyAsync(ctx->sq_indices[k].p, m->indices, nnz * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                     cs));
+        }
+        ctx->prof.end(sp, cs);
+        SGR_CUDA(cudaEventRecord(ctx->sq_up_done[k], cs));
+    };
+    if (stats) *stats = sgr_learned_stats{};
+    if (n_batches) upload(0);
+    size_t row0 = 0;
+    for (uint32_t b = 0; b < n_batches; ++b) {
+        const int k = b & 1;
+        if (b + 1 < n_batches) upload(b + 1);
+        const sgr_csr* m = batches + b;
+        SGR_CUDA(cudaStreamWaitEvent(s, ctx->sq_up_done[k], 0));
+        DevCsr q{ctx->sq_data[k].p, ctx->sq_indices[k].p, ctx->sq_indptr[k].p, m->n_rows, m->n_cols,
+                 (int64_t)m->indptr[m->n_rows]};
+        if (m->n_rows) {
+            if (learned) {
+                sgr_learned_stats st{};
+                annotate_learned(ctx, q, nullptr, quantile, thre, times, min_confidence, check_fraction,
+                                 first_labels + row0, final_labels + row0, &st, row0);
+                if (stats) {
+                    stats->cells += st.cells;
+                    stats->decided += st.decided;
+                    stats->finetuned += st.finetuned;
+                    stats->checked += st.checked;
+                    stats->check_agree += st.check_agree;
+                }
+            } else {
+                annotate_plain(ctx, q, nullptr, quantile, thre, times, first_labels + row0, final_labels + row0,
+                               nullptr);
+            }
+        }
+        SGR_CUDA(cudaEventRecord(ctx->sq_free[k], s));
+        SGR_CUDA(cudaEventRecord(ctx->sq_end, s));
+        SGR_CUDA(cudaEventSynchronize(ctx->sq_end));
+        if (batch_ms) {
+            float ms = 0.f;
+            SGR_CUDA(cudaEventElapsedTime(&ms, ctx->sq_up_start[k], ctx->sq_end));
+            batch_ms[b] = ms;
+        }
+        row0 += m->n_rows;
     }
 }
 
@@ -1326,6 +1487,10 @@ sgr_status sgr_destroy(sgr_ctx* ctx) {
     cudaStream_t cp = ctx->copy;
     if (cp) cudaStreamSynchronize(cp);
     std::vector<cudaEvent_t> up = ctx->up_ev;
+    for (int i = 0; i < 2; ++i)
+        for (cudaEvent_t e : {ctx->sq_up_start[i], ctx->sq_up_done[i], ctx->sq_free[i]})
+            if (e) up.push_back(e);
+    if (ctx->sq_end) up.push_back(ctx->sq_end);
     delete ctx;  // DevBuf destructors free device memory
     if (cp) cudaStreamDestroy(cp);
     for (cudaEvent_t e : up) cudaEventDestroy(e);
@@ -1520,21 +1685,8 @@ sgr_status sgr_annotate(sgr_ctx* ctx, const sgr_csr* qry, float quantile, float 
         reset_status(ctx);
         DevCsr q = query_on_device(ctx, qry, true);
         if (q.n_rows == 0) return;
-        score_device(ctx, q, quantile, finetune_thre, qry->on_device ? nullptr : qry);
-        const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
-        cudaStream_t s = ctx->stream;
-        SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        if (label_scores)
-            SGR_CUDA(cudaMemcpyAsync(label_scores, ctx->label_scores.p, (size_t)Q * L * sizeof(float),
-                                     cudaMemcpyDeviceToHost, s));
-        if (ctx->mode == SGR_MODE_EXACT) {
-            finetune_persistent(ctx, q, ctx->flags.p, quantile, finetune_thre, finetune_times, final_labels, nullptr);
-        } else {
-            std::vector<uint8_t> fl((size_t)Q * L);
-            SGR_CUDA(cudaMemcpyAsync(fl.data(), ctx->flags.p, fl.size(), cudaMemcpyDeviceToHost, s));
-            check_status(ctx);
-            finetune_device(ctx, q, fl.data(), quantile, finetune_thre, finetune_times, final_labels, nullptr);
-        }
+        annotate_plain(ctx, q, qry->on_device ? nullptr : qry, quantile, finetune_thre, finetune_times, first_labels,
+                       final_labels, label_scores);
     });
 }
 
@@ -1760,53 +1912,28 @@ sgr_status sgr_annotate_learned(sgr_ctx* ctx, const sgr_csr* qry, float quantile
         if (!first_labels || !final_labels) fail(SGR_ERR_INVALID_ARGUMENT, "null output");
         reset_status(ctx);
         DevCsr q = query_on_device(ctx, qry, true);
-        const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
         if (stats) *stats = sgr_learned_stats{};
-        if (Q == 0) return;
-        cudaStream_t s = ctx->stream;
-        score_device(ctx, q, quantile, finetune_thre, qry->on_device ? nullptr : qry);
-        const int sp = ctx->prof.begin(ST_MLP, s);
-        ctx->mlp_x.ensure((size_t)Q * L);
-        ctx->mlp_bad.ensure(Q);
-        ctx->prop.ensure(Q);
-        ctx->prop_conf.ensure(Q);
-        ctx->route_final.ensure(Q);
-        ctx->plain.ensure(Q);
-        ctx->role.ensure(Q);
-        ctx->n_plain.ensure(1);
-        ctx->mlp.features(ctx->label_scores.p, (int)Q, ctx->mlp_x.p, ctx->mlp_bad.p, s);
-        ctx->mlp.predict(ctx->mlp_x.p, (int)Q, ctx->prop.p, ctx->prop_conf.p, s);
-        SGR_CUDA(cudaMemsetAsync(ctx->n_plain.p, 0, sizeof(int), s));
-        const uint32_t per10k = (uint32_t)std::lround(std::min(std::max(check_fraction, 0.f), 1.f) * 10000.f);
-        launch_learned_route((int)Q, (int)L, ctx->flags.p, ctx->mlp_bad.p, ctx->prop.p, ctx->prop_conf.p,
-                             min_confidence, per10k, 0x243F6A8885A308D3ull, ctx->route_final.p, ctx->plain.p,
-                             ctx->n_plain.p, ctx->role.p, s);
-        ctx->prof.end(sp, s);
-        finetune_persistent(ctx, q, ctx->flags.p, quantile, finetune_thre, finetune_times, nullptr, nullptr,
-                            ctx->plain.p, ctx->n_plain.p);
-        std::vector<int32_t> rf(Q), ff(Q);
-        std::vector<uint8_t> role(Q);
-        SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        SGR_CUDA(cudaMemcpyAsync(rf.data(), ctx->route_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        SGR_CUDA(cudaMemcpyAsync(ff.data(), ctx->d_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        SGR_CUDA(cudaMemcpyAsync(role.data(), ctx->role.p, Q, cudaMemcpyDeviceToHost, s));
-        check_status(ctx);
-        sgr_learned_stats st{};
-        st.cells = Q;
-        for (uint32_t i = 0; i < Q; ++i) {
-            if (role[i] == 0) {
-                final_labels[i] = rf[i];
-                st.decided++;
-            } else {
-                final_labels[i] = ff[i];
-                st.finetuned++;
-                if (role[i] == 2) {
-                    st.checked++;
-                    st.check_agree += rf[i] == ff[i];
-                }
-            }
+        if (q.n_rows == 0) return;
+        annotate_learned(ctx, q, qry->on_device ? nullptr : qry, quantile, finetune_thre, finetune_times,
+                         min_confidence, check_fraction, first_labels, final_labels, stats);
+    });
+}
+
+sgr_status sgr_annotate_stream(sgr_ctx* ctx, const sgr_csr* batches, uint32_t n_batches, float quantile,
+                               float finetune_thre, int32_t finetune_times, int32_t learned, float min_confidence,
+                               float check_fraction, int32_t* first_labels, int32_t* final_labels, float* batch_ms,
+                               sgr_learned_stats* stats) {
+    return guarded(ctx, [&] {
+        if (!ctx->trained) fail(SGR_ERR_STATE, "annotate before train");
+        if (n_batches && !batches) fail(SGR_ERR_INVALID_ARGUMENT, "null batch array");
+        if (!first_labels || !final_labels) fail(SGR_ERR_INVALID_ARGUMENT, "null output");
+        if (learned) {
+            if (ctx->mode != SGR_MODE_EXACT) fail(SGR_ERR_STATE, "the learned form runs in exact mode");
+            if (!ctx->mlp.ready || ctx->mlp.L != (int)ctx->mk.n_labels) fail(SGR_ERR_STATE, "no proposal network");
         }
-        if (stats) *stats = st;
+        reset_status(ctx);
+        annotate_stream(ctx, batches, n_batches, quantile, finetune_thre, finetune_times, learned != 0,
+                        min_confidence, check_fraction, first_labels, final_labels, batch_ms, stats);
     });
 }
 

@@ -600,12 +600,19 @@ uint64_t launch_count() { return g_launches.load(); }
 void count_launch(uint64_t n) { g_launches += n; }
 
 int device_sm_count() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
+    // cached per device: launch shapes use the SM count of whichever device is current
+    constexpr int kMaxDevices = 64;
+    static std::atomic<int> cached[kMaxDevices];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxDevices) dev = 0;
+    int n = cached[dev].load(std::memory_order_relaxed);
+    if (n <= 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+            cudaGetLastError();
+            n = 148;
+        }
+        cached[dev].store(n, std::memory_order_relaxed);  // every thread stores the same value
     }
     return n;
 }
@@ -667,6 +674,22 @@ __global__ void mark_rows_kernel(const int32_t* list, int n, uint8_t* mask) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) mask[list[i]] = 1;
 }
 }  // namespace
+
+namespace {
+__global__ void sum_listed_kernel(const int32_t* list, const int* n, const int32_t* vals, unsigned long long* out) {
+    unsigned long long t = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < *n; i += gridDim.x * blockDim.x) t += (unsigned)vals[list[i]];
+    t = __reduce_add_sync(0xffffffffu, (unsigned)t);
+    if ((threadIdx.x & 31) == 0 && t) atomicAdd(out, t);
+}
+}  // namespace
+
+void launch_sum_listed(const int32_t* list, const int* n, const int32_t* vals, unsigned long long* out,
+                       cudaStream_t s) {
+    sum_listed_kernel<<<sm_count(), 256, 0, s>>>(list, n, vals, out);
+    SGR_LAUNCH_CHECK();
+    count_launch();
+}
 
 void launch_mark_rows(const int32_t* list, int n, uint8_t* mask, cudaStream_t s) {
     if (n <= 0) return;
@@ -765,6 +788,37 @@ void launch_corr_simt(bool fp32ref, const int8_t* A, const int8_t* B, int nq, in
         corr_simt_kernel<false><<<grid, 256, 0, s>>>(A, B, nq, R, G, Kp, fa, fb, ra, rb, na, nb, scores, ld);
     SGR_LAUNCH_CHECK();
     count_launch();
+}
+
+LabelQ make_lq(int start, int len, float p) {
+    LabelQ q{};
+    q.start = start;
+    q.len = len;
+    if (len <= 1) {
+        q.kind = 0;
+        return q;
+    }
+    const float step = 1.0 / (len - 1);
+    q.step = step;
+    const float first = 0 * step, last = (len - 1) * step;
+    if (p <= first) {
+        q.kind = 1;
+        return q;
+    }
+    if (last <= p) {
+        q.kind = 2;
+        return q;
+    }
+    int lo = 0, hi = len;
+    while (lo < hi) {
+        int mid = (lo + hi) / 2;
+        if (mid * step < p) lo = mid + 1;
+        else hi = mid;
+    }
+    q.kind = 3;
+    q.k = lo;
+    q.prev_index = (lo - 1) * step;
+    return q;
 }
 
 void launch_select_first(const float* scores, int64_t ld, int nq, int L, const LabelQ* lq, float p, float thre,

@@ -78,6 +78,10 @@ void launch_rank(const RankLaunch& a, cudaStream_t s);
 void launch_filter_count(const int32_t* indptr, const int32_t* indices, uint32_t n_rows, uint32_t n_cols,
                          const int32_t* map, int32_t* counts, cudaStream_t s,
                          const uint8_t* row_mask = nullptr);
+// *out += sum of vals[list[i]] for i < *n (n read on the device; *out is not cleared; each value is
+// below 2^32 and a warp's partial sum too).
+void launch_sum_listed(const int32_t* list, const int* n, const int32_t* vals, unsigned long long* out,
+                       cudaStream_t s);
 // mask[list[i]] = 1 for i < n (list entries must be valid rows of mask).
 void launch_mark_rows(const int32_t* list, int n, uint8_t* mask, cudaStream_t s);
 // out[i] = in[0] + ... + in[i-1] for i <= n.  scratch (optional): 2 * ceil(n / 4096) + 1 ints, which
@@ -108,6 +112,10 @@ struct LabelQ {
     int32_t has_nan;     // some reference row of the label has zero variance
     int32_t pad;
 };
+
+// LabelQ of a score list of `len` values at `start` for quantile p: the reference's float index
+// grid i * step with step = 1/(len-1), lower_bound of p (src/cusingler.cu:947-978).  Host function.
+LabelQ make_lq(int start, int len, float p);
 
 // row_len: floats of a score row that the labels cover.  With `lorder` (label ids, longest first)
 // and rows of at most 200 KB, each block stages its row in shared memory before selecting.

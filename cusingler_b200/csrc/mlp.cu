@@ -319,7 +319,8 @@ unsigned blocks_for(int64_t n) { return (unsigned)std::min<int64_t>((n + 255) / 
 // (fallback), 2 plain (check sample; its proposal is kept in final_labels for the comparison).
 __global__ void learned_route_kernel(int Q, int L, const uint8_t* flags, const uint8_t* bad, const int32_t* prop,
                                      const float* conf, float min_conf, uint32_t check_per_10k, uint64_t seed,
-                                     int32_t* final_labels, int32_t* plain, int* n_plain, uint8_t* role) {
+                                     uint64_t row0, int32_t* final_labels, int32_t* plain, int* n_plain,
+                                     uint8_t* role) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= Q) return;
     const uint8_t* f = flags + (int64_t)q * L;
@@ -334,7 +335,9 @@ __global__ void learned_route_kernel(int Q, int L, const uint8_t* flags, const u
         role[q] = 0;
         return;
     }
-    uint64_t z = seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(q + 1));
+    // the check sample is a hash of the cell's row in the whole query (row0: the batch's first row),
+    // so that a query annotated in batches checks the same cells as in one call
+    uint64_t z = seed ^ (0x9E3779B97F4A7C15ull * (row0 + (uint64_t)q + 1));
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     z ^= z >> 31;
@@ -354,11 +357,11 @@ __global__ void learned_route_kernel(int Q, int L, const uint8_t* flags, const u
 }  // namespace
 
 void launch_learned_route(int Q, int L, const uint8_t* flags, const uint8_t* bad, const int32_t* prop,
-                          const float* conf, float min_conf, uint32_t check_per_10k, uint64_t seed,
+                          const float* conf, float min_conf, uint32_t check_per_10k, uint64_t seed, uint64_t row0,
                           int32_t* final_labels, int32_t* plain, int* n_plain, uint8_t* role, cudaStream_t s) {
     if (Q <= 0) return;
     learned_route_kernel<<<(Q + 255) / 256, 256, 0, s>>>(Q, L, flags, bad, prop, conf, min_conf, check_per_10k, seed,
-                                                         final_labels, plain, n_plain, role);
+                                                         row0, final_labels, plain, n_plain, role);
     SGR_LAUNCH_CHECK();
     count_launch();
 }

@@ -31,7 +31,7 @@ struct Mlp {
 // Route cells for the learned form: cells whose proposal is confident, a candidate, and not
 // sampled for checking keep the proposal; the rest are appended to `plain` (device list).
 void launch_learned_route(int Q, int L, const uint8_t* flags, const uint8_t* bad, const int32_t* prop,
-                          const float* conf, float min_conf, uint32_t check_per_10k, uint64_t seed,
+                          const float* conf, float min_conf, uint32_t check_per_10k, uint64_t seed, uint64_t row0,
                           int32_t* final_labels, int32_t* plain, int* n_plain, uint8_t* role, cudaStream_t s);
 
 }  // namespace sgr

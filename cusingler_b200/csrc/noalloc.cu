@@ -40,14 +40,29 @@ __global__ void __launch_bounds__(256) select_noalloc_kernel(const float* scores
     __shared__ float ls[256];
     __shared__ int hist[8][256];
     __shared__ int s_mx;
-    __shared__ int dummy_status;
+    // Status bits of the selection are not reported by this entry point: it only enqueues work and
+    // has no context to return them through.  Bit 8 (no sort scratch) cannot arise, the scratch is
+    // always present; bit 4 (a NaN-bearing list on which libstdc++ would read outside the array,
+    // sorted within bounds instead) is not reported by the main path either.
+    __shared__ int ignored_status;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) ignored_status = 0;
+    __syncthreads();
     float* my_scratch = scratch + (size_t)(blockIdx.x * 8 + warp) * spw;
     for (int q = blockIdx.x; q < nq; q += gridDim.x) {
         const float* row = scores + (size_t)q * ld;
         for (int l = warp; l < L; l += 8) {
             const LabelQ d = lt.q[l];
-            const float r = quantile_warp(row + d.start, d, p, hist[warp], my_scratch, lane, &dummy_status);
+            // a constant query row makes every score NaN: the quantile of an all-NaN list is NaN for
+            // every grid position, so such lists skip the sort (checked only when the first score is NaN)
+            bool all_nan = false;
+            if (row[d.start] != row[d.start]) {
+                bool any = false;
+                for (int i = lane; i < d.len; i += 32) any |= row[d.start + i] == row[d.start + i];
+                all_nan = !__any_sync(0xffffffffu, any);
+            }
+            const float r = all_nan ? __int_as_float(0x7fffffff)
+                                    : quantile_warp(row + d.start, d, p, hist[warp], my_scratch, lane, &ignored_status);
             if (lane == 0) ls[l] = r;
         }
         __syncthreads();
@@ -105,30 +120,7 @@ extern "C" sgr_status sgr_select_labels_noalloc(const float* d_scores, int64_t l
         if ((uint64_t)start + len > (uint64_t)ld) return SGR_ERR_INVALID_ARGUMENT;
         max_len = std::max(max_len, len);
         // the reference's float index grid (src/cusingler.cu:947-978 of STOmics/cusingler)
-        LabelQ& q = lt.q[l];
-        q.start = (int32_t)start;
-        q.len = (int32_t)len;
-        if (len <= 1) {
-            q.kind = 0;
-            continue;
-        }
-        const float step = 1.0 / (len - 1);
-        q.step = step;
-        if (quantile <= 0 * step) {
-            q.kind = 1;
-        } else if ((int)(len - 1) * step <= quantile) {
-            q.kind = 2;
-        } else {
-            int lo = 0, hi = (int)len;
-            while (lo < hi) {
-                const int mid = (lo + hi) / 2;
-                if (mid * step < quantile) lo = mid + 1;
-                else hi = mid;
-            }
-            q.kind = 3;
-            q.k = lo;
-            q.prev_index = (lo - 1) * step;
-        }
+        lt.q[l] = make_lq((int)start, (int)len, quantile);
     }
     // eight warps per block, each with its own max_len-float slice of the fixed scratch array
     const long fit_blocks = (long)kNoallocScratchFloats / (8L * max_len);

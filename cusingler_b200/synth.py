@@ -89,6 +89,17 @@ class CSR:
                    (self.indptr[start:stop + 1] - a).astype(self.indptr.dtype),
                    self.labels[start:stop])
 
+    def take(self, rows) -> "CSR":
+        """The given rows (any order, repeats allowed) as a new CSR."""
+        rows = np.asarray(rows, dtype=np.int64)
+        lens = (self.indptr[rows + 1] - self.indptr[rows]).astype(np.int64)
+        indptr = np.zeros(rows.shape[0] + 1, dtype=np.int64)
+        np.cumsum(lens, out=indptr[1:])
+        src = np.repeat(self.indptr[rows].astype(np.int64) - indptr[:-1], lens) + np.arange(indptr[-1])
+        idt = np.int32 if indptr[-1] < 2**31 else np.int64
+        return CSR(rows.shape[0], self.n_cols, self.data[src], self.indices[src], indptr.astype(idt),
+                   self.labels[rows])
+
 
 def make_world(wl: Workload, seed: int = 0) -> World:
     rng = np.random.default_rng([seed, 7919])

@@ -131,6 +131,8 @@ typedef struct sgr_timings {
     uint64_t ft_split_cells;/* fine-tune cells whose rounds were spread over the GPU             */
     uint64_t ft_split_rounds;/* rounds of the spread path (each: prepare, scan, decide launches)  */
     uint64_t ft_split_rows; /* reference rows scored by the spread path, summed over its rounds   */
+    uint64_t ft_cells;      /* cells that ran at least one fine-tune round                      */
+    uint64_t ft_candidates; /* first-round candidate labels of those cells, summed               */
 } sgr_timings;
 
 sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
@@ -222,6 +224,23 @@ sgr_status sgr_annotate_learned(sgr_ctx* ctx, const sgr_csr* qry, float quantile
                                 int32_t finetune_times, float min_confidence, float check_fraction,
                                 int32_t* first_labels, int32_t* final_labels, sgr_learned_stats* stats);
 
+/* ---- Streaming ----------------------------------------------------------------------------- */
+
+/* Replaces the reference's query slicing (src/cusingler.cu:335-409: copyin_score cuts the query
+ * into slices that fit the free device memory and get_label scores them one after another) for a
+ * query that arrives as a sequence of host CSR batches, e.g. 65,536 cells each.  The reference stays
+ * resident; batch i + 1 is uploaded on the context's copy stream into the second of two device
+ * buffer sets while batch i is annotated, so with page-locked batches the upload is hidden behind
+ * the previous batch's work.  learned = 0 runs the plain form (sgr_annotate), 1 the learned form
+ * (sgr_annotate_learned with min_confidence / check_fraction; stats summed over batches, may be
+ * NULL).  first_labels / final_labels hold the batches' rows one after another (sum of n_rows).
+ * batch_ms (n_batches, may be NULL) receives, per batch, the time from the start of its upload to
+ * its labels on the host. */
+sgr_status sgr_annotate_stream(sgr_ctx* ctx, const sgr_csr* batches, uint32_t n_batches, float quantile,
+                               float finetune_thre, int32_t finetune_times, int32_t learned,
+                               float min_confidence, float check_fraction, int32_t* first_labels,
+                               int32_t* final_labels, float* batch_ms, sgr_learned_stats* stats);
+
 /* ---- Allocation-free selection -------------------------------------------------------------- */
 
 /* This entry point has no counterpart in the reference.  It is for callers that cannot allocate
@@ -244,7 +263,10 @@ sgr_status sgr_annotate_learned(sgr_ctx* ctx, const sgr_csr* qry, float quantile
  * hold at most 131,072 reference columns (SGR_ERR_UNSUPPORTED beyond).  All calls share that
  * array, so calls that overlap on the GPU (other streams, other threads) race and must be
  * serialised by the caller.  The first call on a device looks the array's address up; make that
- * first call before any stream capture. */
+ * first call before any stream capture.  Because the call only enqueues, device-side conditions
+ * that sgr_score_first reports through its status (a NaN input value, an out-of-range column) are
+ * not checked here: the scores are the caller's, and a NaN-bearing list is sorted in libstdc++
+ * order within its bounds, as in the main path. */
 sgr_status sgr_select_labels_noalloc(const float* d_scores, int64_t ld, uint32_t n_rows,
                                      const uint32_t* label_ranges, uint32_t n_labels, float quantile,
                                      float finetune_thre, float* d_label_scores,

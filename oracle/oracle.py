@@ -27,10 +27,11 @@ MODE_FP32REF = 0
 MODE_EXACT = 1
 
 
-def build(ref: bool = False) -> None:
-    """Compile the oracle (and, with ref=True and the reference sources present, oracle/_ref)."""
+def build(ref: bool = False, ref_src: str | None = None) -> None:
+    """Compile the oracle (and, with ref=True, oracle/_ref from the reference sources in ref_src)."""
     targets = ["all"] + (["ref"] if ref else [])
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    extra = [f"REF={ref_src}"] if ref and ref_src else []
+    subprocess.run(["make", "-s", "-C", HERE] + targets + extra, check=True)
 
 
 def _strs(xs):
@@ -73,6 +74,7 @@ def lib():
                                    C.c_void_p, C.c_void_p]),
             "or_finetune": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_int, C.c_int, _i32p, C.c_void_p]),
             "or_set_flags": (None, [C.c_void_p, _f32p]),
+            "or_margins": (None, [C.c_void_p, C.c_int, _f32p]),
             "or_percentile": (C.c_float, [_f32p, C.c_int, C.c_float]),
             "or_minmax": (None, [_f32p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
             "or_sort": (None, [_f32p, C.c_int]),
@@ -206,6 +208,16 @@ class Oracle:
         if rc:
             raise RuntimeError(self.error())
         return first, scores, flags, raw_arr
+
+    def margins(self, which: int) -> np.ndarray:
+        """Per query cell, the smallest distance between a label score and a value it was compared
+        with (the maximum, the minimum, the keep bound) in the last score (which 0) or fine-tune
+        (which 1, every round and the score step) call.  A label that differs between the exact and
+        the FP32-order arithmetic with a margin below the score difference of the two (< 1e-5) is a
+        near-tie."""
+        out = np.zeros(self.p.qry.n_rows, np.float32)
+        self.L.or_margins(self.h, which, out)
+        return out
 
     def set_flags(self, flags):
         self.L.or_set_flags(self.h, np.ascontiguousarray(flags, np.float32))

@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -78,6 +79,11 @@ struct Ctx {
     std::vector<float> label_scores;  // Q x L
     std::vector<float> flags;         // Q x L (the reference's float `labels`, src/types.h:34)
     std::vector<int> first;
+    // Decision margins per query cell (for near-tie checks of arithmetic-order label flips): the
+    // smallest distance, over every keep / drop / argmax comparison the cell's labels went
+    // through, between a score and the value it was compared with.  margin_first covers the score
+    // step, margin_final the score step and every fine-tune round.
+    std::vector<float> margin_first, margin_final;
     bool trained = false, scored = false;
 };
 
@@ -437,6 +443,21 @@ std::pair<int, int> minmax_idx(const float* v, int n) {
     return {int(e.first - v), int(e.second - v)};
 }
 
+// Smallest distance between a score of `v` and the thresholds it is compared with: the maximum
+// (argmax), the minimum (the fine-tune's `<= min` drop, when `with_min`) and `t` (the keep bound);
+// NaN scores are skipped.  A label decision can only change under score perturbations of at least
+// half this margin.
+float decision_margin(const float* v, int n, int mn, int mx, float t, bool with_min) {
+    float m = std::numeric_limits<float>::infinity();
+    for (int i = 0; i < n; ++i) {
+        if (std::isnan(v[i])) continue;
+        m = std::min(m, std::fabs(v[i] - t));
+        if (i != mx && !std::isnan(v[mx])) m = std::min(m, v[mx] - v[i]);
+        if (with_min && i != mn && !std::isnan(v[mn])) m = std::min(m, v[i] - v[mn]);
+    }
+    return m;
+}
+
 // src/cusingler.cu:986-1136 (get_label) without slicing: every ref row in one pass.
 bool score(Ctx& c, float q, float thre, int mode, int* first_out, float* scores_out, float* flags_out,
            float* raw_out) {
@@ -452,6 +473,7 @@ bool score(Ctx& c, float q, float thre, int mode, int* first_out, float* scores_
     c.label_scores.assign((size_t)Q * L, 0.f);
     c.flags.assign((size_t)Q * L, 0.f);
     c.first.assign(Q, 0);
+    c.margin_first.assign(Q, std::numeric_limits<float>::infinity());
     parallel_for(c.cores, Q, [&](size_t qi) {
         std::vector<uint16_t> codes(G);
         dense_codes(c.qry_s, qi, G, codes.data());
@@ -474,6 +496,7 @@ bool score(Ctx& c, float q, float thre, int mode, int* first_out, float* scores_
         float t = ls[mm.second] - thre;
         for (uint32_t l = 0; l < L; ++l)
             if (ls[l] >= t) c.flags[qi * L + l] = 1;
+        c.margin_first[qi] = decision_margin(ls, (int)L, mm.first, mm.second, t, false);
     });
     if (first_out) std::copy(c.first.begin(), c.first.end(), first_out);
     if (scores_out) std::copy(c.label_scores.begin(), c.label_scores.end(), scores_out);
@@ -484,7 +507,7 @@ bool score(Ctx& c, float q, float thre, int mode, int* first_out, float* scores_
 
 // src/cusingler.cu:1138-1296 (finetune_round).
 std::vector<uint32_t> finetune_round(const Ctx& c, uint32_t cell, const std::vector<uint32_t>& top, float q,
-                                     float thre, int mode) {
+                                     float thre, int mode, float* margin) {
     const uint32_t L = c.label_names.size();
     std::set<uint32_t> uniq;
     int gene_thre = std::round(500 * std::pow(2 / 3.0, std::log2((double)top.size())));
@@ -523,6 +546,7 @@ std::vector<uint32_t> finetune_round(const Ctx& c, uint32_t cell, const std::vec
     float mn = scores[mm.first], mx = scores[mm.second];
     float t = mx - thre;
     if (std::isnan(mx)) return {top.front()};
+    *margin = std::min(*margin, decision_margin(scores.data(), (int)scores.size(), mm.first, mm.second, t, true));
     std::vector<uint32_t> res;
     for (uint32_t i = 0; i < scores.size(); ++i) {
         if (scores[i] <= mn || scores[i] < t) continue;
@@ -538,15 +562,18 @@ std::vector<uint32_t> finetune_round(const Ctx& c, uint32_t cell, const std::vec
 // src/cusingler.cu:1297-1333 (cufinetune).
 bool finetune(Ctx& c, float q, float thre, int times, int mode, int* final_out, int* rounds_out) {
     const uint32_t L = c.label_names.size();
+    c.margin_final.assign(c.qry_h, std::numeric_limits<float>::infinity());
     parallel_for(c.cores, c.qry_h, [&](size_t i) {
         std::vector<uint32_t> top;
         for (uint32_t l = 0; l < L; ++l)
             if (c.flags.at(i * L + l) != 0) top.push_back(l);
         int t = 0, rounds = 0;
+        float margin = i < c.margin_first.size() ? c.margin_first[i] : std::numeric_limits<float>::infinity();
         while (top.size() > 1 && (times == 0 || t++ < times)) {
-            top = finetune_round(c, i, top, q, thre, mode);
+            top = finetune_round(c, i, top, q, thre, mode, &margin);
             rounds++;
         }
+        c.margin_final[i] = margin;
         final_out[i] = top.empty() ? 0 : (int)top.front();
         if (rounds_out) rounds_out[i] = rounds;
     });
@@ -653,6 +680,13 @@ int or_finetune(void* h, float quantile, float thre, int times, int mode, int* f
     Ctx& c = *static_cast<Ctx*>(h);
     if (!c.scored) return 1;
     return finetune(c, quantile, thre, times, mode, final_labels, rounds) ? 0 : 1;
+}
+
+// Decision margins of the last score (which 0) or fine-tune (which 1) call, one per query cell.
+void or_margins(void* h, int which, float* out) {
+    Ctx& c = *static_cast<Ctx*>(h);
+    const std::vector<float>& m = which == 0 ? c.margin_first : c.margin_final;
+    std::copy(m.begin(), m.end(), out);
 }
 
 // Overrides the first-round flags (Q x L) so that fine-tune can be checked on its own.

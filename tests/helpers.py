@@ -38,8 +38,21 @@ def oracle_run(kind: str, mode: int, times: int = 0):
     orc = O.Oracle(problem(kind))
     orc.train()
     first, scores, flags, raw = orc.score(mode=mode, raw=True)
+    margin_first = orc.margins(0)
     final, rounds = orc.finetune(mode=mode, times=times)
-    return dict(first=first, scores=scores, flags=flags, raw=raw, final=final, rounds=rounds, oracle=orc)
+    return dict(first=first, scores=scores, flags=flags, raw=raw, final=final, rounds=rounds, oracle=orc,
+                margin_first=margin_first, margin_final=orc.margins(1))
+
+
+NEAR_TIE = 1e-5  # exact and FP32-order scores differ by less than this (tested per score)
+
+
+def unexplained_flips(labels, ref_labels, margins, tol=NEAR_TIE):
+    """Cells whose label differs from `ref_labels` although the oracle's decision margin there is
+    at least `tol` (a flip that arithmetic order cannot explain).  Empty when every difference is a
+    near-tie."""
+    diff = np.nonzero(np.asarray(labels) != np.asarray(ref_labels))[0]
+    return diff[~(np.asarray(margins)[diff] < tol)]
 
 
 def ulp_diff(a, b):

@@ -163,12 +163,21 @@ def test_many_query_rows_tiled_scan():
     _run_both(prob, abi.MODE_EXACT)
 
 
-def test_host_rows_copied_in_chunks():
+@pytest.mark.parametrize("pinned", [False, True])
+def test_host_rows_copied_in_chunks(pinned):
     """A host query's rows are copied to the device one block of queries at a time, overlapped with
     the scoring of the blocks before.  With 1 MiB score blocks the 9,000-row query takes about 21
     blocks; scores, labels, flags and rounds equal the oracle's, through both the score-then-
-    fine-tune calls and the one-call annotation."""
+    fine-tune calls and the one-call annotation.  From pageable memory every copy has landed before
+    the call returns from queuing it; from page-locked memory the copies really run behind the
+    scoring, so the waits between the copy stream and the compute stream are exercised."""
     w, ref, qry = synth.custom_dataset(600, 9000, 3000, 7, 0.08, seed=13)
+    keep = None
+    if pinned:
+        import torch
+        pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory()  # noqa: E731
+        keep = (pin(qry.data), pin(qry.indices), pin(qry.indptr.astype(np.int32)))
+        qry = synth.CSR(qry.n_rows, qry.n_cols, keep[0].numpy(), keep[1].numpy(), keep[2].numpy(), qry.labels)
     prob = O.Problem(ref, qry, synth.names("CT", 7), ref.labels, synth.names("G", ref.n_cols),
                      synth.names("G", qry.n_cols))
     a = abi.Annotator(gpuid=0, mode=abi.MODE_EXACT)
@@ -249,3 +258,35 @@ def test_autotune_keeps_results():
     first, final = a.annotate(prob.qry)
     o = H.oracle_run("families", 1)
     assert np.array_equal(first, o["first"]) and np.array_equal(final, o["final"])
+
+
+@pytest.mark.parametrize("learned", [False, True])
+def test_stream_of_batches_matches_one_call(learned):
+    """sgr_annotate_stream over uneven page-locked batches (one of them empty) gives the labels of
+    one sgr_annotate / sgr_annotate_learned call over the whole query, and per-batch latencies."""
+    import torch
+
+    prob = H.problem("families")
+    a = abi.Annotator(gpuid=0)
+    a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
+    q = prob.qry
+    if learned:
+        f0, fin0, sc = a.annotate(q, with_scores=True)
+        a.mlp_train(sc, fin0, epochs=5, batch=64, seed=1)
+        want_first, want_final, _ = a.annotate_learned(q, min_confidence=0.9, check_fraction=0.2)
+    else:
+        want_first, want_final = a.annotate(q)
+    cuts = [0, 37, 37, 120, q.n_rows]
+    pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory()  # noqa: E731
+    batches, keep = [], []
+    for lo, hi in zip(cuts, cuts[1:]):
+        part = q.rows(lo, hi)
+        t = (pin(part.data), pin(part.indices), pin(part.indptr.astype(np.int32)))
+        keep.append(t)
+        batches.append(abi.SgrCsr(part.n_rows, part.n_cols, t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), 0))
+    for _ in range(2):  # the second call reuses the context's batch buffers
+        first, final, ms, st = a.annotate_stream(batches, learned=learned, min_confidence=0.9, check_fraction=0.2)
+        assert np.array_equal(first, want_first) and np.array_equal(final, want_final)
+        assert ms.shape == (len(batches),) and (ms >= 0).all()
+        if learned:
+            assert st["cells"] == q.n_rows and st["decided"] + st["finetuned"] == q.n_rows

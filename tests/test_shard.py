@@ -77,3 +77,39 @@ def test_two_gloo_ranks_match_unsharded():
             got = np.load(os.path.join(d, f"rank{r}.npz"))
             assert np.array_equal(got["first"], want_first)
             assert np.array_equal(got["final"], want_final)
+
+
+def _device_rank_main(rank, world, port, out_dir):
+    """One rank of the device-sharded run: its own context on cuda:0 annotates its row block through
+    libsgr.so, and the labels are gathered over gloo."""
+    import torch.distributed as dist
+
+    from cusingler_b200 import abi
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        prob = H.problem("families")
+        a = abi.Annotator(gpuid=0)
+        a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
+        first, final = shard.annotate_sharded(lambda part: a.annotate(part), prob.qry)
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), first=first, final=final)
+        a.close()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_two_ranks_drive_the_library_and_gather():
+    """Two processes, each with its own context on cuda:0 (independent kernels, no rank waits on
+    another's kernels), annotate their row blocks through the C ABI; the gathered labels equal the
+    oracle's unsharded labels."""
+    want = H.oracle_run("families", 1)
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_device_rank_main, args=(2, _free_port(), d), nprocs=2, join=True,
+                           start_method="spawn")
+        for r in range(2):
+            got = np.load(os.path.join(d, f"rank{r}.npz"))
+            assert np.array_equal(got["first"], want["first"])
+            assert np.array_equal(got["final"], want["final"])
