@@ -405,7 +405,8 @@ def main():
             ann.set_tuning(0, args.ft_warps)
             ann.set_tuning(1, args.ft_heavy)
             tuning["learned" if learned else "plain"] = {"pinned": True, "ft_warps": args.ft_warps,
-                                                          "ft_heavy": args.ft_heavy, "score_chunk_mb": 1024}
+                                                          "ft_heavy": args.ft_heavy, "score_chunk_mb": 1024,
+                                                          "corr_pair": 0, "corr_gm": 1, "select_warps": 16}
             return
         tuning["learned" if learned else "plain"] = ann.autotune(
             tune_sample, learned=learned, min_confidence=args.min_confidence, check_fraction=args.check_fraction)
@@ -416,6 +417,10 @@ def main():
             ann.set_tuning(0, t["ft_warps"])
             ann.set_tuning(1, t["ft_heavy"])
             ann.set_tuning(2, t["score_chunk_mb"])
+            if mode == abi.MODE_EXACT:
+                ann.set_tuning(5, t["corr_pair"])
+            ann.set_tuning(6, t["corr_gm"])
+            ann.set_tuning(7, t["select_warps"])
 
     def timed(fn, csr, steps, name):
         for _ in range(args.warmup):

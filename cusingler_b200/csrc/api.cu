@@ -137,6 +137,10 @@ struct sgr_ctx {
     DevBuf<int> next_cell;
     DevBuf<uint8_t> ft_row_mask;   // rows of the listed cells (learned form's fine-tune)
     int corr_f16 = 0;              // tuning: score-step correlation on FP16 operands (not exact)
+    int corr_pair = 0;             // tuning: exact correlation on SM pairs (cta_group::2, 256-row tiles)
+    int corr_gm = 1;               // tuning: row bands per group of the correlation's tile order
+    int select_warps = 16;         // tuning: score-step selection, 8 or 16 warps per row-staging CTA, 0 a warp per row
+    int host_training = 0;         // tuning: marker medians and pair lists on the host instead of the device
     DevBuf<uint16_t> ref_f16;      // reference ranks as IEEE half rows [R][Kp]
     bool ref_f16_ready = false;
     DevBuf<int32_t> d_lorder;     // label ids by reference-cell count, longest first (score-step selection)
@@ -452,18 +456,20 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     ctx->trained = false;
     ctx->markers_ready = false;
     HostCsr h{ref->n_rows, ref->n_cols, ref->data, ref->indices, ref->indptr};
-    train_markers(h, celltypes, n_labels, ref_genes, qry_genes, n_qry, ctx->cores, ctx->mk);
     Markers& mk = ctx->mk;
+    const bool on_device = ctx->device >= 0 && !ctx->host_training;
+    if (on_device) prepare_markers(h, celltypes, n_labels, ref_genes, qry_genes, n_qry, mk);
+    else train_markers(h, celltypes, n_labels, ref_genes, qry_genes, n_qry, ctx->cores, mk);
     ctx->R = ref->n_rows;
     ctx->ref_cols = ref->n_cols;
     ctx->ref_f16_ready = false;
-    ctx->G = (int)mk.common.size();
-    ctx->Kp = round_up(std::max(ctx->G, 1), 128);
-    ctx->Wt = (uint32_t)mk.thre.size();
-    ctx->markers_ready = true;
-    if (ctx->device < 0) return;  // host-only context: marker training only
-    if (ctx->G > 8128) fail(SGR_ERR_UNSUPPORTED, "more than 8128 score-step marker genes");
-    if (ctx->Wt > 40000) fail(SGR_ERR_UNSUPPORTED, "fine-tune gene pool above 40000 genes");
+    if (ctx->device < 0) {  // host-only context: marker training only
+        ctx->G = (int)mk.common.size();
+        ctx->Kp = round_up(std::max(ctx->G, 1), 128);
+        ctx->Wt = (uint32_t)mk.thre.size();
+        ctx->markers_ready = true;
+        return;
+    }
 
     // regrouped reference CSR
     std::vector<int32_t> indptr(ctx->R + 1, 0);
@@ -482,6 +488,16 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     ctx->ref_data.upload(data, s);
     ctx->ref_indices.upload(indices, s);
     ctx->ref_indptr.upload(indptr, s);
+    // medians and per-pair marker lists on the device
+    if (on_device)
+        rank_markers_device(ctx->ref_data.p, ctx->ref_indices.p, ctx->ref_indptr.p, ctx->R, ctx->ref_cols,
+                            (int64_t)indptr[ctx->R], mk, s);
+    ctx->G = (int)mk.common.size();
+    ctx->Kp = round_up(std::max(ctx->G, 1), 128);
+    ctx->Wt = (uint32_t)mk.thre.size();
+    ctx->markers_ready = true;
+    if (ctx->G > 8128) fail(SGR_ERR_UNSUPPORTED, "more than 8128 score-step marker genes");
+    if (ctx->Wt > 40000) fail(SGR_ERR_UNSUPPORTED, "fine-tune gene pool above 40000 genes");
     ctx->ref_map_common.upload(position_map(mk.ref_colmap, mk.common, mk.W), s);
     ctx->qry_map_common.upload(position_map(mk.qry_colmap, mk.common, mk.W), s);
     ctx->ref_map_thre.upload(position_map(mk.ref_colmap, mk.thre, mk.W), s);
@@ -600,7 +616,7 @@ void correlate(sgr_ctx* ctx, bool fp32, const int8_t* A, int nq, uint32_t q0, fl
     if (ctx->corr_f16 && !fp32) {
         launch_corr_tc(A, reinterpret_cast<const int8_t*>(ctx->ref_f16.p), nq, (int)ctx->R, ctx->Kp,
                        ctx->q_rinv.p + q0, ctx->ref_rinv.p, ctx->q_n2.p + q0, ctx->ref_n2.p, out, ld, ctx->status.p,
-                       ctx->stream, true, ext);
+                       ctx->stream, true, ext, false, ctx->corr_gm);
         return;
     }
     if (fp32 || exact_simt())
@@ -609,7 +625,8 @@ void correlate(sgr_ctx* ctx, bool fp32, const int8_t* A, int nq, uint32_t q0, fl
                          ld, ctx->stream);
     else
         launch_corr_tc(A, ctx->ref_limbs.p, nq, (int)ctx->R, ctx->Kp, ctx->q_rinv.p + q0, ctx->ref_rinv.p,
-                       ctx->q_n2.p + q0, ctx->ref_n2.p, out, ld, ctx->status.p, ctx->stream, false, ext);
+                       ctx->q_n2.p + q0, ctx->ref_n2.p, out, ld, ctx->status.p, ctx->stream, false, ext,
+                       ctx->corr_pair != 0, ctx->corr_gm);
 }
 
 // Score-step device pass over the rows of `q`.  host: the caller's host CSR when q's rows are not yet
@@ -708,7 +725,8 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const sgr_
         ctx->prof.acc.select_bytes += 4ull * (uint64_t)nq * R;
         launch_select_first(ctx->scores.p, R, nq, (int)L, ctx->lq.p, p, thre, ctx->q_n2.p + q0,
                             ctx->label_scores.p + (size_t)q0 * L, ctx->first.p + q0, ctx->flags.p + (size_t)q0 * L,
-                            scratch, max_len, ctx->status.p, (int)R, ctx->d_lorder.p, s, ext.kmin, ext.kmax);
+                            scratch, max_len, ctx->status.p, (int)R, ctx->d_lorder.p, s, ext.kmin, ext.kmax,
+                            ctx->select_warps);
         ctx->prof.end(sp, s);
     }
     ctx->prof.acc.cells += Q;
@@ -1525,11 +1543,26 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
                        : sgr_annotate(ctx, sample, quantile, finetune_thre, finetune_times, first.data(), fin.data(),
                                       nullptr);
     };
-    const int warps[] = {8, 32};
-    const int heavy[] = {4, 6, 9, 16, 1 << 30};
-    const int chunk_mb[] = {256, 1024};
-    const int keep_w = ctx->ft_warps, keep_h = ctx->ft_heavy;
+    auto run_score = [&]() -> sgr_status {
+        return sgr_score_first(ctx, sample, quantile, finetune_thre, first.data(), nullptr, nullptr);
+    };
+    auto wall = [](auto&& f, sgr_status& stt) {
+        const auto t0 = std::chrono::steady_clock::now();
+        stt = f();
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
+    // every knob is restored if a candidate fails or changes a label
+    const int keep_w = ctx->ft_warps, keep_h = ctx->ft_heavy, keep_pair = ctx->corr_pair, keep_gm = ctx->corr_gm,
+              keep_sw = ctx->select_warps;
     const size_t keep_c = ctx->score_chunk_bytes;
+    auto restore = [&]() {
+        ctx->ft_warps = keep_w;
+        ctx->ft_heavy = keep_h;
+        ctx->score_chunk_bytes = keep_c;
+        ctx->corr_pair = keep_pair;
+        ctx->corr_gm = keep_gm;
+        ctx->select_warps = keep_sw;
+    };
     sgr_tuning best{};
     best.best_ms = 1e300;
     // one untimed pass grows every buffer to the sample's size
@@ -1537,40 +1570,75 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
     if (stt != SGR_OK) return stt;
     first0 = first;
     fin0 = fin;
+
+    // phase 1: score-step shapes (correlation form and tile order, score block, selection CTA width),
+    // each timed on the score step of the sample; first labels must not change
+    const bool exact = ctx->mode == SGR_MODE_EXACT;
+    const int pairs[] = {0, 1}, gms[] = {1, 16}, chunk_mb[] = {256, 1024}, sel_w[] = {0, 16};
+    double score_best = 1e300;
+    for (int pr : pairs)
+        for (int gm : gms) {
+            if (!exact && (pr || gm != 1)) continue;  // the FP32-order correlation runs on CUDA cores
+            for (int c : chunk_mb)
+                for (int w : sel_w) {
+                    ctx->corr_pair = pr;
+                    ctx->corr_gm = gm;
+                    ctx->score_chunk_bytes = (size_t)c << 20;
+                    ctx->select_warps = w;
+                    const double ms = wall(run_score, stt);
+                    if (stt != SGR_OK) {
+                        restore();
+                        return stt;
+                    }
+                    if (first != first0) {
+                        restore();
+                        ctx->err = "autotune: score-step shapes disagree on the labels";
+                        return SGR_ERR_STATE;
+                    }
+                    best.score_trials++;
+                    if (ms < score_best) {
+                        score_best = ms;
+                        best.corr_pair = pr;
+                        best.corr_gm = gm;
+                        best.score_chunk_mb = c;
+                        best.select_warps = w;
+                    }
+                }
+        }
+    ctx->corr_pair = best.corr_pair;
+    ctx->corr_gm = best.corr_gm;
+    ctx->score_chunk_bytes = (size_t)best.score_chunk_mb << 20;
+    ctx->select_warps = best.select_warps;
+    best.score_best_ms = score_best;
+
+    // phase 2: fine-tune shapes with the chosen score step, timed on the whole annotation; first and
+    // final labels must not change
+    const int warps[] = {8, 32};
+    const int heavy[] = {4, 6, 9, 16, 1 << 30};
     for (int w : warps)
-        for (int h : heavy)
-            for (int c : chunk_mb) {
-                ctx->ft_warps = w;
-                ctx->ft_heavy = h;
-                ctx->score_chunk_bytes = (size_t)c << 20;
-                const auto t0 = std::chrono::steady_clock::now();
-                stt = run();
-                const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-                if (stt != SGR_OK) {
-                    ctx->ft_warps = keep_w;
-                    ctx->ft_heavy = keep_h;
-                    ctx->score_chunk_bytes = keep_c;
-                    return stt;
-                }
-                if (first != first0 || fin != fin0) {
-                    ctx->ft_warps = keep_w;
-                    ctx->ft_heavy = keep_h;
-                    ctx->score_chunk_bytes = keep_c;
-                    ctx->err = "autotune: launch shapes disagree on the labels";
-                    return SGR_ERR_STATE;
-                }
-                best.trials++;
-                best.worst_ms = std::max(best.worst_ms, ms);
-                if (ms < best.best_ms) {
-                    best.best_ms = ms;
-                    best.ft_warps = w;
-                    best.ft_heavy = h;
-                    best.score_chunk_mb = c;
-                }
+        for (int h : heavy) {
+            ctx->ft_warps = w;
+            ctx->ft_heavy = h;
+            const double ms = wall(run, stt);
+            if (stt != SGR_OK) {
+                restore();
+                return stt;
             }
+            if (first != first0 || fin != fin0) {
+                restore();
+                ctx->err = "autotune: launch shapes disagree on the labels";
+                return SGR_ERR_STATE;
+            }
+            best.trials++;
+            best.worst_ms = std::max(best.worst_ms, ms);
+            if (ms < best.best_ms) {
+                best.best_ms = ms;
+                best.ft_warps = w;
+                best.ft_heavy = h;
+            }
+        }
     ctx->ft_warps = best.ft_warps;
     ctx->ft_heavy = best.ft_heavy;
-    ctx->score_chunk_bytes = (size_t)best.score_chunk_mb << 20;
     *out = best;
     return SGR_OK;
 }
@@ -1601,6 +1669,26 @@ sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value) {
     if (what == 3) {
         if (value != 0 && value != 1) return SGR_ERR_INVALID_ARGUMENT;
         ctx->pack_scan = value;
+        return SGR_OK;
+    }
+    if (what == 5) {
+        if (value != 0 && value != 1) return SGR_ERR_INVALID_ARGUMENT;
+        ctx->corr_pair = value;
+        return SGR_OK;
+    }
+    if (what == 6) {
+        if (value < 1 || value > 4096) return SGR_ERR_INVALID_ARGUMENT;
+        ctx->corr_gm = value;
+        return SGR_OK;
+    }
+    if (what == 7) {
+        if (value != 0 && value != 8 && value != 16) return SGR_ERR_INVALID_ARGUMENT;
+        ctx->select_warps = value;
+        return SGR_OK;
+    }
+    if (what == 8) {
+        if (value != 0 && value != 1) return SGR_ERR_INVALID_ARGUMENT;
+        ctx->host_training = value;
         return SGR_OK;
     }
     return SGR_ERR_INVALID_ARGUMENT;

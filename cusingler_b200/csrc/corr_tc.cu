@@ -28,6 +28,15 @@
 //               also keeps each (query, label) list's min / max for the selection
 // A second instantiation (F16) is the FP16-operand variant benchmarked beside the exact one: d as
 // IEEE half (exact for |d| <= 2048), one kind::f16 accumulator with FP32 sums (not exact).
+// A third (PAIR) runs the exact product on SM pairs: a cluster of two CTAs issues
+// tcgen05.mma.cta_group::2 with M = 256 (each CTA holds 128 query rows of A and 80 of the tile's 160
+// reference rows of B, and receives its 128 x 160 accumulators in its own TMEM).  Per SM the MMA
+// then reads A and half of B from shared memory, so each SM's TMA writes and MMA operand reads per
+// tile drop from 995 KB to 718 KB.  The leader CTA (rank 0) issues the MMAs; both CTAs' TMA loads
+// signal the leader's stage barriers, each MMA commit arrives on the matching barrier of both CTAs
+// (one commit per CTA), and both CTAs' epilogues release the accumulators on the leader's barriers.
+// Tiles are visited in groups of `gm` row bands (band fastest), so that the CTAs working at the
+// same time share a few bands of A and a slab of B in L2 instead of streaming all of B per band.
 // No TMA multicast is used.  Every mbarrier wait is bounded: on timeout the kernel records
 // SGR_TC_TIMEOUT in *status, drains its own TMA copies (bounded), frees TMEM and returns.
 
@@ -55,6 +64,12 @@ constexpr int TMEM_COLS = 512;
 constexpr int EPI_WARPS = 8;                // warps 4 .. 11
 constexpr int THREADS = 32 * (4 + EPI_WARPS);
 constexpr int STAGING_BYTES = BM * BN * 4;  // one score tile; 16-byte chunks XOR-swizzled by row
+// SM-pair form: per CTA 128 rows of A and BN / 2 rows of B per stage
+constexpr int B_HALF_BYTES = (BN / 2) * BK;
+constexpr int PAIR_STAGE_BYTES = A_BYTES + B_HALF_BYTES;  // 26 KB, a multiple of 1024
+constexpr int PAIR_STAGES = 5;
+constexpr int MAX_STAGES = PAIR_STAGES > STAGES ? PAIR_STAGES : STAGES;
+static_assert(PAIR_STAGE_BYTES % 1024 == 0, "stage buffers must keep 1024-byte alignment");
 constexpr long long WAIT_CYCLES = 4000000000LL;  // about 2 s at 1.9 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -77,11 +92,25 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
+// try_wait with cluster-scope acquire (phases completed by the peer CTA's arrivals)
+__device__ __forceinline__ bool mbar_try_cluster(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // Bounded wait; false on timeout (or when another role already gave up).
+template <bool CLUSTER = false>
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
     const long long t0 = clock64();
     for (uint32_t i = 0;; ++i) {
-        if (mbar_try(bar, parity)) return true;
+        if (CLUSTER ? mbar_try_cluster(bar, parity) : mbar_try(bar, parity)) return true;
         if ((i & 63) == 63) {
             if (*abort_flag) return false;
             if (clock64() - t0 > WAIT_CYCLES) return false;
@@ -93,6 +122,47 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
+// Arrival on a barrier given by its shared::cluster address (this CTA's or the peer's).
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t cluster_id_x() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t n_clusters_x() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+    return r;
+}
+
+// shared::cluster address of the variable at shared::cta address `addr` in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t mapa(uint32_t addr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// L2 policy: keep the lines of a reused operand over streaming data
+__device__ __forceinline__ uint64_t policy_evict_last() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
@@ -101,6 +171,26 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d_hint(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar,
+                                                 uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, %3}], "
+        "[%4], %5;" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar), "l"(policy)
+        : "memory");
+}
+
+// Load into this CTA's shared memory whose completion is counted on a barrier of either CTA of the
+// pair (bar: shared::cluster address).  No multicast.
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar,
+                                                 uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], "
+        "[%1, {%2, %3}], [%4], %5;" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar), "l"(policy)
         : "memory");
 }
 
@@ -135,6 +225,20 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_c, uint64_t da, uint64_t d
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_c),
         "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void umma_i8_pair(uint32_t tmem_c, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}" ::"r"(tmem_c),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+// Completion of this thread's earlier MMAs arrives on the barrier at shared::cluster address `bar`
+// (a barrier of either CTA of the pair); one commit per barrier.
+__device__ __forceinline__ void umma_commit_pair(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
@@ -172,8 +276,8 @@ __device__ __forceinline__ uint32_t ord_key(float f) {
 }
 
 struct __align__(8) TcShared {
-    uint64_t full[STAGES];
-    uint64_t empty[STAGES];
+    uint64_t full[MAX_STAGES];
+    uint64_t empty[MAX_STAGES];
     uint64_t tmem_full;
     uint64_t tmem_empty;    // accumulator regions of P1 and P3 released by the epilogue
     uint64_t tmem_empty_c;  // accumulator region of P2 released
@@ -182,100 +286,158 @@ struct __align__(8) TcShared {
     int abort_flag;
 };
 
+// Tile t of the visiting order -> (row band, column tile): groups of `gm` bands, band fastest.
+__device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int gm, int& mb, int& nb) {
+    const int group = gm * tiles_n;
+    const int g = t / group, first = g * gm;
+    const int gme = min(gm, tiles_m - first);
+    const int local = t - g * group;
+    mb = first + local % gme;
+    nb = local / gme;
+}
+
 // F16: the FP16-operand variant -- one plane of d as half (2 * Kp bytes per row), kind::f16 with
 // FP32 accumulation into one accumulator, score = float((acc * 1/sqrt(n_q)) * 1/sqrt(n_r)).
-template <bool F16>
+// PAIR: the exact product on a cluster of two CTAs (tcgen05 cta_group::2, M = 256).
+template <bool F16, bool PAIR>
 __global__ void __launch_bounds__(THREADS, 1)
     corr_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nq, int R,
                    int Kp, const double* __restrict__ rq, const double* __restrict__ rr,
                    const int64_t* __restrict__ nq2, const int64_t* __restrict__ nr2, float* __restrict__ out,
-                   int64_t ld, int* status, LabelExtremes ext) {
+                   int64_t ld, int* status, LabelExtremes ext, int gm) {
+    static_assert(!(F16 && PAIR), "the SM-pair form is exact only");
+    constexpr int NST = PAIR ? PAIR_STAGES : STAGES;
+    constexpr int SBYTES = PAIR ? PAIR_STAGE_BYTES : STAGE_BYTES;
+    constexpr int MT = PAIR ? 2 * BM : BM;  // query rows of a tile
+    constexpr int NEPI = PAIR ? 2 * EPI_WARPS : EPI_WARPS;  // epilogue warps releasing an accumulator
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ TcShared sh;
     // stage buffers must start on a 1024-byte boundary (128B swizzle atoms)
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tiles_n = (R + BN - 1) / BN, tiles_m = (nq + BM - 1) / BM;
+    const uint32_t rank = PAIR ? cluster_rank() : 0;
+    const int unit = PAIR ? (int)cluster_id_x() : (int)blockIdx.x;        // this CTA's (pair's) tile stream
+    const int n_units = PAIR ? (int)n_clusters_x() : (int)gridDim.x;
+    const int tiles_n = (R + BN - 1) / BN, tiles_m = (nq + MT - 1) / MT;
     const int n_tiles = tiles_m * tiles_n;
     const int kblocks = (F16 ? 2 : 3) * Kp / BK, seg_blocks = F16 ? kblocks : Kp / BK;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; ++s) {
+        for (int s = 0; s < NST; ++s) {
             mbar_init(smem_u32(&sh.full[s]), 1);
             mbar_init(smem_u32(&sh.empty[s]), 1);
         }
         mbar_init(smem_u32(&sh.tmem_full), 1);
-        mbar_init(smem_u32(&sh.tmem_empty), EPI_WARPS);
-        mbar_init(smem_u32(&sh.tmem_empty_c), EPI_WARPS);
+        mbar_init(smem_u32(&sh.tmem_empty), NEPI);
+        mbar_init(smem_u32(&sh.tmem_empty_c), NEPI);
         mbar_init(smem_u32(&sh.drain), 1);
         sh.abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh.tmem_base)),
-                     "r"(TMEM_COLS)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        if (PAIR) {
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             smem_u32(&sh.tmem_base)),
+                         "r"(TMEM_COLS)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             smem_u32(&sh.tmem_base)),
+                         "r"(TMEM_COLS)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
     }
     __syncthreads();
+    if (PAIR) cluster_sync();  // both CTAs' barriers are initialised before either signals the other's
     tc_fence_after();
     const uint32_t tmem = sh.tmem_base;
     volatile int* abort_flag = &sh.abort_flag;
+    // gives up this CTA's waits and, in a pair, the peer's
+    auto give_up = [&]() {
+        atomicOr(status, SGR_TC_TIMEOUT);
+        sh.abort_flag = 1;
+        if (PAIR)
+            asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(mapa(smem_u32(&sh.abort_flag), rank ^ 1u)), "r"(1)
+                         : "memory");
+    };
 
     if (warp == 0) {
         // ---- TMA producer ------------------------------------------------------------------
         if (lane == 0) {
+            const uint64_t keep = policy_evict_last();  // the reference operand is read by every band
             uint32_t it = 0;
             bool ok = true;
-            for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
-                const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+            for (int t = unit; t < n_tiles && ok; t += n_units) {
+                int mb, nb;
+                tile_coords(t, tiles_m, tiles_n, gm, mb, nb);
+                const int m0 = mb * MT + (PAIR ? BM * (int)rank : 0);
+                const int n0 = nb * BN + (PAIR ? (BN / 2) * (int)rank : 0);
                 for (int kb = 0; kb < kblocks; ++kb, ++it) {
-                    const int s = it % STAGES;
-                    const uint32_t ph = (it / STAGES) & 1;
-                    if (!mbar_wait(smem_u32(&sh.empty[s]), ph ^ 1, abort_flag)) {
+                    const int s = it % NST;
+                    const uint32_t ph = (it / NST) & 1;
+                    if (!mbar_wait<PAIR>(smem_u32(&sh.empty[s]), ph ^ 1, abort_flag)) {
                         ok = false;
                         break;
                     }
-                    const uint32_t a_dst = smem_u32(smem + s * STAGE_BYTES);
+                    const uint32_t a_dst = smem_u32(smem + s * SBYTES);
                     const uint32_t b_dst = a_dst + A_BYTES;
-                    const uint32_t fb = smem_u32(&sh.full[s]);
-                    mbar_expect_tx(fb, STAGE_BYTES);
                     // planes in the order H, S, L (the MMA's accumulator order)
                     const int grp = kb / seg_blocks, seg = F16 ? 0 : (grp == 0 ? 0 : (grp == 1 ? 2 : 1));
                     const int kx = F16 ? kb * BK : (seg * seg_blocks + kb % seg_blocks) * BK;
-                    tma_load_2d(a_dst, &tmA, kx, m0, fb);
-                    tma_load_2d(b_dst, &tmB, kx, n0, fb);
+                    if (PAIR) {
+                        // both CTAs' copies complete on the leader's stage barrier
+                        const uint32_t fb = mapa(smem_u32(&sh.full[s]), 0);
+                        if (rank == 0) mbar_expect_tx(smem_u32(&sh.full[s]), 2 * PAIR_STAGE_BYTES);
+                        tma_load_2d_pair(a_dst, &tmA, kx, m0, fb, keep);
+                        tma_load_2d_pair(b_dst, &tmB, kx, n0, fb, keep);
+                    } else {
+                        const uint32_t fb = smem_u32(&sh.full[s]);
+                        mbar_expect_tx(fb, STAGE_BYTES);
+                        tma_load_2d(a_dst, &tmA, kx, m0, fb);
+                        tma_load_2d_hint(b_dst, &tmB, kx, n0, fb, keep);
+                    }
                 }
             }
-            if (!ok) {
-                atomicOr(status, SGR_TC_TIMEOUT);
-                sh.abort_flag = 1;
-            }
-            // drain: every issued stage's copies land before the CTA can exit
-            for (uint32_t j = (it > STAGES ? it - STAGES : 0); j < it; ++j) {
-                const uint32_t s = j % STAGES, ph = (j / STAGES) & 1;
-                const long long t0 = clock64();
-                while (!mbar_try(smem_u32(&sh.full[s]), ph) && clock64() - t0 < WAIT_CYCLES) {
+            if (!ok) give_up();
+            // drain: every issued stage's copies land before the CTA can exit (in a pair the leader
+            // sees both CTAs' copies on its barriers; both CTAs leave only through the final cluster
+            // barrier)
+            if (!PAIR || rank == 0)
+                for (uint32_t j = (it > (uint32_t)NST ? it - NST : 0); j < it; ++j) {
+                    const uint32_t s = j % NST, ph = (j / NST) & 1;
+                    const long long t0 = clock64();
+                    while (!mbar_try(smem_u32(&sh.full[s]), ph) && clock64() - t0 < WAIT_CYCLES) {
+                    }
                 }
-            }
         }
     } else if (warp == 1) {
-        // ---- MMA issuer ----------------------------------------------------------------------
-        if (lane == 0) {
-            constexpr uint32_t idesc = F16 ? idesc_f16(BM, BN) : idesc_i8(BM, BN);
+        // ---- MMA issuer (the leader CTA of a pair) ---------------------------------------------
+        if (lane == 0 && rank == 0) {
+            constexpr uint32_t idesc = F16 ? idesc_f16(BM, BN) : idesc_i8(MT, BN);
             uint32_t it = 0, tile_iter = 0;
             bool ok = true;
-            for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++tile_iter) {
-                if (!mbar_wait(smem_u32(&sh.tmem_empty), (tile_iter & 1) ^ 1, abort_flag)) {
+            // arrival on a barrier of both CTAs (pair) or this CTA
+            auto commit = [&](uint64_t* bar) {
+                if (PAIR) {
+                    umma_commit_pair(mapa(smem_u32(bar), 0));
+                    umma_commit_pair(mapa(smem_u32(bar), 1));
+                } else {
+                    umma_commit(smem_u32(bar));
+                }
+            };
+            for (int t = unit; t < n_tiles && ok; t += n_units, ++tile_iter) {
+                if (!mbar_wait<PAIR>(smem_u32(&sh.tmem_empty), (tile_iter & 1) ^ 1, abort_flag)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
                 for (int kb = 0; kb < kblocks; ++kb, ++it) {
-                    const int s = it % STAGES;
-                    const uint32_t ph = (it / STAGES) & 1;
-                    if (!mbar_wait(smem_u32(&sh.full[s]), ph, abort_flag)) {
+                    const int s = it % NST;
+                    const uint32_t ph = (it / NST) & 1;
+                    if (!mbar_wait<PAIR>(smem_u32(&sh.full[s]), ph, abort_flag)) {
                         ok = false;
                         break;
                     }
@@ -284,36 +446,38 @@ __global__ void __launch_bounds__(THREADS, 1)
                     // L plane -> P2 (region 2), which may still be read by the previous epilogue
                     const int grp = F16 ? 2 : kb / seg_blocks;  // the F16 accumulator is released with P2's barrier
                     if (kb == (F16 ? 0 : 2 * seg_blocks)) {
-                        if (!mbar_wait(smem_u32(&sh.tmem_empty_c), (tile_iter & 1) ^ 1, abort_flag)) {
+                        if (!mbar_wait<PAIR>(smem_u32(&sh.tmem_empty_c), (tile_iter & 1) ^ 1, abort_flag)) {
                             ok = false;
                             break;
                         }
                         tc_fence_after();
                     }
-                    const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
+                    const uint32_t a_addr = smem_u32(smem + s * SBYTES);
                     const uint64_t da = smem_desc(a_addr), db = smem_desc(a_addr + A_BYTES);
                     const uint32_t tc = tmem + (F16 ? 0 : grp * BN);
                     const bool first = (kb % seg_blocks) == 0;
 #pragma unroll
                     for (int k = 0; k < BK / 32; ++k) {  // 32 bytes of K per MMA (32 int8 or 16 half)
+                        const uint32_t acc = (first && k == 0) ? 0u : 1u;
                         if (F16)
-                            umma_f16(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (first && k == 0) ? 0u : 1u);
+                            umma_f16(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, acc);
+                        else if (PAIR)
+                            umma_i8_pair(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, acc);
                         else
-                            umma_i8(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (first && k == 0) ? 0u : 1u);
+                            umma_i8(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, acc);
                     }
-                    umma_commit(smem_u32(&sh.empty[s]));
+                    commit(&sh.empty[s]);
                 }
                 if (!ok) break;
-                umma_commit(smem_u32(&sh.tmem_full));
+                commit(&sh.tmem_full);
             }
-            if (!ok) {
-                atomicOr(status, SGR_TC_TIMEOUT);
-                sh.abort_flag = 1;
-            }
-            // every MMA this thread issued has finished before TMEM is freed
-            umma_commit(smem_u32(&sh.drain));
+            if (!ok) give_up();
+            // every MMA this thread issued has finished before TMEM is freed (in both CTAs of a pair)
+            commit(&sh.drain);
+        }
+        if (lane == 0) {
             const long long t0 = clock64();
-            while (!mbar_try(smem_u32(&sh.drain), 0) && clock64() - t0 < WAIT_CYCLES) {
+            while (!mbar_try_cluster(smem_u32(&sh.drain), 0) && clock64() - t0 < WAIT_CYCLES) {
             }
         }
     } else if (warp >= 4) {
@@ -324,12 +488,17 @@ __global__ void __launch_bounds__(THREADS, 1)
         // the row-per-lane writes and the row-contiguous reads.  A warp reads back only what it
         // wrote, so the next tile may overwrite the staging rows once the warp's stores are issued.
         const int quarter = warp & 3, half = (warp - 4) >> 2;
-        float4* staging = reinterpret_cast<float4*>(smem + STAGES * STAGE_BYTES);
+        float4* staging = reinterpret_cast<float4*>(smem + NST * SBYTES);
         const bool vec_store = (ld % 4) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
         const int row = 32 * quarter + lane;
+        // the accumulators are released on the leader's barriers (this CTA's own when alone)
+        const uint32_t rel_ab = PAIR ? mapa(smem_u32(&sh.tmem_empty), 0) : smem_u32(&sh.tmem_empty);
+        const uint32_t rel_c = PAIR ? mapa(smem_u32(&sh.tmem_empty_c), 0) : smem_u32(&sh.tmem_empty_c);
         uint32_t tile_iter = 0;
-        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++tile_iter) {
-            const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+        for (int t = unit; t < n_tiles; t += n_units, ++tile_iter) {
+            int mb, nb;
+            tile_coords(t, tiles_m, tiles_n, gm, mb, nb);
+            const int m0 = mb * MT + (PAIR ? BM * (int)rank : 0), n0 = nb * BN;
             // norms of this tile's rows and columns, loaded while the accumulator is still being computed
             const int q = m0 + row;
             const double rqv = q < nq ? rq[q] : 0.0;  // NaN when the query row is constant
@@ -339,12 +508,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const int r = n0 + half * HALF + c * 16 + lane;
                 rrv[c] = (lane < 16 && r < R) ? rr[r] : 0.0;  // NaN for a constant reference row
             }
-            const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh.tmem_full), tile_iter & 1, abort_flag));
+            const bool got =
+                __all_sync(0xffffffffu, mbar_wait<PAIR>(smem_u32(&sh.tmem_full), tile_iter & 1, abort_flag));
             if (!got) {
-                if (lane == 0) {
-                    atomicOr(status, SGR_TC_TIMEOUT);
-                    sh.abort_flag = 1;
-                }
+                if (lane == 0) give_up();
                 break;
             }
             tc_fence_after();
@@ -364,7 +531,10 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&sh.tmem_empty));
+            if (lane == 0) {
+                if (PAIR) mbar_arrive_cluster(rel_ab);
+                else mbar_arrive(rel_ab);
+            }
             // per-(query, label) extremes of this warp's columns, flushed at label ends (labels are
             // column ranges, the same for every lane, so the flushes are warp-uniform)
             int lab = 0, lab_end = 0;
@@ -439,7 +609,10 @@ __global__ void __launch_bounds__(THREADS, 1)
             // all of this warp's TMEM reads are done: release its share of P2
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&sh.tmem_empty_c));
+            if (lane == 0) {
+                if (PAIR) mbar_arrive_cluster(rel_c);
+                else mbar_arrive(rel_c);
+            }
             if (ext.kmin && seen && q < nq) {
                 atomicMin(ext.kmin + (size_t)q * ext.L + lab, ord_key(mnf));
                 atomicMax(ext.kmax + (size_t)q * ext.L + lab, ord_key(mxf));
@@ -465,9 +638,15 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     }
     __syncthreads();
+    // a pair leaves together: no CTA exits while the other may still signal its barriers or read its
+    // shared memory through the MMA
+    if (PAIR) cluster_sync();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+        if (PAIR)
+            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+        else
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
     }
 }
 
@@ -503,23 +682,55 @@ CUtensorMap limb_map(const int8_t* base, int rows, int row_bytes, int box_rows) 
 
 }  // namespace
 
-size_t corr_tc_smem() { return (size_t)STAGES * STAGE_BYTES + STAGING_BYTES + 1024; }
+size_t corr_tc_smem(bool pair) {
+    return pair ? (size_t)PAIR_STAGES * PAIR_STAGE_BYTES + STAGING_BYTES + 1024
+                : (size_t)STAGES * STAGE_BYTES + STAGING_BYTES + 1024;
+}
 
 void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
                     const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s,
-                    bool f16, LabelExtremes ext) {
+                    bool f16, LabelExtremes ext, bool pair, int gm) {
     if (nq <= 0 || R <= 0) return;
     if (Kp % BK != 0 || (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15))
         fail(SGR_ERR_INVALID_ARGUMENT, "tensor-core correlation: misaligned operands");
+    pair = pair && !f16;
+    gm = std::max(gm, 1);
     const int row_bytes = (f16 ? 2 : 3) * Kp;
-    const CUtensorMap ta = limb_map(A, nq, row_bytes, BM), tb = limb_map(B, R, row_bytes, BN);
-    const size_t smem = corr_tc_smem();
-    auto kern = f16 ? corr_tc_kernel<true> : corr_tc_kernel<false>;
+    const CUtensorMap ta = limb_map(A, nq, row_bytes, BM), tb = limb_map(B, R, row_bytes, pair ? BN / 2 : BN);
+    const size_t smem = corr_tc_smem(pair);
+    const int mt = pair ? 2 * BM : BM;
+    const long tiles = (long)((nq + mt - 1) / mt) * ((R + BN - 1) / BN);
+    if (!pair) {
+        auto kern = f16 ? corr_tc_kernel<true, false> : corr_tc_kernel<false, false>;
+        SGR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int grid = (int)std::min<long>(tiles, device_sm_count());
+        kern<<<grid, THREADS, smem, s>>>(ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status, ext, gm);
+        SGR_LAUNCH_CHECK();
+        count_launch();
+        return;
+    }
+    auto kern = corr_tc_kernel<false, true>;
     SGR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const long tiles = (long)((nq + BM - 1) / BM) * ((R + BN - 1) / BN);
-    const int grid = (int)std::min<long>(tiles, device_sm_count());
-    kern<<<grid, THREADS, smem, s>>>(ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status, ext);
-    SGR_LAUNCH_CHECK();
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    // as many pairs as can be resident at once (a pair needs two SMs of one GPC)
+    cfg.gridDim = dim3(2 * (unsigned)std::max(1, device_sm_count() / 2));
+    int max_pairs = 0;
+    if (cudaOccupancyMaxActiveClusters(&max_pairs, kern, &cfg) != cudaSuccess || max_pairs < 1) {
+        cudaGetLastError();
+        max_pairs = std::max(1, device_sm_count() / 2);
+    }
+    cfg.gridDim = dim3(2 * (unsigned)std::min<long>(tiles, max_pairs));
+    SGR_CUDA(cudaLaunchKernelEx(&cfg, kern, ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status, ext, gm));
     count_launch();
 }
 

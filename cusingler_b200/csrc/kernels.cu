@@ -524,6 +524,60 @@ __global__ void __launch_bounds__(NW * 32) select_first_kernel(const float* scor
     }
 }
 
+// Warp-per-row form: each warp selects every label of its query rows straight from the score rows
+// (global memory; a label's second pass hits L1 / L2), so no block barrier waits for a row's longest
+// label, and a CTA needs only a histogram per warp (up to 64 warps per SM).  Every row has the same
+// labels, so the warps' work is balanced by construction.  Each warp prefetches its next row into L2.
+template <int NW>
+__global__ void __launch_bounds__(NW * 32) select_rows_kernel(const float* scores, int64_t ld, int nq, int L,
+                                                           const LabelQ* lq, float p, float thre,
+                                                           const int64_t* qn2, float* label_scores, int32_t* first,
+                                                           uint8_t* flags, float* scratch, int64_t spw, int* status,
+                                                           int row_len, const int32_t* lorder,
+                                                           const uint32_t* ext_min, const uint32_t* ext_max) {
+    __shared__ int hist[NW][256];
+    __shared__ float ls_all[NW][256];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gw = blockIdx.x * NW + warp, n_warps = gridDim.x * NW;
+    float* my_scratch = scratch ? scratch + (size_t)gw * spw : nullptr;
+    float* ls = ls_all[warp];
+    const bool pf = (ld % 4) == 0 && (reinterpret_cast<uintptr_t>(scores) & 15) == 0;
+    for (int q = gw; q < nq; q += n_warps) {
+        const float* row = scores + (size_t)q * ld;
+        const bool qnan = qn2[q] == 0;
+        if (pf && lane == 0 && q + n_warps < nq && qn2[q + n_warps] != 0) {
+            const uint32_t bytes = (uint32_t)(row_len * 4 + 15) & ~15u;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(scores + (size_t)(q + n_warps) * ld),
+                         "r"(bytes)
+                         : "memory");
+        }
+        for (int i = 0; i < L; ++i) {
+            const int l = lorder[i];
+            const LabelQ d = lq[l];
+            float r;
+            if (qnan) r = __int_as_float(0x7fffffff);
+            else if (ext_min && !d.has_nan && d.kind != 0)  // extremes from the correlation epilogue
+                r = quantile_warp_core(row + d.start, d, p, hist[warp], my_scratch, lane, status,
+                                       ext_min[(size_t)q * L + l], ext_max[(size_t)q * L + l], false);
+            else r = quantile_warp(row + d.start, d, p, hist[warp], my_scratch, lane, status);
+            if (lane == 0) ls[l] = r;
+        }
+        __syncwarp();
+        int mn = 0, mx = 0;
+        if (lane == 0) {
+            stl::minmax(ls, L, &mn, &mx);
+            first[q] = mx;
+        }
+        mx = __shfl_sync(FULL, mx, 0);
+        const float t = __fsub_rn(ls[mx], thre);
+        for (int l = lane; l < L; l += 32) {
+            label_scores[(size_t)q * L + l] = ls[l];
+            if (flags) flags[(size_t)q * L + l] = ls[l] >= t ? 1 : 0;
+        }
+        __syncwarp();
+    }
+}
+
 // ---- fine-tune correlation and selection ------------------------------------------------------
 
 template <bool FP32>
@@ -824,19 +878,26 @@ LabelQ make_lq(int start, int len, float p) {
 void launch_select_first(const float* scores, int64_t ld, int nq, int L, const LabelQ* lq, float p, float thre,
                          const int64_t* qn2, float* label_scores, int32_t* first, uint8_t* flags, float* scratch,
                          int64_t spw, int* status, int row_len, const int32_t* lorder, cudaStream_t s,
-                         const uint32_t* ext_min, const uint32_t* ext_max) {
+                         const uint32_t* ext_min, const uint32_t* ext_max, int warps) {
     if (nq <= 0) return;
     const size_t stage_bytes = (((size_t)std::max(row_len, 1) * 4 + 15) & ~size_t(15));
-    if (lorder && stage_bytes <= 200 * 1024) {
-        SGR_CUDA(cudaFuncSetAttribute(select_first_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)stage_bytes));
+    if (lorder && warps == 0) {  // one warp per row, 16 warps per CTA, up to 4 CTAs per SM
         int per_sm = 0;
-        SGR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, select_first_kernel<true>, 512, stage_bytes));
-        per_sm = std::max(1, std::min(per_sm, 2));  // scratch is sized for two 16-warp blocks per SM
+        SGR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, select_rows_kernel<16>, 512, 0));
+        per_sm = std::max(1, std::min(per_sm, 4));  // scratch is sized for 64 warps per SM
+        const unsigned blocks = (unsigned)std::min<long>((nq + 15) / 16, (long)sm_count() * per_sm);
+        select_rows_kernel<16><<<blocks, 512, 0, s>>>(scores, ld, nq, L, lq, p, thre, qn2, label_scores, first, flags,
+                                                      scratch, spw, status, row_len, lorder, ext_min, ext_max);
+    } else if (lorder && stage_bytes <= 200 * 1024) {
+        auto kern = warps == 8 ? select_first_kernel<true, 8> : select_first_kernel<true, 16>;
+        const int threads = 32 * (warps == 8 ? 8 : 16);
+        SGR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes));
+        int per_sm = 0;
+        SGR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, stage_bytes));
+        per_sm = std::max(1, std::min(per_sm, 2));  // at most 32 warps per SM use scratch
         const unsigned blocks = (unsigned)std::min<long>(nq, (long)sm_count() * per_sm);
-        select_first_kernel<true><<<blocks, 512, stage_bytes, s>>>(scores, ld, nq, L, lq, p, thre, qn2, label_scores,
-                                                                   first, flags, scratch, spw, status, row_len,
-                                                                   lorder, ext_min, ext_max);
+        kern<<<blocks, threads, stage_bytes, s>>>(scores, ld, nq, L, lq, p, thre, qn2, label_scores, first, flags,
+                                                  scratch, spw, status, row_len, lorder, ext_min, ext_max);
     } else {
         const unsigned blocks = scratch ? (unsigned)std::min<long>(nq, sm_count() * 2)
                                         : (unsigned)std::min<long>(nq, sm_count() * 8);

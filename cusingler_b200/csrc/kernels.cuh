@@ -20,9 +20,9 @@ void count_launch(uint64_t n = 1);
 
 // Grid caps of the selection kernels; their scratch (NaN-bearing lists) is sized per warp of the
 // capped grid.
-// Warps of the score-step selection that may use NaN-list scratch at once: two blocks per SM of at
-// most 16 warps.
-inline int select_warps_with_scratch() { return device_sm_count() * 2 * 16; }
+// Warps of the score-step selection that may use NaN-list scratch at once: 64 per SM (the warp-per-row
+// form; the staged form runs at most two blocks of 16 warps per SM).
+inline int select_warps_with_scratch() { return device_sm_count() * 64; }
 
 // ---- gather + rank ----------------------------------------------------------------------------
 //
@@ -120,11 +120,13 @@ LabelQ make_lq(int start, int len, float p);
 // row_len: floats of a score row that the labels cover.  With `lorder` (label ids, longest first)
 // and rows of at most 200 KB, each block stages its row in shared memory before selecting.
 // ext_min / ext_max (optional, staged path): per (row, label) extreme order keys from the
-// correlation epilogue, used instead of a min / max pass for lists that cannot hold NaN.
+// correlation epilogue, used instead of a min / max pass for lists that cannot hold NaN.  warps: 8 or 16
+// warps per CTA of the staged form (a block per row), 0 the warp-per-row form (with `lorder`).
 void launch_select_first(const float* scores, int64_t ld, int nq, int L, const LabelQ* lq, float p,
                          float thre, const int64_t* qn2, float* label_scores, int32_t* first, uint8_t* flags,
                          float* scratch, int64_t scratch_per_warp, int* status, int row_len, const int32_t* lorder,
-                         cudaStream_t s, const uint32_t* ext_min = nullptr, const uint32_t* ext_max = nullptr);
+                         cudaStream_t s, const uint32_t* ext_min = nullptr, const uint32_t* ext_max = nullptr,
+                         int warps = 16);
 
 // ---- fine-tune ----------------------------------------------------------------------------------
 struct FtGroup {
@@ -162,7 +164,8 @@ void launch_ft_select(const FtGroup* groups, const FtSelItem* items, uint32_t n_
                       int64_t scratch_per_warp, int* status, cudaStream_t s);
 
 // Exact score-step correlation on the tensor cores (corr_tc.cu): A/B are LIMBS rows of 3 * Kp bytes.
-size_t corr_tc_smem();
+// pair: tiles of 256 query rows on clusters of two CTAs (tcgen05 cta_group::2); exact mode only.
+size_t corr_tc_smem(bool pair);
 // Per-(query, label) extremes written by the correlation epilogue for the selection: label l's
 // reference columns are [lstart[l], lstart[l+1]); kmin / kmax (Q x L order keys, preset to all ones /
 // zero) receive atomicMin / atomicMax of each list's scores.  kmin = nullptr: not written.
@@ -173,9 +176,11 @@ struct LabelExtremes {
     uint32_t* kmax = nullptr;
 };
 
+// gm: row bands per group of the tile order (the bands of a group sweep the reference tiles together,
+// so the CTAs at work share them through L2); 1 visits band after band.
 void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
                     const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s,
-                    bool f16 = false, LabelExtremes ext = LabelExtremes{});
+                    bool f16 = false, LabelExtremes ext = LabelExtremes{}, bool pair = false, int gm = 1);
 
 // Persistent exact fine-tune (finetune.cu).
 struct FtPersistentArgs {

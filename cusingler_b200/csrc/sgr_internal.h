@@ -91,10 +91,23 @@ struct Markers {
     std::vector<uint32_t> ft_idx;      // (start, len) per ordered pair
 };
 
-// Gene-name intersection, label regrouping and marker training (see train.cpp).
+// Gene-name intersection, label regrouping and marker training on the host (see train.cpp):
+// prepare_markers (intersection, regrouping: colmaps, ref_order, ctidx) then rank_markers_host
+// (medians, per-pair lists, gene sets).
 void train_markers(const HostCsr& ref, const int32_t* celltypes, uint32_t n_labels,
                    const char* const* ref_genes, const char* const* qry_genes, uint32_t n_qry_genes,
                    int cores, Markers& out);
+void prepare_markers(const HostCsr& ref, const int32_t* celltypes, uint32_t n_labels,
+                     const char* const* ref_genes, const char* const* qry_genes, uint32_t n_qry_genes, Markers& m);
+void rank_markers_host(const HostCsr& ref, int cores, Markers& m);
+// From pair_genes / pair_idx and the score-step and fine-tune gene flags (W each): the gene sets
+// common and thre and the fine-tune pair lists.
+void finish_markers(Markers& m, const uint8_t* in_common, const uint8_t* in_thre);
+// The medians and per-pair lists on the device (train_gpu.cu) from the label-grouped reference CSR
+// in device memory (rows in m.ref_order order, original columns); fills pair_genes, pair_idx and,
+// through finish_markers, the gene sets.
+void rank_markers_device(const float* data, const int32_t* indices, const int32_t* indptr, uint32_t R,
+                         uint32_t ref_cols, int64_t nnz, Markers& m, cudaStream_t s);
 
 // Reference's marker-count formula round(500 * (2/3)^log2(n)) (src/io.cpp:209,
 // src/cusingler.cu:1142).

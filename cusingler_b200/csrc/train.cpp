@@ -111,9 +111,8 @@ void rank_pair(const std::vector<float>& m1, const std::vector<float>& m2, size_
 
 }  // namespace
 
-void train_markers(const HostCsr& ref, const int32_t* celltypes, uint32_t n_labels,
-                   const char* const* ref_genes, const char* const* qry_genes, uint32_t n_qry_genes,
-                   int cores, Markers& m) {
+void prepare_markers(const HostCsr& ref, const int32_t* celltypes, uint32_t n_labels,
+                     const char* const* ref_genes, const char* const* qry_genes, uint32_t n_qry_genes, Markers& m) {
     m = Markers();
     m.n_labels = n_labels;
     m.W = ref.n_cols;
@@ -138,6 +137,47 @@ void train_markers(const HostCsr& ref, const int32_t* celltypes, uint32_t n_labe
         start += (uint32_t)by[l].size();
         m.ref_order.insert(m.ref_order.end(), by[l].begin(), by[l].end());
     }
+    if ((size_t)marker_count(n_labels) > m.W) fail(SGR_ERR_UNSUPPORTED, "more marker genes per label pair than genes");
+}
+
+void finish_markers(Markers& m, const uint8_t* in_common, const uint8_t* in_thre) {
+    const uint32_t W = m.W, L = m.n_labels;
+    m.common.clear();
+    m.thre.clear();
+    std::vector<int32_t> thre_id(W, -1);
+    for (uint32_t g = 0; g < W; ++g) {
+        if (in_common[g]) m.common.push_back(g);
+        if (in_thre[g]) {
+            thre_id[g] = (int32_t)m.thre.size();
+            m.thre.push_back(g);
+        }
+    }
+    // Pair lists restricted to the thre pool, in thre-compact ids (src/io.cpp:722-757).
+    m.ft_genes.clear();
+    m.ft_idx.clear();
+    uint32_t fstart = 0;
+    for (size_t p = 0; p < (size_t)L * L; ++p) {
+        uint32_t pos = m.pair_idx[2 * p], len = m.pair_idx[2 * p + 1];
+        if (pos == 0 && len == 0) {
+            m.ft_idx.push_back(0);
+            m.ft_idx.push_back(0);
+            continue;
+        }
+        for (uint32_t j = pos; j < pos + len; ++j) {
+            int32_t t = thre_id[m.pair_genes[j]];
+            if (t >= 0) m.ft_genes.push_back((uint32_t)t);
+        }
+        m.ft_idx.push_back(fstart);
+        m.ft_idx.push_back((uint32_t)m.ft_genes.size() - fstart);
+        fstart = (uint32_t)m.ft_genes.size();
+    }
+}
+
+void rank_markers_host(const HostCsr& ref, int cores, Markers& m) {
+    const uint32_t n_labels = m.n_labels;
+    std::vector<std::vector<uint32_t>> by(n_labels);
+    for (uint32_t l = 0; l < n_labels; ++l)
+        by[l].assign(m.ref_order.begin() + m.ctidx[2 * l], m.ref_order.begin() + m.ctidx[2 * l] + m.ctidx[2 * l + 1]);
 
     // Per-label medians over every gene id (implicit zeros included).
     const uint32_t W = m.W;
@@ -168,14 +208,15 @@ void train_markers(const HostCsr& ref, const int32_t* celltypes, uint32_t n_labe
 
     const size_t n_common = (size_t)marker_count(n_labels);
     const size_t n_thre = (size_t)marker_count(2);
-    if (n_common > W) fail(SGR_ERR_UNSUPPORTED, "more marker genes per label pair than genes");
     std::vector<PairLists> pl((size_t)n_labels * n_labels);
     run_parallel(cores, pl.size(), [&](size_t p) {
         size_t a = p / n_labels, b = p % n_labels;
         if (a != b) rank_pair(med[a], med[b], n_common, pl[p]);
     });
-    std::vector<char> in_common(W, 0), in_thre(W, 0);
+    std::vector<uint8_t> in_common(W, 0), in_thre(W, 0);
     uint32_t off = 0;
+    m.pair_genes.clear();
+    m.pair_idx.clear();
     for (size_t p = 0; p < pl.size(); ++p) {
         if (p / n_labels == p % n_labels) {
             m.pair_idx.push_back(0);
@@ -190,31 +231,14 @@ void train_markers(const HostCsr& ref, const int32_t* celltypes, uint32_t n_labe
         m.pair_idx.push_back((uint32_t)pos.size());
         off += (uint32_t)pos.size();
     }
-    std::vector<int32_t> thre_id(W, -1);
-    for (uint32_t g = 0; g < W; ++g) {
-        if (in_common[g]) m.common.push_back(g);
-        if (in_thre[g]) {
-            thre_id[g] = (int32_t)m.thre.size();
-            m.thre.push_back(g);
-        }
-    }
-    // Pair lists restricted to the thre pool, in thre-compact ids (src/io.cpp:722-757).
-    uint32_t fstart = 0;
-    for (size_t p = 0; p < pl.size(); ++p) {
-        uint32_t pos = m.pair_idx[2 * p], len = m.pair_idx[2 * p + 1];
-        if (pos == 0 && len == 0) {
-            m.ft_idx.push_back(0);
-            m.ft_idx.push_back(0);
-            continue;
-        }
-        for (uint32_t j = pos; j < pos + len; ++j) {
-            int32_t t = thre_id[m.pair_genes[j]];
-            if (t >= 0) m.ft_genes.push_back((uint32_t)t);
-        }
-        m.ft_idx.push_back(fstart);
-        m.ft_idx.push_back((uint32_t)m.ft_genes.size() - fstart);
-        fstart = (uint32_t)m.ft_genes.size();
-    }
+    finish_markers(m, in_common.data(), in_thre.data());
+}
+
+void train_markers(const HostCsr& ref, const int32_t* celltypes, uint32_t n_labels,
+                   const char* const* ref_genes, const char* const* qry_genes, uint32_t n_qry_genes,
+                   int cores, Markers& m) {
+    prepare_markers(ref, celltypes, n_labels, ref_genes, qry_genes, n_qry_genes, m);
+    rank_markers_host(ref, cores, m);
 }
 
 }  // namespace sgr

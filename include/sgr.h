@@ -142,7 +142,12 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
  * instead of one CTA (>= 2; large values disable the split path); what 2: MiB of score-step
  * correlations per block of queries (small blocks are read back from L2 by the selection); what 3:
  * 1 (default) lets the fine-tune row scan keep each value run's count and e-sum in one packed
- * 32-bit word when the trained reference allows it, 0 always uses the two-register scan.
+ * 32-bit word when the trained reference allows it, 0 always uses the two-register scan; what 5:
+ * 1 runs the exact correlation on SM pairs (clusters of two CTAs, tcgen05 cta_group::2, 256-row
+ * tiles), 0 one CTA per 128-row tile; what 6: row bands per group of the correlation's tile order
+ * (1 to 4096; the bands of a group sweep the reference together so that the CTAs at work share
+ * operand tiles in L2); what 7: the score-step selection's form: 8 or 16 warps per CTA that stages
+ * a query row in shared memory, or 0 for one warp per query row reading the scores directly.
  * No choice above changes any result.  what 4 (exact mode only; no counterpart in the reference):
  * 1 runs the score-step correlation on FP16 operands with FP32 accumulation (one tensor-core
  * product instead of three INT8 products; scores are not exact, their error against the exact
@@ -150,19 +155,28 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
 sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value);
 sgr_status sgr_reset_timings(sgr_ctx* ctx);
 
-/* Autotuner (no counterpart in the reference): runs the annotation of `sample` (host or device
- * CSR) once per candidate launch shape -- fine-tune warps per CTA {8, 32} x split-path threshold
- * {4, 6, 9, 16, off} x score block {256, 1024} MiB -- keeps the fastest by wall time, and leaves
- * it set in the context.  learned = 1 tunes the learned form (sgr_annotate_learned with
- * min_confidence / check_fraction), 0 the plain form.  Every candidate must give the same first and
- * final labels (SGR_ERR_STATE otherwise).  The trials count in sgr_timings. */
+/* Autotuner (no counterpart in the reference).  Phase 1 times the score step of `sample` (host or
+ * device CSR) for every score-step shape -- correlation on one CTA or an SM pair per tile x tile
+ * order of 1 or 16 bands per group x score block {256, 1024} MiB x selection form {warp per row,
+ * 16-warp row-staging CTA}
+ * (exact mode; fp32ref mode tunes the last two) -- and keeps the fastest; phase 2 then times the
+ * whole annotation for every fine-tune shape -- warps per CTA {8, 32} x split-path threshold
+ * {4, 6, 9, 16, off} -- and keeps the fastest by wall time.  All choices stay set in the context.
+ * learned = 1 tunes the learned form (sgr_annotate_learned with min_confidence / check_fraction), 0
+ * the plain form.  Every candidate must give the same first (and, in phase 2, final) labels
+ * (SGR_ERR_STATE otherwise).  The trials count in sgr_timings. */
 typedef struct sgr_tuning {
     int32_t ft_warps;
     int32_t ft_heavy;       /* 1 << 30 when the split path is off */
     int32_t score_chunk_mb;
-    int32_t trials;
+    int32_t trials;         /* phase-2 trials */
     double best_ms;         /* wall time of the chosen candidate on the sample */
-    double worst_ms;        /* slowest candidate */
+    double worst_ms;        /* slowest phase-2 candidate */
+    int32_t corr_pair;      /* 1: SM-pair correlation */
+    int32_t corr_gm;        /* row bands per group of the correlation's tile order */
+    int32_t select_warps;
+    int32_t score_trials;   /* phase-1 trials */
+    double score_best_ms;   /* wall time of the chosen score step on the sample */
 } sgr_tuning;
 sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, float finetune_thre,
                         int32_t finetune_times, int32_t learned, float min_confidence, float check_fraction,

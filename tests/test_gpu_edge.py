@@ -22,8 +22,10 @@ def _csr_from_rows(rows, n_cols):
                      np.array(ptr, np.int32), np.zeros(len(rows), np.int32))
 
 
-def _run_both(prob, mode):
+def _run_both(prob, mode, tuning=()):
     a = abi.Annotator(gpuid=0, mode=mode)
+    for what, value in tuning:
+        a.set_tuning(what, value)
     a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
     first, scores, flags = a.score_first(prob.qry)
     final, rounds = a.finetune(prob.qry, flags)
@@ -124,7 +126,8 @@ def test_dense_rows_take_the_large_sort_tier(mode):
         assert np.array_equal(d_ref[i], orc.rank_row(0, i)), i
 
 
-def test_long_labels_ties_and_nan_lists():
+@pytest.mark.parametrize("select_form", [0, 16])
+def test_long_labels_ties_and_nan_lists(select_form):
     """Long score lists in exact mode.  Five labels, four of them over 1,024 reference cells: one long
     label holds an empty reference row (its lists hold NaN and are sorted exactly), one holds 1,000
     copies of a single cell (the order statistic's value bin exceeds the 256-key buffer, so the radix
@@ -150,7 +153,7 @@ def test_long_labels_ties_and_nan_lists():
     q = _csr_from_rows(rows_q, qry.n_cols)
     prob = O.Problem(r, q, synth.names("CT", 5), ref.labels, synth.names("G", ref.n_cols),
                      synth.names("G", qry.n_cols))
-    _run_both(prob, abi.MODE_EXACT)
+    _run_both(prob, abi.MODE_EXACT, tuning=[(7, select_form)])
 
 
 def test_many_query_rows_tiled_scan():
@@ -252,9 +255,10 @@ def test_autotune_keeps_results():
     a = abi.Annotator(gpuid=0)
     a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
     t = a.autotune(prob.qry)
-    assert t["trials"] == 20
+    assert t["trials"] == 10 and t["score_trials"] == 16
     assert t["ft_warps"] in (8, 32) and t["ft_heavy"] in (4, 6, 9, 16, 1 << 30)
     assert t["score_chunk_mb"] in (256, 1024) and 0 < t["best_ms"] <= t["worst_ms"]
+    assert t["corr_pair"] in (0, 1) and t["corr_gm"] in (1, 16) and t["select_warps"] in (0, 16)
     first, final = a.annotate(prob.qry)
     o = H.oracle_run("families", 1)
     assert np.array_equal(first, o["first"]) and np.array_equal(final, o["final"])

@@ -128,3 +128,34 @@ def test_fp16_variant_close_to_exact(kind):
     assert (f16 == f_exact).mean() >= 0.99
     # back on the exact form, bit-exact again
     assert H.ulp_diff(a.debug_scores(prob.qry), raw_exact).max() == 0
+
+
+@pytest.mark.parametrize("kind", ["tiny", "small"])
+@pytest.mark.parametrize("pair,gm", [(0, 8), (1, 1), (1, 8)])
+def test_correlation_forms_bit_exact(kind, pair, gm):
+    """Both tensor-core forms of the exact correlation -- one CTA per 128-row tile, or a cluster of two
+    CTAs per 256-row tile (tcgen05 cta_group::2) -- in band-by-band or grouped tile order give the
+    oracle's exact scores bit for bit, and the oracle's labels (query and reference counts that are
+    not multiples of the tile sizes included)."""
+    a, prob = annotator(kind, abi.MODE_EXACT)
+    a.set_tuning(5, pair)
+    a.set_tuning(6, gm)
+    raw = a.debug_scores(prob.qry)
+    res = H.oracle_run(kind, 1)
+    assert H.ulp_diff(raw, res["raw"]).max() == 0
+    first, final = a.annotate(prob.qry)
+    assert np.array_equal(first, res["first"]) and np.array_equal(final, res["final"])
+
+
+@pytest.mark.parametrize("kind", ["tiny", "families", "small"])
+@pytest.mark.parametrize("form", [0, 8])
+def test_selection_forms(kind, form):
+    """The score-step selection as one warp per query row (form 0) and as 8-warp row-staging CTAs
+    gives the oracle's label scores (ulp-equal), first labels and flags."""
+    a, prob = annotator(kind, abi.MODE_EXACT)
+    a.set_tuning(7, form)
+    first, scores, flags = a.score_first(prob.qry)
+    res = H.oracle_run(kind, 1)
+    assert H.ulp_diff(scores, res["scores"]).max() == 0
+    assert np.array_equal(first, res["first"])
+    assert np.array_equal(flags, res["flags"].astype(np.uint8))
