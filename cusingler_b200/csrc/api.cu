@@ -141,6 +141,9 @@ struct sgr_ctx {
     int corr_gm = 1;               // tuning: row bands per group of the correlation's tile order
     int select_warps = 16;         // tuning: score-step selection, 8 or 16 warps per row-staging CTA, 0 a warp per row
     int host_training = 0;         // tuning: marker medians and pair lists on the host instead of the device
+    int pipeline = 0;              // tuning: fine-tune each score block on its own stream while the next is scored
+    cudaStream_t ft_s = nullptr;   // the pipelined fine-tune's stream
+    std::vector<cudaEvent_t> blk_ev;  // one per score block (+ 1): block scored / fine-tune joined
     DevBuf<uint16_t> ref_f16;      // reference ranks as IEEE half rows [R][Kp]
     bool ref_f16_ready = false;
     DevBuf<int32_t> d_lorder;     // label ids by reference-cell count, longest first (score-step selection)
@@ -274,6 +277,7 @@ sgr_status guarded(sgr_ctx* ctx, F&& f) {
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         if (ctx->side) cudaStreamSynchronize(ctx->side);
         if (ctx->copy) cudaStreamSynchronize(ctx->copy);  // no copy may read caller memory after return
+        if (ctx->ft_s) cudaStreamSynchronize(ctx->ft_s);
         cudaGetLastError();
         ctx->prof.spans.clear();
         ctx->prof.used = 0;
@@ -629,41 +633,59 @@ void correlate(sgr_ctx* ctx, bool fp32, const int8_t* A, int nq, uint32_t q0, fl
                        ctx->corr_pair != 0, ctx->corr_gm);
 }
 
-// Score-step device pass over the rows of `q`.  host: the caller's host CSR when q's rows are not yet
-// on the device (query_on_device with defer_rows); they are copied chunk by chunk on the copy stream
-// and each chunk is ranked and scored once its rows have arrived.
-void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const sgr_csr* host = nullptr) {
+// A score step in progress: the query's rows are ranked and scored in blocks of `chunk` rows.
+struct ScorePlan {
+    DevCsr q;
+    const sgr_csr* host = nullptr;
+    float p = 0.8f, thre = 0.05f;
+    uint32_t chunk = 1, n_chunks = 0;
+    bool fp32 = false, f16 = false, tc_ext = false;
+    int rank_out = RANK_LIMBS, rank_norm = NORM_NONE;
+    float* scratch = nullptr;
+    uint32_t max_len = 1;
+    LabelExtremes ext{};
+};
+
+// Prepares the score step over the rows of `q`.  host: the caller's host CSR when q's rows are not
+// yet on the device (query_on_device with defer_rows); they are copied block by block on the copy
+// stream now, and each block is ranked and scored by score_block once its rows have arrived.
+ScorePlan score_begin(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const sgr_csr* host) {
     cudaStream_t s = ctx->stream;
+    ScorePlan pl;
+    pl.q = q;
+    pl.host = host;
+    pl.p = p;
+    pl.thre = thre;
     const uint32_t Q = q.n_rows, R = ctx->R, L = ctx->mk.n_labels;
-    const bool fp32 = ctx->mode == SGR_MODE_FP32REF;
+    pl.fp32 = ctx->mode == SGR_MODE_FP32REF;
     ctx->q_limbs.ensure((size_t)Q * 3 * ctx->Kp);
     ctx->q_n2.ensure(Q);
     ctx->q_rinv.ensure(Q);
     ctx->q_f32.ensure(Q);
-    const bool f16 = ctx->corr_f16 && !fp32;
-    if (f16) ensure_ref_f16(ctx);
-    const uint32_t chunk =
-        (uint32_t)std::max<size_t>(1, std::min<size_t>(Q, ctx->score_chunk_bytes / (4 * (size_t)R)));
-    const uint32_t n_chunks = (Q + chunk - 1) / chunk;
-    // Rows already on the device are ranked in one launch.  Host rows are ranked chunk by chunk as
-    // they arrive: one rank group per chunk, each writing its own rows' limbs and norms.
-    const size_t row_bytes = (size_t)(f16 ? 2 : 3) * ctx->Kp;
-    const uint32_t n_groups = host ? n_chunks : 1;
+    pl.f16 = ctx->corr_f16 && !pl.fp32;
+    if (pl.f16) ensure_ref_f16(ctx);
+    pl.chunk = (uint32_t)std::max<size_t>(1, std::min<size_t>(Q, ctx->score_chunk_bytes / (4 * (size_t)R)));
+    pl.n_chunks = (Q + pl.chunk - 1) / pl.chunk;
+    // Rows already on the device are ranked in one launch.  Host rows are ranked block by block as
+    // they arrive: one rank group per block, each writing its own rows' limbs and norms.
+    const size_t row_bytes = (size_t)(pl.f16 ? 2 : 3) * ctx->Kp;
+    const uint32_t n_groups = host ? pl.n_chunks : 1;
     std::vector<RankGroup> groups(n_groups);
     for (uint32_t c = 0; c < n_groups; ++c) {
-        const size_t r0 = (size_t)c * chunk;
+        const size_t r0 = (size_t)c * pl.chunk;
         groups[c] = RankGroup{ctx->qry_map_common.p, ctx->G,          ctx->Kp,
                               ctx->q_limbs.p + r0 * row_bytes, ctx->q_n2.p + r0, ctx->q_rinv.p + r0,
                               ctx->q_f32.p + r0};
     }
     ctx->rank_groups.upload(groups, s);
-    const int rank_out = f16 ? RANK_F16 : RANK_LIMBS, rank_norm = fp32 ? NORM_SEQ : NORM_NONE;
+    pl.rank_out = pl.f16 ? RANK_F16 : RANK_LIMBS;
+    pl.rank_norm = pl.fp32 ? NORM_SEQ : NORM_NONE;
     if (host) {
-        copy_row_chunks(ctx, host, q, chunk, n_chunks);
+        copy_row_chunks(ctx, host, q, pl.chunk, pl.n_chunks);
     } else {
         const uint64_t l0 = launch_count();
         const int sp = ctx->prof.begin(ST_RANK, s);
-        rank_range(ctx, q, ctx->rank_groups.p, ctx->G, ctx->Kp, 0, Q, rank_out, rank_norm);
+        rank_range(ctx, q, ctx->rank_groups.p, ctx->G, ctx->Kp, 0, Q, pl.rank_out, pl.rank_norm);
         ctx->prof.end(sp, s);
         ctx->prof.acc.rank_launches += launch_count() - l0;
     }
@@ -681,57 +703,69 @@ void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const sgr_
     std::stable_sort(lorder.begin(), lorder.end(),
                      [&](int32_t x, int32_t y) { return ctx->mk.ctidx[2 * x + 1] > ctx->mk.ctidx[2 * y + 1]; });
     ctx->d_lorder.upload(lorder, s);
-    uint32_t max_len = 1;
-    for (uint32_t l = 0; l < L; ++l) max_len = std::max(max_len, ctx->mk.ctidx[2 * l + 1]);
-    float* scratch = nullptr;
-    if (any_nan_ref) {
-        scratch = ctx->sel_scratch.ensure((size_t)select_warps_with_scratch() * max_len);
-    }
+    for (uint32_t l = 0; l < L; ++l) pl.max_len = std::max(pl.max_len, ctx->mk.ctidx[2 * l + 1]);
+    if (any_nan_ref) pl.scratch = ctx->sel_scratch.ensure((size_t)select_warps_with_scratch() * pl.max_len);
     ctx->label_scores.ensure((size_t)Q * L);
     ctx->first.ensure(Q);
     ctx->flags.ensure((size_t)Q * L);
-    ctx->scores.ensure((size_t)chunk * R);
+    ctx->scores.ensure((size_t)pl.chunk * R);
     // the tensor-core correlation also writes each (query, label) list's extremes for the selection
-    const bool tc_ext = !fp32 && !exact_simt();
-    LabelExtremes ext{};
-    if (tc_ext) {
-        ext.lstart = ctx->d_lstart.p;
-        ext.L = (int)L;
-        ext.kmin = ctx->ext_min.ensure((size_t)chunk * L);
-        ext.kmax = ctx->ext_max.ensure((size_t)chunk * L);
+    pl.tc_ext = !pl.fp32 && !exact_simt();
+    if (pl.tc_ext) {
+        pl.ext.lstart = ctx->d_lstart.p;
+        pl.ext.L = (int)L;
+        pl.ext.kmin = ctx->ext_min.ensure((size_t)pl.chunk * L);
+        pl.ext.kmax = ctx->ext_max.ensure((size_t)pl.chunk * L);
     }
-    for (uint32_t c = 0, q0 = 0; q0 < Q; ++c, q0 += chunk) {
-        const int nq = (int)std::min(chunk, Q - q0);
-        int sp = -1;
-        if (host) {
-            SGR_CUDA(cudaStreamWaitEvent(s, ctx->up_ev[c], 0));
-            const uint64_t l0 = launch_count();
-            sp = ctx->prof.begin(ST_RANK, s);
-            rank_range(ctx, q, ctx->rank_groups.p + c, ctx->G, ctx->Kp, q0, (uint32_t)nq, rank_out, rank_norm);
-            ctx->prof.end(sp, s);
-            ctx->prof.acc.rank_launches += launch_count() - l0;
-        }
-        const uint64_t c0 = launch_count();
-        sp = ctx->prof.begin(ST_CORR, s);
-        if (tc_ext) {
-            SGR_CUDA(cudaMemsetAsync(ext.kmin, 0xff, (size_t)nq * L * sizeof(uint32_t), s));
-            SGR_CUDA(cudaMemsetAsync(ext.kmax, 0, (size_t)nq * L * sizeof(uint32_t), s));
-        }
-        correlate(ctx, fp32, ctx->q_limbs.p + (size_t)q0 * (f16 ? 2 : 3) * ctx->Kp, nq, q0, ctx->scores.p, R, ext);
+    return pl;
+}
+
+// Block c of the score step on the context's stream: rows [c * chunk, min(Q, (c + 1) * chunk)).
+void score_block(sgr_ctx* ctx, const ScorePlan& pl, uint32_t c) {
+    cudaStream_t s = ctx->stream;
+    const uint32_t Q = pl.q.n_rows, R = ctx->R, L = ctx->mk.n_labels;
+    const uint32_t q0 = c * pl.chunk;
+    const int nq = (int)std::min(pl.chunk, Q - q0);
+    int sp = -1;
+    if (pl.host) {
+        SGR_CUDA(cudaStreamWaitEvent(s, ctx->up_ev[c], 0));
+        const uint64_t l0 = launch_count();
+        sp = ctx->prof.begin(ST_RANK, s);
+        rank_range(ctx, pl.q, ctx->rank_groups.p + c, ctx->G, ctx->Kp, q0, (uint32_t)nq, pl.rank_out, pl.rank_norm);
         ctx->prof.end(sp, s);
-        ctx->prof.acc.corr_launches += launch_count() - c0;
-        sp = ctx->prof.begin(ST_SELECT, s);
-        ctx->prof.acc.select_launches++;
-        ctx->prof.acc.select_bytes += 4ull * (uint64_t)nq * R;
-        launch_select_first(ctx->scores.p, R, nq, (int)L, ctx->lq.p, p, thre, ctx->q_n2.p + q0,
-                            ctx->label_scores.p + (size_t)q0 * L, ctx->first.p + q0, ctx->flags.p + (size_t)q0 * L,
-                            scratch, max_len, ctx->status.p, (int)R, ctx->d_lorder.p, s, ext.kmin, ext.kmax,
-                            ctx->select_warps);
-        ctx->prof.end(sp, s);
+        ctx->prof.acc.rank_launches += launch_count() - l0;
     }
+    const uint64_t c0 = launch_count();
+    sp = ctx->prof.begin(ST_CORR, s);
+    if (pl.tc_ext) {
+        SGR_CUDA(cudaMemsetAsync(pl.ext.kmin, 0xff, (size_t)nq * L * sizeof(uint32_t), s));
+        SGR_CUDA(cudaMemsetAsync(pl.ext.kmax, 0, (size_t)nq * L * sizeof(uint32_t), s));
+    }
+    correlate(ctx, pl.fp32, ctx->q_limbs.p + (size_t)q0 * (pl.f16 ? 2 : 3) * ctx->Kp, nq, q0, ctx->scores.p, R, pl.ext);
+    ctx->prof.end(sp, s);
+    ctx->prof.acc.corr_launches += launch_count() - c0;
+    sp = ctx->prof.begin(ST_SELECT, s);
+    ctx->prof.acc.select_launches++;
+    ctx->prof.acc.select_bytes += 4ull * (uint64_t)nq * R;
+    launch_select_first(ctx->scores.p, R, nq, (int)L, ctx->lq.p, pl.p, pl.thre, ctx->q_n2.p + q0,
+                        ctx->label_scores.p + (size_t)q0 * L, ctx->first.p + q0, ctx->flags.p + (size_t)q0 * L,
+                        pl.scratch, pl.max_len, ctx->status.p, (int)R, ctx->d_lorder.p, s, pl.ext.kmin,
+                        pl.ext.kmax, ctx->select_warps);
+    ctx->prof.end(sp, s);
+}
+
+void score_end(sgr_ctx* ctx, const ScorePlan& pl) {
+    const uint32_t Q = pl.q.n_rows;
     ctx->prof.acc.cells += Q;
-    ctx->prof.acc.corr_ops += 2ull * Q * R * (uint64_t)ctx->G;
-    ctx->prof.acc.rank_bytes += 8ull * (uint64_t)(q.nnz) + 4ull * (Q + 1) + 3ull * Q * (uint64_t)ctx->Kp;
+    ctx->prof.acc.corr_ops += 2ull * Q * ctx->R * (uint64_t)ctx->G;
+    ctx->prof.acc.rank_bytes += 8ull * (uint64_t)(pl.q.nnz) + 4ull * (Q + 1) + 3ull * Q * (uint64_t)ctx->Kp;
+}
+
+// Score-step device pass over the rows of `q` (see score_begin for `host`).
+void score_device(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const sgr_csr* host = nullptr) {
+    const ScorePlan pl = score_begin(ctx, q, p, thre, host);
+    for (uint32_t c = 0; c < pl.n_chunks; ++c) score_block(ctx, pl, c);
+    score_end(ctx, pl);
 }
 
 // ---- fine-tune ---------------------------------------------------------------------------------
@@ -1031,9 +1065,11 @@ cudaStream_t side_stream(sgr_ctx* ctx) {
 
 // Exact-mode fine-tune: the persistent kernel over a device work queue.  `flags_dev` is the
 // Q x L candidate-flag matrix in device memory.
+// out_row0: the cells' outputs go to ctx->d_final / d_rounds from this row on (the row of q's first
+// cell in a larger query whose blocks are fine-tuned one after another).
 void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev, float p, float thre, int times,
                          int32_t* final_labels, int32_t* rounds_out, const int32_t* cell_list = nullptr,
-                         const int* n_list = nullptr) {
+                         const int* n_list = nullptr, uint32_t out_row0 = 0) {
     cudaStream_t s = ctx->stream;
     const Markers& mk = ctx->mk;
     const uint32_t Q = q.n_rows, L = mk.n_labels, Wt = ctx->Wt;
@@ -1075,8 +1111,8 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     ctx->ft_scratch.ensure((size_t)grid * per_cta);
     ctx->next_cell.ensure(1);
     SGR_CUDA(cudaMemsetAsync(ctx->next_cell.p, 0, sizeof(int), s));
-    ctx->d_final.ensure(Q);
-    ctx->d_rounds.ensure(Q);
+    ctx->d_final.ensure((size_t)out_row0 + Q);
+    ctx->d_rounds.ensure((size_t)out_row0 + Q);
     FtPersistentArgs a{};
     a.ref_sorted = ctx->ref_sorted.p;
     a.pack_shift = ctx->pack_scan ? ctx->pack_shift : 0;
@@ -1144,8 +1180,8 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     a.cell_list = cell_list;
     a.n_list = n_list;
     a.next_cell = ctx->next_cell.p;
-    a.final_labels = ctx->d_final.p;
-    a.rounds = ctx->d_rounds.p;
+    a.final_labels = ctx->d_final.p + out_row0;
+    a.rounds = ctx->d_rounds.p + out_row0;
     a.scratch = ctx->ft_scratch.p;
     a.scratch_per_cta = per_cta;
     a.max_rcand = (int)ctx->R32;
@@ -1278,20 +1314,15 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     }
     ctx->prof.end(sp_ft, s);
     if (!final_labels) {  // caller reads ctx->d_final / d_rounds itself
-        if (ctx->prof.on && listed) {  // rounds of the listed cells, summed on the device
-            if (!ctx->prof.h_rounds)
-                SGR_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->prof.h_rounds), sizeof(unsigned long long)));
-            unsigned long long* d = ctx->d_round_sum.ensure(1);
-            SGR_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), s));
-            launch_sum_listed(listed, n_listed, ctx->d_rounds.p, d, s);
-            SGR_CUDA(cudaMemcpyAsync(ctx->prof.h_rounds, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-            ctx->prof.rounds_pending = true;
-        }
+        // profiling: rounds of the listed cells, added on the device (rounds_sum_begin / _end)
+        if (ctx->prof.on && listed && ctx->d_round_sum.p)
+            launch_sum_listed(listed, n_listed, ctx->d_rounds.p + out_row0, ctx->d_round_sum.p, s);
         return;
     }
-    SGR_CUDA(cudaMemcpyAsync(final_labels, ctx->d_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SGR_CUDA(cudaMemcpyAsync(final_labels, ctx->d_final.p + out_row0, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     std::vector<int32_t> rounds(Q);
-    SGR_CUDA(cudaMemcpyAsync(rounds.data(), ctx->d_rounds.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SGR_CUDA(cudaMemcpyAsync(rounds.data(), ctx->d_rounds.p + out_row0, Q * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                             s));
     check_status(ctx);
     for (uint32_t i = 0; i < Q; ++i) {
         if (rounds_out) rounds_out[i] = rounds[i];
@@ -1299,10 +1330,143 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     }
 }
 
+// Profiling of the learned form: the fine-tune rounds of its listed cells are summed on the device
+// over a call and read back with the call's results.
+void rounds_sum_begin(sgr_ctx* ctx) {
+    if (!ctx->prof.on) return;
+    if (!ctx->prof.h_rounds)
+        SGR_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->prof.h_rounds), sizeof(unsigned long long)));
+    SGR_CUDA(cudaMemsetAsync(ctx->d_round_sum.ensure(1), 0, sizeof(unsigned long long), ctx->stream));
+}
+
+void rounds_sum_end(sgr_ctx* ctx) {
+    if (!ctx->prof.on) return;
+    SGR_CUDA(cudaMemcpyAsync(ctx->prof.h_rounds, ctx->d_round_sum.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    ctx->prof.rounds_pending = true;
+}
+
+// The context's fine-tune stream for the pipelined annotation, created on first use.
+cudaStream_t ft_stream(sgr_ctx* ctx) {
+    if (!ctx->ft_s) SGR_CUDA(cudaStreamCreateWithFlags(&ctx->ft_s, cudaStreamNonBlocking));
+    return ctx->ft_s;
+}
+
+cudaEvent_t block_event(sgr_ctx* ctx, size_t i) {
+    while (ctx->blk_ev.size() <= i) {
+        cudaEvent_t e;
+        SGR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->blk_ev.push_back(e);
+    }
+    return ctx->blk_ev[i];
+}
+
+// Exact-mode annotation with the fine-tune of each score block on a stream of its own: block c's
+// fine-tune runs while block c + 1 is ranked, correlated and selected (and, for a host query, while
+// later blocks are still being copied).  A cell's fine-tune reads only its own row, flags and the
+// trained reference, so blocks are independent.  learned: the proposal network routes each block's
+// cells as sgr_annotate_learned does (row0: the query's first row in a streamed sequence, for the
+// hashed check sample).  Results land in host arrays.
+void annotate_pipelined(sgr_ctx* ctx, const DevCsr& q, const sgr_csr* host, float p, float thre, int32_t times,
+                        bool learned, float min_confidence, float check_fraction, int32_t* first_labels,
+                        int32_t* final_labels, float* label_scores, sgr_learned_stats* stats, uint64_t row0) {
+    const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
+    cudaStream_t s = ctx->stream, f = ft_stream(ctx);
+    if (learned) rounds_sum_begin(ctx);
+    ScorePlan pl = score_begin(ctx, q, p, thre, host);
+    ctx->d_final.ensure(Q);
+    ctx->d_rounds.ensure(Q);
+    if (learned) {
+        ctx->mlp_x.ensure((size_t)Q * L);
+        ctx->mlp_bad.ensure(Q);
+        ctx->prop.ensure(Q);
+        ctx->prop_conf.ensure(Q);
+        ctx->route_final.ensure(Q);
+        ctx->plain.ensure(Q);
+        ctx->role.ensure(Q);
+        ctx->n_plain.ensure(pl.n_chunks);
+        SGR_CUDA(cudaMemsetAsync(ctx->n_plain.p, 0, pl.n_chunks * sizeof(int), s));
+    }
+    const uint32_t per10k = (uint32_t)std::lround(std::min(std::max(check_fraction, 0.f), 1.f) * 10000.f);
+    auto finetune_block = [&](uint32_t c) {
+        const uint32_t r0 = c * pl.chunk, n = std::min(pl.chunk, Q - r0);
+        SGR_CUDA(cudaStreamWaitEvent(f, block_event(ctx, c), 0));
+        DevCsr qc{q.data, q.indices, q.indptr + r0, n, q.n_cols, -1};
+        ctx->stream = f;
+        try {
+            finetune_persistent(ctx, qc, ctx->flags.p + (size_t)r0 * L, p, thre, times,
+                                learned ? nullptr : final_labels + r0, nullptr, learned ? ctx->plain.p + r0 : nullptr,
+                                learned ? ctx->n_plain.p + c : nullptr, r0);
+        } catch (...) {
+            ctx->stream = s;
+            throw;
+        }
+        ctx->stream = s;
+    };
+    for (uint32_t c = 0; c < pl.n_chunks; ++c) {
+        score_block(ctx, pl, c);
+        if (learned) {
+            const uint32_t r0 = c * pl.chunk, n = std::min(pl.chunk, Q - r0);
+            const int sp = ctx->prof.begin(ST_MLP, s);
+            ctx->mlp.features(ctx->label_scores.p + (size_t)r0 * L, (int)n, ctx->mlp_x.p + (size_t)r0 * L,
+                              ctx->mlp_bad.p + r0, s);
+            ctx->mlp.predict(ctx->mlp_x.p + (size_t)r0 * L, (int)n, ctx->prop.p + r0, ctx->prop_conf.p + r0, s);
+            launch_learned_route((int)n, (int)L, ctx->flags.p + (size_t)r0 * L, ctx->mlp_bad.p + r0, ctx->prop.p + r0,
+                                 ctx->prop_conf.p + r0, min_confidence, per10k, 0x243F6A8885A308D3ull, row0 + r0,
+                                 ctx->route_final.p + r0, ctx->plain.p + r0, ctx->n_plain.p + c, ctx->role.p + r0, s);
+            ctx->prof.end(sp, s);
+        }
+        SGR_CUDA(cudaEventRecord(block_event(ctx, c), s));
+        if (c > 0) finetune_block(c - 1);  // runs while block c is on the score stream
+    }
+    score_end(ctx, pl);
+    if (pl.n_chunks) finetune_block(pl.n_chunks - 1);
+    // join the fine-tune stream
+    cudaEvent_t done = block_event(ctx, pl.n_chunks);
+    SGR_CUDA(cudaEventRecord(done, f));
+    SGR_CUDA(cudaStreamWaitEvent(s, done, 0));
+    SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    if (label_scores)
+        SGR_CUDA(cudaMemcpyAsync(label_scores, ctx->label_scores.p, (size_t)Q * L * sizeof(float),
+                                 cudaMemcpyDeviceToHost, s));
+    if (!learned) {
+        check_status(ctx);
+        return;
+    }
+    rounds_sum_end(ctx);
+    std::vector<int32_t> rf(Q), ff(Q);
+    std::vector<uint8_t> role(Q);
+    SGR_CUDA(cudaMemcpyAsync(rf.data(), ctx->route_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SGR_CUDA(cudaMemcpyAsync(ff.data(), ctx->d_final.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SGR_CUDA(cudaMemcpyAsync(role.data(), ctx->role.p, Q, cudaMemcpyDeviceToHost, s));
+    check_status(ctx);
+    sgr_learned_stats st{};
+    st.cells = Q;
+    for (uint32_t i = 0; i < Q; ++i) {
+        if (role[i] == 0) {
+            final_labels[i] = rf[i];
+            st.decided++;
+        } else {
+            final_labels[i] = ff[i];
+            st.finetuned++;
+            if (role[i] == 2) {
+                st.checked++;
+                st.check_agree += rf[i] == ff[i];
+            }
+        }
+    }
+    if (stats) *stats = st;
+}
+
 // Plain form (score step, then the fine-tune) of a query whose rows are on the device, or are copied
 // block by block from `host` during the score step.  Results land in host arrays.
 void annotate_plain(sgr_ctx* ctx, const DevCsr& q, const sgr_csr* host, float quantile, float finetune_thre,
                     int32_t finetune_times, int32_t* first_labels, int32_t* final_labels, float* label_scores) {
+    if (ctx->pipeline && ctx->mode == SGR_MODE_EXACT) {
+        annotate_pipelined(ctx, q, host, quantile, finetune_thre, finetune_times, false, 0.f, 0.f, first_labels,
+                           final_labels, label_scores, nullptr, 0);
+        return;
+    }
     score_device(ctx, q, quantile, finetune_thre, host);
     const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
     cudaStream_t s = ctx->stream;
@@ -1325,8 +1489,14 @@ void annotate_plain(sgr_ctx* ctx, const DevCsr& q, const sgr_csr* host, float qu
 void annotate_learned(sgr_ctx* ctx, const DevCsr& q, const sgr_csr* host, float quantile, float finetune_thre,
                       int32_t finetune_times, float min_confidence, float check_fraction, int32_t* first_labels,
                       int32_t* final_labels, sgr_learned_stats* stats, uint64_t row0 = 0) {
+    if (ctx->pipeline) {
+        annotate_pipelined(ctx, q, host, quantile, finetune_thre, finetune_times, true, min_confidence, check_fraction,
+                           first_labels, final_labels, nullptr, stats, row0);
+        return;
+    }
     const uint32_t Q = q.n_rows, L = ctx->mk.n_labels;
     cudaStream_t s = ctx->stream;
+    rounds_sum_begin(ctx);
     score_device(ctx, q, quantile, finetune_thre, host);
     const int sp = ctx->prof.begin(ST_MLP, s);
     ctx->mlp_x.ensure((size_t)Q * L);
@@ -1347,6 +1517,7 @@ void annotate_learned(sgr_ctx* ctx, const DevCsr& q, const sgr_csr* host, float 
     ctx->prof.end(sp, s);
     finetune_persistent(ctx, q, ctx->flags.p, quantile, finetune_thre, finetune_times, nullptr, nullptr,
                         ctx->plain.p, ctx->n_plain.p);
+    rounds_sum_end(ctx);
     std::vector<int32_t> rf(Q), ff(Q);
     std::vector<uint8_t> role(Q);
     SGR_CUDA(cudaMemcpyAsync(first_labels, ctx->first.p, Q * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -1509,7 +1680,11 @@ sgr_status sgr_destroy(sgr_ctx* ctx) {
         for (cudaEvent_t e : {ctx->sq_up_start[i], ctx->sq_up_done[i], ctx->sq_free[i]})
             if (e) up.push_back(e);
     if (ctx->sq_end) up.push_back(ctx->sq_end);
+    for (cudaEvent_t e : ctx->blk_ev) up.push_back(e);
+    cudaStream_t fts = ctx->ft_s;
+    if (fts) cudaStreamSynchronize(fts);
     delete ctx;  // DevBuf destructors free device memory
+    if (fts) cudaStreamDestroy(fts);
     if (cp) cudaStreamDestroy(cp);
     for (cudaEvent_t e : up) cudaEventDestroy(e);
     if (s) cudaStreamDestroy(s);
@@ -1553,7 +1728,7 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
     };
     // every knob is restored if a candidate fails or changes a label
     const int keep_w = ctx->ft_warps, keep_h = ctx->ft_heavy, keep_pair = ctx->corr_pair, keep_gm = ctx->corr_gm,
-              keep_sw = ctx->select_warps;
+              keep_sw = ctx->select_warps, keep_pipe = ctx->pipeline;
     const size_t keep_c = ctx->score_chunk_bytes;
     auto restore = [&]() {
         ctx->ft_warps = keep_w;
@@ -1562,6 +1737,7 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
         ctx->corr_pair = keep_pair;
         ctx->corr_gm = keep_gm;
         ctx->select_warps = keep_sw;
+        ctx->pipeline = keep_pipe;
     };
     sgr_tuning best{};
     best.best_ms = 1e300;
@@ -1615,8 +1791,12 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
     // final labels must not change
     const int warps[] = {8, 32};
     const int heavy[] = {4, 6, 9, 16, 1 << 30};
+    const int pipes[] = {0, 1};
+    for (int pipe : pipes)
     for (int w : warps)
         for (int h : heavy) {
+            if (pipe && !exact) continue;  // the FP32-order fine-tune is not pipelined
+            ctx->pipeline = pipe;
             ctx->ft_warps = w;
             ctx->ft_heavy = h;
             const double ms = wall(run, stt);
@@ -1635,10 +1815,12 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
                 best.best_ms = ms;
                 best.ft_warps = w;
                 best.ft_heavy = h;
+                best.pipeline = pipe;
             }
         }
     ctx->ft_warps = best.ft_warps;
     ctx->ft_heavy = best.ft_heavy;
+    ctx->pipeline = best.pipeline;
     *out = best;
     return SGR_OK;
 }
@@ -1689,6 +1871,11 @@ sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value) {
     if (what == 8) {
         if (value != 0 && value != 1) return SGR_ERR_INVALID_ARGUMENT;
         ctx->host_training = value;
+        return SGR_OK;
+    }
+    if (what == 9) {
+        if (value != 0 && value != 1) return SGR_ERR_INVALID_ARGUMENT;
+        ctx->pipeline = value;
         return SGR_OK;
     }
     return SGR_ERR_INVALID_ARGUMENT;

@@ -147,7 +147,9 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
  * tiles), 0 one CTA per 128-row tile; what 6: row bands per group of the correlation's tile order
  * (1 to 4096; the bands of a group sweep the reference together so that the CTAs at work share
  * operand tiles in L2); what 7: the score-step selection's form: 8 or 16 warps per CTA that stages
- * a query row in shared memory, or 0 for one warp per query row reading the scores directly.
+ * a query row in shared memory, or 0 for one warp per query row reading the scores directly;
+ * what 8: 1 trains the markers on the host instead of the device; what 9 (exact mode): 1 fine-tunes
+ * each score block on a second stream while the next block is scored.
  * No choice above changes any result.  what 4 (exact mode only; no counterpart in the reference):
  * 1 runs the score-step correlation on FP16 operands with FP32 accumulation (one tensor-core
  * product instead of three INT8 products; scores are not exact, their error against the exact
@@ -160,8 +162,8 @@ sgr_status sgr_reset_timings(sgr_ctx* ctx);
  * order of 1 or 16 bands per group x score block {256, 1024} MiB x selection form {warp per row,
  * 16-warp row-staging CTA}
  * (exact mode; fp32ref mode tunes the last two) -- and keeps the fastest; phase 2 then times the
- * whole annotation for every fine-tune shape -- warps per CTA {8, 32} x split-path threshold
- * {4, 6, 9, 16, off} -- and keeps the fastest by wall time.  All choices stay set in the context.
+ * whole annotation for every fine-tune shape -- pipelined or not (exact mode) x warps per CTA
+ * {8, 32} x split-path threshold {4, 6, 9, 16, off} -- and keeps the fastest by wall time.  All choices stay set in the context.
  * learned = 1 tunes the learned form (sgr_annotate_learned with min_confidence / check_fraction), 0
  * the plain form.  Every candidate must give the same first (and, in phase 2, final) labels
  * (SGR_ERR_STATE otherwise).  The trials count in sgr_timings. */
@@ -177,6 +179,8 @@ typedef struct sgr_tuning {
     int32_t select_warps;
     int32_t score_trials;   /* phase-1 trials */
     double score_best_ms;   /* wall time of the chosen score step on the sample */
+    int32_t pipeline;       /* 1: each score block's fine-tune overlaps the next block's score step */
+    int32_t pad;
 } sgr_tuning;
 sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, float finetune_thre,
                         int32_t finetune_times, int32_t learned, float min_confidence, float check_fraction,

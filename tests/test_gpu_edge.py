@@ -255,7 +255,7 @@ def test_autotune_keeps_results():
     a = abi.Annotator(gpuid=0)
     a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
     t = a.autotune(prob.qry)
-    assert t["trials"] == 10 and t["score_trials"] == 16
+    assert t["trials"] == 20 and t["score_trials"] == 16 and t["pipeline"] in (0, 1)
     assert t["ft_warps"] in (8, 32) and t["ft_heavy"] in (4, 6, 9, 16, 1 << 30)
     assert t["score_chunk_mb"] in (256, 1024) and 0 < t["best_ms"] <= t["worst_ms"]
     assert t["corr_pair"] in (0, 1) and t["corr_gm"] in (1, 16) and t["select_warps"] in (0, 16)
@@ -294,3 +294,49 @@ def test_stream_of_batches_matches_one_call(learned):
         assert ms.shape == (len(batches),) and (ms >= 0).all()
         if learned:
             assert st["cells"] == q.n_rows and st["decided"] + st["finetuned"] == q.n_rows
+
+
+@pytest.mark.parametrize("host_input", [False, True])
+def test_pipelined_blocks_match_oracle(host_input):
+    """With 1 MiB score blocks (six blocks of the 800-cell query) each block's fine-tune runs on a
+    second stream while the next block is scored; first and final labels equal the oracle's, for a
+    device query and for a page-locked host query whose rows are copied block by block."""
+    import torch
+
+    prob = H.problem("small")
+    a = abi.Annotator(gpuid=0)
+    a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
+    a.set_tuning(2, 1)
+    a.set_tuning(9, 1)
+    q = prob.qry
+    keep = None
+    if host_input:
+        pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory()  # noqa: E731
+        keep = (pin(q.data), pin(q.indices), pin(q.indptr.astype(np.int32)))
+        csr = abi.SgrCsr(q.n_rows, q.n_cols, keep[0].data_ptr(), keep[1].data_ptr(), keep[2].data_ptr(), 0)
+    else:
+        dev = torch.device("cuda", 0)
+        keep = (torch.from_numpy(q.data).to(dev), torch.from_numpy(q.indices).to(dev),
+                torch.from_numpy(q.indptr.astype(np.int32)).to(dev))
+        csr = abi.device_csr(q.n_rows, q.n_cols, keep[0].data_ptr(), keep[1].data_ptr(), keep[2].data_ptr())
+    res = H.oracle_run("small", 1)
+    for _ in range(2):
+        first, final = a.annotate(csr)
+        assert np.array_equal(first, res["first"]) and np.array_equal(final, res["final"])
+
+
+def test_pipelined_learned_matches_unpipelined():
+    """The learned form with each block's routed cells fine-tuned on the second stream gives the same
+    labels and routing counts as the one-pass learned form."""
+    prob = H.problem("small")
+    a = abi.Annotator(gpuid=0)
+    a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
+    f0, fin0, sc = a.annotate(prob.qry, with_scores=True)
+    a.mlp_train(sc, fin0, epochs=5, batch=256, seed=1)
+    a.set_tuning(2, 1)
+    want = a.annotate_learned(prob.qry, min_confidence=0.9, check_fraction=0.2)
+    a.set_tuning(9, 1)
+    for _ in range(2):
+        got = a.annotate_learned(prob.qry, min_confidence=0.9, check_fraction=0.2)
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+        assert got[2] == want[2]
