@@ -118,6 +118,8 @@ struct sgr_ctx {
     DevBuf<float> ref_data;
     DevBuf<int32_t> ref_indices, ref_indptr;
     DevBuf<int32_t> ref_map_common, qry_map_common, ref_map_thre, qry_map_thre;
+    DevBuf<uint32_t> ref_bits, qry_bits;     // the score-step column maps as bits + per-word prefixes
+    DevBuf<uint16_t> ref_prefix, qry_prefix;
     DevBuf<int8_t> ref_limbs;
     DevBuf<int64_t> ref_n2;
     DevBuf<double> ref_rinv;
@@ -335,6 +337,9 @@ struct DevCsr {
 // score_device copies the rows chunk by chunk, overlapped with the scoring of earlier chunks.
 DevCsr query_on_device(sgr_ctx* ctx, const sgr_csr* q, bool defer_rows = false) {
     check_csr_shape(q, "query");
+    if (ctx->markers_ready && q->n_cols != ctx->mk.qry_colmap.size())
+        fail(SGR_ERR_INVALID_ARGUMENT, "query has " + std::to_string(q->n_cols) + " columns, the query gene names given "
+                                       "at training " + std::to_string(ctx->mk.qry_colmap.size()));
     if (q->on_device) {
         int32_t nnz = 0;
         if (q->n_rows) {
@@ -363,7 +368,7 @@ int sort_cap(int G) { return std::min(pow2_at_least(std::max(G, 32)), 4096); }
 
 // Gather + rank of rows [r0, r0 + n) of a device CSR; `group` (device) holds the outputs of row r0.
 void rank_range(sgr_ctx* ctx, const DevCsr& m, const RankGroup* group, int G, int Kp, uint32_t r0, uint32_t n,
-                int out_mode, int norm_mode) {
+                int out_mode, int norm_mode, const uint32_t* map_bits = nullptr, const uint16_t* map_prefix = nullptr) {
     RankLaunch a{};
     a.data = m.data;
     a.indices = m.indices;
@@ -380,13 +385,27 @@ void rank_range(sgr_ctx* ctx, const DevCsr& m, const RankGroup* group, int G, in
     a.status = ctx->status.p;
     a.overflow = ctx->rank_overflow.ensure(std::max<uint32_t>(n, 1));
     a.n_overflow = ctx->rank_n_overflow.ensure(1);
+    a.map_bits = map_bits;
+    a.map_prefix = map_prefix;
     launch_rank(a, ctx->stream);
 }
 
 // Gather + rank of rows [0, n) of a device CSR over one gene subset.
-void rank_rows(sgr_ctx* ctx, const DevCsr& m, const RankGroup& grp, int out_mode, int norm_mode) {
+void rank_rows(sgr_ctx* ctx, const DevCsr& m, const RankGroup& grp, int out_mode, int norm_mode,
+               const uint32_t* map_bits = nullptr, const uint16_t* map_prefix = nullptr) {
     ctx->rank_groups.upload(&grp, 1, ctx->stream);
-    rank_range(ctx, m, ctx->rank_groups.p, grp.G, grp.Kp, 0, m.n_rows, out_mode, norm_mode);
+    rank_range(ctx, m, ctx->rank_groups.p, grp.G, grp.Kp, 0, m.n_rows, out_mode, norm_mode, map_bits, map_prefix);
+}
+
+// The compact form (bits + per-word prefixes) of an increasing column map, uploaded.
+void upload_column_bits(const std::vector<int32_t>& colmap, DevBuf<uint32_t>& bits, DevBuf<uint16_t>& prefix,
+                        cudaStream_t s) {
+    const size_t n_words = (colmap.size() + 31) / 32;
+    std::vector<uint32_t> b(std::max<size_t>(n_words, 1), 0);
+    std::vector<uint16_t> p(std::max<size_t>(n_words, 1), 0);
+    column_bits(colmap.data(), (uint32_t)colmap.size(), b.data(), p.data());
+    bits.upload(b, s);
+    prefix.upload(p, s);
 }
 
 // The context's copy stream, created on first use.
@@ -502,8 +521,15 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     ctx->markers_ready = true;
     if (ctx->G > 8128) fail(SGR_ERR_UNSUPPORTED, "more than 8128 score-step marker genes");
     if (ctx->Wt > 40000) fail(SGR_ERR_UNSUPPORTED, "fine-tune gene pool above 40000 genes");
-    ctx->ref_map_common.upload(position_map(mk.ref_colmap, mk.common, mk.W), s);
-    ctx->qry_map_common.upload(position_map(mk.qry_colmap, mk.common, mk.W), s);
+    {
+        const std::vector<int32_t> rmap = position_map(mk.ref_colmap, mk.common, mk.W);
+        const std::vector<int32_t> qmap = position_map(mk.qry_colmap, mk.common, mk.W);
+        ctx->ref_map_common.upload(rmap, s);
+        ctx->qry_map_common.upload(qmap, s);
+        upload_column_bits(rmap, ctx->ref_bits, ctx->ref_prefix, s);
+        upload_column_bits(qmap, ctx->qry_bits, ctx->qry_prefix, s);
+        SGR_CUDA(cudaStreamSynchronize(s));  // the host maps are freed on leaving this block
+    }
     ctx->ref_map_thre.upload(position_map(mk.ref_colmap, mk.thre, mk.W), s);
     ctx->qry_map_thre.upload(position_map(mk.qry_colmap, mk.thre, mk.W), s);
 
@@ -516,7 +542,7 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     DevCsr rm{ctx->ref_data.p, ctx->ref_indices.p, ctx->ref_indptr.p, ctx->R, ctx->ref_cols, (int64_t)indptr[ctx->R]};
     RankGroup g{ctx->ref_map_common.p, ctx->G, ctx->Kp, ctx->ref_limbs.p, ctx->ref_n2.p, ctx->ref_rinv.p,
                 ctx->ref_f32.p};
-    rank_rows(ctx, rm, g, RANK_LIMBS, NORM_SEQ);
+    rank_rows(ctx, rm, g, RANK_LIMBS, NORM_SEQ, ctx->ref_bits.p, ctx->ref_prefix.p);
     ctx->h_ref_n2.resize(ctx->R);
     SGR_CUDA(cudaMemcpyAsync(ctx->h_ref_n2.data(), ctx->ref_n2.p, ctx->R * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     // fine-tune: reference compacted to the thre pool, each row's entries sorted by value
@@ -610,7 +636,7 @@ void ensure_ref_f16(sgr_ctx* ctx) {
     f32.ensure(ctx->R);
     DevCsr rm{ctx->ref_data.p, ctx->ref_indices.p, ctx->ref_indptr.p, ctx->R, ctx->ref_cols, -1};
     RankGroup g{ctx->ref_map_common.p, ctx->G, ctx->Kp, ctx->ref_f16.p, n2.p, rinv.p, f32.p};
-    rank_rows(ctx, rm, g, RANK_F16, NORM_NONE);
+    rank_rows(ctx, rm, g, RANK_F16, NORM_NONE, ctx->ref_bits.p, ctx->ref_prefix.p);
     SGR_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->ref_f16_ready = true;
 }
@@ -685,7 +711,8 @@ ScorePlan score_begin(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const 
     } else {
         const uint64_t l0 = launch_count();
         const int sp = ctx->prof.begin(ST_RANK, s);
-        rank_range(ctx, q, ctx->rank_groups.p, ctx->G, ctx->Kp, 0, Q, pl.rank_out, pl.rank_norm);
+        rank_range(ctx, q, ctx->rank_groups.p, ctx->G, ctx->Kp, 0, Q, pl.rank_out, pl.rank_norm, ctx->qry_bits.p,
+                   ctx->qry_prefix.p);
         ctx->prof.end(sp, s);
         ctx->prof.acc.rank_launches += launch_count() - l0;
     }
@@ -731,7 +758,8 @@ void score_block(sgr_ctx* ctx, const ScorePlan& pl, uint32_t c) {
         SGR_CUDA(cudaStreamWaitEvent(s, ctx->up_ev[c], 0));
         const uint64_t l0 = launch_count();
         sp = ctx->prof.begin(ST_RANK, s);
-        rank_range(ctx, pl.q, ctx->rank_groups.p + c, ctx->G, ctx->Kp, q0, (uint32_t)nq, pl.rank_out, pl.rank_norm);
+        rank_range(ctx, pl.q, ctx->rank_groups.p + c, ctx->G, ctx->Kp, q0, (uint32_t)nq, pl.rank_out, pl.rank_norm,
+                   ctx->qry_bits.p, ctx->qry_prefix.p);
         ctx->prof.end(sp, s);
         ctx->prof.acc.rank_launches += launch_count() - l0;
     }
@@ -1554,6 +1582,9 @@ void annotate_stream(sgr_ctx* ctx, const sgr_csr* batches, uint32_t n_batches, f
         const sgr_csr* m = batches + b;
         check_csr_shape(m, "query batch");
         if (m->on_device) fail(SGR_ERR_INVALID_ARGUMENT, "streamed query batches are host CSRs");
+        if (m->n_cols != ctx->mk.qry_colmap.size())
+            fail(SGR_ERR_INVALID_ARGUMENT, "a query batch's column count differs from the query gene names given at "
+                                           "training");
         validate_host_csr(m, "query batch");
         max_nnz = std::max<size_t>(max_nnz, (size_t)m->indptr[m->n_rows]);
         max_rows = std::max<size_t>(max_rows, (size_t)m->n_rows + 1);
@@ -2019,7 +2050,7 @@ sgr_status sgr_debug_ranks(sgr_ctx* ctx, const sgr_csr* rows, int which, int32_t
             ctx->q_rinv.ensure(n);
             ctx->q_f32.ensure(n);
             RankGroup g{ctx->qry_map_common.p, G, Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p};
-            rank_rows(ctx, q, g, RANK_LIMBS, NORM_NONE);
+            rank_rows(ctx, q, g, RANK_LIMBS, NORM_NONE, ctx->qry_bits.p, ctx->qry_prefix.p);
             limbs.resize((size_t)n * 3 * Kp);
             SGR_CUDA(cudaMemcpyAsync(limbs.data(), ctx->q_limbs.p, limbs.size(), cudaMemcpyDeviceToHost, s));
             check_status(ctx);
@@ -2051,7 +2082,8 @@ sgr_status sgr_debug_scores(sgr_ctx* ctx, const sgr_csr* qry, float* out) {
         const bool f16 = ctx->corr_f16 && !fp32;
         if (f16) ensure_ref_f16(ctx);
         RankGroup g{ctx->qry_map_common.p, ctx->G, ctx->Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p};
-        rank_rows(ctx, q, g, f16 ? RANK_F16 : RANK_LIMBS, fp32 ? NORM_SEQ : NORM_NONE);
+        rank_rows(ctx, q, g, f16 ? RANK_F16 : RANK_LIMBS, fp32 ? NORM_SEQ : NORM_NONE, ctx->qry_bits.p,
+                  ctx->qry_prefix.p);
         DevBuf<float> sc;
         sc.ensure((size_t)Q * R);
         correlate(ctx, fp32, ctx->q_limbs.p, (int)Q, 0, sc.p, R);

@@ -62,8 +62,20 @@ __device__ __forceinline__ int rank_bucket(uint64_t key, float fmin, float scale
 __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    // with a compact column map: its bits and per-word prefixes first, then the warps' buffers
+    const int n_words = (int)((a.n_cols + 31) / 32);
+    const int map_bytes = a.map_bits ? ((n_words * 6 + 15) & ~15) : 0;
+    uint32_t* sbits = reinterpret_cast<uint32_t*>(smem);
+    uint16_t* spre = reinterpret_cast<uint16_t*>(smem + 4 * n_words);
+    if (a.map_bits) {
+        for (int w = threadIdx.x; w < n_words; w += blockDim.x) {
+            sbits[w] = a.map_bits[w];
+            spre[w] = a.map_prefix[w];
+        }
+        __syncthreads();
+    }
     // per warp: keys (cap x 8 B) | values by bucket (cap x 4 B) | 256 bucket counts / ends | stage
-    uint64_t* keys = reinterpret_cast<uint64_t*>(smem + (size_t)warp * warp_bytes);
+    uint64_t* keys = reinterpret_cast<uint64_t*>(smem + map_bytes + (size_t)warp * warp_bytes);
     uint32_t* vals = reinterpret_cast<uint32_t*>(keys + a.cap);
     int* hist = reinterpret_cast<int*>(vals + a.cap);
     unsigned char* stage = reinterpret_cast<unsigned char*>(hist + 256);
@@ -84,29 +96,62 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
         // 1) compact the row's entries in the gene subset into (value key, position) sort keys;
         //    four chunks of 32 entries per step, their loads issued before any is used
         int k = 0, bad = 0;
-        for (int base = beg; base < end; base += 128) {
-            int c[4], pos[4];
-            float v[4];
+        if (a.map_bits) {
+            // compact map in shared memory: index and value loads are independent, one memory
+            // latency per step
+            for (int base = beg; base < end; base += 128) {
+                int c[4];
+                float v[4];
 #pragma unroll
-            for (int t = 0; t < 4; ++t) {
-                const int i = base + 32 * t + lane;
-                c[t] = i < end ? __ldg(a.indices + i) : -1;
-                bad |= (i < end && (unsigned)c[t] >= a.n_cols) ? 1 : 0;
-            }
-#pragma unroll
-            for (int t = 0; t < 4; ++t) pos[t] = (unsigned)c[t] < a.n_cols ? __ldg(g.colmap + c[t]) : -1;
-#pragma unroll
-            for (int t = 0; t < 4; ++t) v[t] = pos[t] >= 0 ? __ldg(a.data + base + 32 * t + lane) : 0.f;
-#pragma unroll
-            for (int t = 0; t < 4; ++t) {
-                const bool hit = pos[t] >= 0;
-                if (hit && v[t] != v[t]) bad |= 2;
-                const unsigned m = __ballot_sync(FULL, hit);
-                if (hit) {
-                    const int idx = k + __popc(m & ((1u << lane) - 1u));
-                    if (idx < a.cap) keys[idx] = ((uint64_t)ord_key(canon_zero(v[t])) << 32) | (uint32_t)pos[t];
+                for (int t = 0; t < 4; ++t) {
+                    const int i = base + 32 * t + lane;
+                    c[t] = i < end ? __ldcs(a.indices + i) : -1;
+                    v[t] = i < end ? __ldcs(a.data + i) : 0.f;
                 }
-                k += __popc(m);
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const int i = base + 32 * t + lane;
+                    bad |= (i < end && (unsigned)c[t] >= a.n_cols) ? 1 : 0;
+                    int pos = -1;
+                    if ((unsigned)c[t] < a.n_cols) {
+                        const uint32_t wv = sbits[c[t] >> 5], bit = 1u << (c[t] & 31);
+                        if (wv & bit) pos = (int)spre[c[t] >> 5] + __popc(wv & (bit - 1u));
+                    }
+                    const bool hit = pos >= 0;
+                    if (hit && v[t] != v[t]) bad |= 2;
+                    const unsigned m = __ballot_sync(FULL, hit);
+                    if (hit) {
+                        const int idx = k + __popc(m & ((1u << lane) - 1u));
+                        if (idx < a.cap) keys[idx] = ((uint64_t)ord_key(canon_zero(v[t])) << 32) | (uint32_t)pos;
+                    }
+                    k += __popc(m);
+                }
+            }
+        } else {
+            for (int base = beg; base < end; base += 128) {
+                int c[4], pos[4];
+                float v[4];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const int i = base + 32 * t + lane;
+                    c[t] = i < end ? __ldg(a.indices + i) : -1;
+                    bad |= (i < end && (unsigned)c[t] >= a.n_cols) ? 1 : 0;
+                }
+#pragma unroll
+                for (int t = 0; t < 4; ++t) pos[t] = (unsigned)c[t] < a.n_cols ? __ldg(g.colmap + c[t]) : -1;
+#pragma unroll
+                for (int t = 0; t < 4; ++t) v[t] = pos[t] >= 0 ? __ldg(a.data + base + 32 * t + lane) : 0.f;
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const bool hit = pos[t] >= 0;
+                    if (hit && v[t] != v[t]) bad |= 2;
+                    const unsigned m = __ballot_sync(FULL, hit);
+                    if (hit) {
+                        const int idx = k + __popc(m & ((1u << lane) - 1u));
+                        if (idx < a.cap) keys[idx] = ((uint64_t)ord_key(canon_zero(v[t])) << 32) | (uint32_t)pos[t];
+                    }
+                    k += __popc(m);
+                }
             }
         }
         bad = __reduce_or_sync(FULL, bad);
@@ -679,11 +724,20 @@ namespace {
 void launch_rank_tier(const RankLaunch& a, long max_blocks, cudaStream_t s) {
     const int stage_bytes = a.out_mode == RANK_LIMBS ? 3 * a.max_Kp : 2 * a.max_Kp;
     const int warp_bytes = ((a.cap * 12 + 256 * 4 + stage_bytes) + 15) & ~15;
-    const int budget = 200 * 1024;
-    int wpb = budget / warp_bytes;
-    if (wpb > 8) wpb = 8;
+    const int map_bytes = a.map_bits ? (int)(((a.n_cols + 31) / 32 * 6 + 15) & ~15u) : 0;
+    // warps per CTA: the most resident warps per SM, then the widest CTA
+    int wpb = 0, best = 0;
+    for (int w = 8; w >= 1; --w) {
+        const int sm_bytes = map_bytes + w * warp_bytes;
+        if (sm_bytes > 200 * 1024) continue;
+        const int resident = w * std::min(8, (228 * 1024) / (sm_bytes + 1024));
+        if (resident > best) {
+            best = resident;
+            wpb = w;
+        }
+    }
     if (wpb < 1) fail(SGR_ERR_UNSUPPORTED, "gene subset too wide for the rank kernel's shared memory");
-    const int smem = wpb * warp_bytes;
+    const int smem = map_bytes + wpb * warp_bytes;
     SGR_CUDA(cudaFuncSetAttribute(rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int per_sm = std::max(1, std::min(8, (228 * 1024) / (smem + 1024)));
     long blocks = (long)sm_count() * per_sm;
@@ -693,6 +747,23 @@ void launch_rank_tier(const RankLaunch& a, long max_blocks, cudaStream_t s) {
     count_launch();
 }
 }  // namespace
+
+void column_bits(const int32_t* colmap, uint32_t n_cols, uint32_t* bits, uint16_t* prefix) {
+    const uint32_t n_words = (n_cols + 31) / 32;
+    uint32_t count = 0;
+    for (uint32_t w = 0; w < n_words; ++w) {
+        if (count > 0xffffu) fail(SGR_ERR_UNSUPPORTED, "column subset above 65535 positions");
+        prefix[w] = (uint16_t)count;
+        uint32_t b = 0;
+        for (uint32_t i = 0; i < 32 && 32 * w + i < n_cols; ++i)
+            if (colmap[32 * w + i] >= 0) {
+                if ((uint32_t)colmap[32 * w + i] != count) fail(SGR_ERR_INVALID_ARGUMENT, "column map not increasing");
+                b |= 1u << i;
+                ++count;
+            }
+        bits[w] = b;
+    }
+}
 
 void launch_rank(const RankLaunch& a, cudaStream_t s) {
     if (a.n_items == 0) return;

@@ -70,7 +70,16 @@ struct RankLaunch {
     RankItem* overflow = nullptr;
     int* n_overflow = nullptr;
     const int* n_items_dev = nullptr;  // item count read from device memory (second tier)
+    // Optional compact form of the (one) column map every group shares, kept in shared memory: bit c
+    // of map_bits is set when column c is in the subset, and its position is map_prefix[c / 32] plus
+    // the set bits below it in its word (the map must be increasing over the subset's columns).
+    const uint32_t* map_bits = nullptr;
+    const uint16_t* map_prefix = nullptr;
 };
+
+// map_bits / map_prefix (ceil(n_cols / 32) words each) of an increasing column map (-1 = not in the
+// subset), on the host.
+void column_bits(const int32_t* colmap, uint32_t n_cols, uint32_t* bits, uint16_t* prefix);
 
 void launch_rank(const RankLaunch& a, cudaStream_t s);
 
