@@ -187,6 +187,10 @@ struct sgr_ctx {
     cudaEvent_t sq_up_start[2] = {nullptr, nullptr}, sq_up_done[2] = {nullptr, nullptr};
     cudaEvent_t sq_free[2] = {nullptr, nullptr}, sq_end = nullptr;
 
+    // the autotuner's device copy of a host sample
+    DevBuf<float> tn_data;
+    DevBuf<int32_t> tn_indices, tn_indptr;
+
     // per-call query buffers
     DevBuf<float> q_data;
     DevBuf<int32_t> q_indices, q_indptr;
@@ -1740,6 +1744,21 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
                         sgr_tuning* out) {
     if (!ctx || !sample || !out) return SGR_ERR_INVALID_ARGUMENT;
     if (ctx->device < 0) return SGR_ERR_STATE;
+    // a host sample is copied to the device once, so that the trials time the kernels and not the
+    // copy of the sample
+    sgr_csr dev_sample = *sample;
+    if (!sample->on_device) {
+        const sgr_status st0 = guarded(ctx, [&] {
+            validate_host_csr(sample, "sample");
+            const size_t nnz = (size_t)sample->indptr[sample->n_rows];
+            ctx->tn_data.upload(sample->data, nnz, ctx->stream);
+            ctx->tn_indices.upload(sample->indices, nnz, ctx->stream);
+            ctx->tn_indptr.upload(sample->indptr, (size_t)sample->n_rows + 1, ctx->stream);
+        });
+        if (st0 != SGR_OK) return st0;
+        dev_sample = sgr_csr{sample->n_rows, sample->n_cols, ctx->tn_data.p, ctx->tn_indices.p, ctx->tn_indptr.p, 1};
+    }
+    sample = &dev_sample;
     const uint32_t Q = sample->n_rows;
     std::vector<int32_t> first(std::max<uint32_t>(Q, 1)), fin(first.size()), first0, fin0;
     sgr_learned_stats st{};

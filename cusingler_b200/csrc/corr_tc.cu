@@ -56,18 +56,20 @@ constexpr int BN = 160;  // 3 x 160 accumulator columns fit TMEM's 512
 constexpr int HALF = BN / 2;       // columns per epilogue warp
 constexpr int CH = HALF / 16;      // 16-column TMEM chunks per epilogue warp
 constexpr int BK = 128;  // bytes of K per stage (one 128-byte swizzle row)
-constexpr int STAGES = 4;
+constexpr int STAGES = 5;
 constexpr int A_BYTES = BM * BK;
 constexpr int B_BYTES = BN * BK;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int TMEM_COLS = 512;
 constexpr int EPI_WARPS = 8;                // warps 4 .. 11
 constexpr int THREADS = 32 * (4 + EPI_WARPS);
-constexpr int STAGING_BYTES = BM * BN * 4;  // one score tile; 16-byte chunks XOR-swizzled by row
+// per epilogue warp, one 32-row x 16-column chunk of scores on its way to global memory
+constexpr int CHUNK_BYTES = 32 * 16 * 4;
+constexpr int STAGING_BYTES = EPI_WARPS * CHUNK_BYTES;
 // SM-pair form: per CTA 128 rows of A and BN / 2 rows of B per stage
 constexpr int B_HALF_BYTES = (BN / 2) * BK;
 constexpr int PAIR_STAGE_BYTES = A_BYTES + B_HALF_BYTES;  // 26 KB, a multiple of 1024
-constexpr int PAIR_STAGES = 5;
+constexpr int PAIR_STAGES = 7;
 constexpr int MAX_STAGES = PAIR_STAGES > STAGES ? PAIR_STAGES : STAGES;
 static_assert(PAIR_STAGE_BYTES % 1024 == 0, "stage buffers must keep 1024-byte alignment");
 constexpr long long WAIT_CYCLES = 4000000000LL;  // about 2 s at 1.9 GHz
@@ -278,9 +280,8 @@ __device__ __forceinline__ uint32_t ord_key(float f) {
 struct __align__(8) TcShared {
     uint64_t full[MAX_STAGES];
     uint64_t empty[MAX_STAGES];
-    uint64_t tmem_full;
-    uint64_t tmem_empty;    // accumulator regions of P1 and P3 released by the epilogue
-    uint64_t tmem_empty_c;  // accumulator region of P2 released
+    uint64_t acc_full[3];   // accumulator region g (P1, P3, P2; the F16 one is 0) holds its plane's sums
+    uint64_t acc_empty[3];  // ... and has been read by every epilogue warp
     uint64_t drain;
     uint32_t tmem_base;
     int abort_flag;
@@ -328,9 +329,10 @@ __global__ void __launch_bounds__(THREADS, 1)
             mbar_init(smem_u32(&sh.full[s]), 1);
             mbar_init(smem_u32(&sh.empty[s]), 1);
         }
-        mbar_init(smem_u32(&sh.tmem_full), 1);
-        mbar_init(smem_u32(&sh.tmem_empty), NEPI);
-        mbar_init(smem_u32(&sh.tmem_empty_c), NEPI);
+        for (int g = 0; g < 3; ++g) {
+            mbar_init(smem_u32(&sh.acc_full[g]), 1);
+            mbar_init(smem_u32(&sh.acc_empty[g]), NEPI);
+        }
         mbar_init(smem_u32(&sh.drain), 1);
         sh.abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -429,12 +431,20 @@ __global__ void __launch_bounds__(THREADS, 1)
                 }
             };
             for (int t = unit; t < n_tiles && ok; t += n_units, ++tile_iter) {
-                if (!mbar_wait<PAIR>(smem_u32(&sh.tmem_empty), (tile_iter & 1) ^ 1, abort_flag)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
                 for (int kb = 0; kb < kblocks; ++kb, ++it) {
+                    // groups of k-blocks: H plane -> P1 (region 0), S plane -> P3 (region 1),
+                    // L plane -> P2 (region 2); a region is written once the previous tile's epilogue
+                    // has read it, and signalled as soon as its plane is done, so the epilogue drains
+                    // P1 and P3 while the later planes are still being multiplied
+                    const int grp = kb / seg_blocks;
+                    const bool first = (kb % seg_blocks) == 0;
+                    if (first) {
+                        if (!mbar_wait<PAIR>(smem_u32(&sh.acc_empty[grp]), (tile_iter & 1) ^ 1, abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                    }
                     const int s = it % NST;
                     const uint32_t ph = (it / NST) & 1;
                     if (!mbar_wait<PAIR>(smem_u32(&sh.full[s]), ph, abort_flag)) {
@@ -442,20 +452,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                         break;
                     }
                     tc_fence_after();
-                    // groups of k-blocks: H plane -> P1 (region 0), S plane -> P3 (region 1),
-                    // L plane -> P2 (region 2), which may still be read by the previous epilogue
-                    const int grp = F16 ? 2 : kb / seg_blocks;  // the F16 accumulator is released with P2's barrier
-                    if (kb == (F16 ? 0 : 2 * seg_blocks)) {
-                        if (!mbar_wait<PAIR>(smem_u32(&sh.tmem_empty_c), (tile_iter & 1) ^ 1, abort_flag)) {
-                            ok = false;
-                            break;
-                        }
-                        tc_fence_after();
-                    }
                     const uint32_t a_addr = smem_u32(smem + s * SBYTES);
                     const uint64_t da = smem_desc(a_addr), db = smem_desc(a_addr + A_BYTES);
-                    const uint32_t tc = tmem + (F16 ? 0 : grp * BN);
-                    const bool first = (kb % seg_blocks) == 0;
+                    const uint32_t tc = tmem + grp * BN;
 #pragma unroll
                     for (int k = 0; k < BK / 32; ++k) {  // 32 bytes of K per MMA (32 int8 or 16 half)
                         const uint32_t acc = (first && k == 0) ? 0u : 1u;
@@ -467,9 +466,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                             umma_i8(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, acc);
                     }
                     commit(&sh.empty[s]);
+                    if (kb % seg_blocks == seg_blocks - 1) commit(&sh.acc_full[grp]);
                 }
                 if (!ok) break;
-                commit(&sh.tmem_full);
             }
             if (!ok) give_up();
             // every MMA this thread issued has finished before TMEM is freed (in both CTAs of a pair)
@@ -482,18 +481,28 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     } else if (warp >= 4) {
         // ---- epilogue ------------------------------------------------------------------------
-        // Lane = tile row (32 * quarter + lane); this warp's 64 columns are scored into the staging
-        // tile, TMEM is released, and the warp then stores its 32 rows x 64 columns, 16 lanes per
-        // row.  Staging row r holds 16-byte chunk c at position c ^ (r & 7): conflict-free for both
-        // the row-per-lane writes and the row-contiguous reads.  A warp reads back only what it
-        // wrote, so the next tile may overwrite the staging rows once the warp's stores are issued.
+        // Lane = tile row (32 * quarter + lane); this warp scores its 80 columns in chunks of 16.
+        // Each chunk goes through the warp's 32 x 16 staging buffer: lane r writes row r's four
+        // 16-byte pieces at position u ^ ((r >> 1) & 3) (conflict-free), and the warp then stores
+        // 8 rows x 64 contiguous bytes per instruction.
         const int quarter = warp & 3, half = (warp - 4) >> 2;
-        float4* staging = reinterpret_cast<float4*>(smem + NST * SBYTES);
+        float4* chunk = reinterpret_cast<float4*>(smem + NST * SBYTES + (warp - 4) * CHUNK_BYTES);
         const bool vec_store = (ld % 4) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
         const int row = 32 * quarter + lane;
         // the accumulators are released on the leader's barriers (this CTA's own when alone)
-        const uint32_t rel_ab = PAIR ? mapa(smem_u32(&sh.tmem_empty), 0) : smem_u32(&sh.tmem_empty);
-        const uint32_t rel_c = PAIR ? mapa(smem_u32(&sh.tmem_empty_c), 0) : smem_u32(&sh.tmem_empty_c);
+        auto release = [&](int g) {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                if (PAIR) mbar_arrive_cluster(mapa(smem_u32(&sh.acc_empty[g]), 0));
+                else mbar_arrive(smem_u32(&sh.acc_empty[g]));
+            }
+        };
+        auto acquire = [&](int g, uint32_t parity) {
+            const bool got = __all_sync(0xffffffffu, mbar_wait<PAIR>(smem_u32(&sh.acc_full[g]), parity, abort_flag));
+            if (got) tc_fence_after();
+            return got;
+        };
         uint32_t tile_iter = 0;
         for (int t = unit; t < n_tiles; t += n_units, ++tile_iter) {
             int mb, nb;
@@ -508,32 +517,42 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const int r = n0 + half * HALF + c * 16 + lane;
                 rrv[c] = (lane < 16 && r < R) ? rr[r] : 0.0;  // NaN for a constant reference row
             }
-            const bool got =
-                __all_sync(0xffffffffu, mbar_wait<PAIR>(smem_u32(&sh.tmem_full), tile_iter & 1, abort_flag));
+            const uint32_t par = tile_iter & 1;
+            const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
+            // phase 1: T = 127 P1 + P3 for this warp's columns; P1 is released as soon as it is read,
+            // P3 likewise, while the MMA works on the later planes
+            int T[CH][16];
+            bool got = true;
+            if (!F16) {
+                got = acquire(0, par);
+                if (got) {
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) {
+                        uint32_t pa[16];
+                        tmem_ld16(lane_base + half * HALF + c * 16, pa);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) T[c][j] = 127 * (int)pa[j];
+                    }
+                    release(0);
+                    got = acquire(1, par);
+                }
+                if (got) {
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) {
+                        uint32_t pb[16];
+                        tmem_ld16(lane_base + BN + half * HALF + c * 16, pb);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) T[c][j] += (int)pb[j];
+                    }
+                    release(1);
+                }
+            }
+            if (got) got = acquire(F16 ? 0 : 2, par);
             if (!got) {
                 if (lane == 0) give_up();
                 break;
-            }
-            tc_fence_after();
-            const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
-            float4* srow = staging + row * (BN / 4);
-            // phase 1: T = 127 P1 + P3 for this warp's columns, then P1 and P3 are released
-            int T[CH][16];
-#pragma unroll
-            for (int c = 0; c < CH; ++c) {
-                if (F16) break;
-                uint32_t pa[16], pb[16];
-                tmem_ld16(lane_base + half * HALF + c * 16, pa);
-                tmem_ld16(lane_base + BN + half * HALF + c * 16, pb);
-                tmem_wait_ld();
-#pragma unroll
-                for (int j = 0; j < 16; ++j) T[c][j] = 127 * (int)pa[j] + (int)pb[j];
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) {
-                if (PAIR) mbar_arrive_cluster(rel_ab);
-                else mbar_arrive(rel_ab);
             }
             // per-(query, label) extremes of this warp's columns, flushed at label ends (labels are
             // column ranges, the same for every lane, so the flushes are warp-uniform)
@@ -551,8 +570,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                 lab = lo;
                 lab_end = __ldg(ext.lstart + lab + 1);
             }
-            // phase 2: P2 (the F16 accumulator), reads one chunk ahead of the arithmetic
+            // phase 2: P2 (the F16 accumulator), reads one chunk ahead of the arithmetic; each chunk of
+            // scores is staged and stored before the next
             const uint32_t base2 = lane_base + (F16 ? 0 : 2 * BN);
+            constexpr int last_region = F16 ? 0 : 2;
             uint32_t p2[2][16];
             tmem_ld16(base2 + half * HALF, p2[0]);
             tmem_wait_ld();
@@ -570,7 +591,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
-                    srow[((col0 >> 2) + u) ^ (row & 7)] = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+                    chunk[lane * 4 + (u ^ ((lane >> 1) & 3))] =
+                        make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
                 if (ext.kmin && n0 + col0 + 16 <= min(lab_end, R)) {  // the chunk lies in one label
                     float a0 = fminf(fminf(v[0], v[1]), fminf(v[2], v[3]));
                     float b0 = fmaxf(fmaxf(v[0], v[1]), fmaxf(v[2], v[3]));
@@ -605,36 +627,31 @@ __global__ void __launch_bounds__(THREADS, 1)
                     }
                 }
                 if (c + 1 < CH) tmem_wait_ld();
-            }
-            // all of this warp's TMEM reads are done: release its share of P2
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) {
-                if (PAIR) mbar_arrive_cluster(rel_c);
-                else mbar_arrive(rel_c);
+                else release(last_region);  // all of this warp's TMEM reads are done
+                // the chunk's 32 rows x 16 columns: lane l stores piece l % 4 of row l / 4 (+ 8 i)
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = 8 * i + (lane >> 2), u = lane & 3;
+                    const int qq = m0 + 32 * quarter + r, col = n0 + col0 + 4 * u;
+                    const float4 val = chunk[r * 4 + (u ^ ((r >> 1) & 3))];
+                    if (qq >= nq || col >= R) continue;
+                    float* dst = out + (size_t)qq * ld + col;
+                    if (vec_store && col + 3 < R) {
+                        *reinterpret_cast<float4*>(dst) = val;
+                    } else {
+                        dst[0] = val.x;
+                        if (col + 1 < R) dst[1] = val.y;
+                        if (col + 2 < R) dst[2] = val.z;
+                        if (col + 3 < R) dst[3] = val.w;
+                    }
+                }
+                __syncwarp();  // the next chunk may overwrite the staging buffer
             }
             if (ext.kmin && seen && q < nq) {
                 atomicMin(ext.kmin + (size_t)q * ext.L + lab, ord_key(mnf));
                 atomicMax(ext.kmax + (size_t)q * ext.L + lab, ord_key(mxf));
             }
-            constexpr int F4 = HALF / 4;  // 16-byte chunks per row of this warp
-#pragma unroll 4
-            for (int it = lane; it < 32 * F4; it += 32) {
-                const int rr_ = 32 * quarter + it / F4, c4 = half * F4 + it % F4;
-                const int qq = m0 + rr_, col = n0 + 4 * c4;
-                if (qq >= nq || col >= R) continue;
-                const float4 val = staging[rr_ * (BN / 4) + (c4 ^ (rr_ & 7))];
-                float* dst = out + (size_t)qq * ld + col;
-                if (vec_store && col + 3 < R) {
-                    *reinterpret_cast<float4*>(dst) = val;
-                } else {
-                    dst[0] = val.x;
-                    if (col + 1 < R) dst[1] = val.y;
-                    if (col + 2 < R) dst[2] = val.z;
-                    if (col + 3 < R) dst[3] = val.w;
-                }
-            }
-            __syncwarp();
         }
     }
     __syncthreads();

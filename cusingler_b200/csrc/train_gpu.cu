@@ -96,8 +96,9 @@ __device__ __forceinline__ int scaled_diff(float a, float b) {
     return (int)round(__dmul_rn((double)__fsub_rn(a, b), 1e6));
 }
 
+// (0x7fffffff - d) in unsigned arithmetic: negative d would overflow a signed subtraction
 __device__ __forceinline__ uint64_t desc_key(int d, uint32_t g) {
-    return ((uint64_t)(uint32_t)(0x7fffffff - d) << 32) | g;
+    return ((uint64_t)(0x7fffffffu - (uint32_t)d) << 32) | g;
 }
 
 // block-wide sum of per-thread values

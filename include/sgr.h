@@ -157,8 +157,9 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
 sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value);
 sgr_status sgr_reset_timings(sgr_ctx* ctx);
 
-/* Autotuner (no counterpart in the reference).  Phase 1 times the score step of `sample` (host or
- * device CSR) for every score-step shape -- correlation on one CTA or an SM pair per tile x tile
+/* Autotuner (no counterpart in the reference).  A host `sample` is first copied to the device once
+ * (the trials then time the kernels, not the copy).  Phase 1 times the score step of `sample` for
+ * every score-step shape -- correlation on one CTA or an SM pair per tile x tile
  * order of 1 or 16 bands per group x score block {256, 1024} MiB x selection form {warp per row,
  * 16-warp row-staging CTA}
  * (exact mode; fp32ref mode tunes the last two) -- and keeps the fastest; phase 2 then times the
