@@ -290,6 +290,35 @@ def stream_leg(args, ann, torch, world, wl, rank, learned):
     return out
 
 
+def sweep(args, ann, abi, torch, csr_dev, stream):
+    """Device stage times of the score step (rank, correlation, selection) for every score-step
+    shape the autotuner chooses from, on the device-resident batch; first labels must not change."""
+    base = None
+    shapes = [(pair, gm, mb, sel) for pair in (0, 1) for gm in (1, 16, 64) for mb in (256, 1024)
+              for sel in (0, 1, 16)]
+    for pair, gm, mb, sel in shapes:
+        for what, value in ((5, pair), (6, gm), (2, mb), (7, sel)):
+            ann.set_tuning(what, value)
+        ann.score_first(csr_dev)
+        torch.cuda.synchronize()
+        ann.reset_timings()
+        ann.set_profiling(True)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            first, _, _ = ann.score_first(csr_dev)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ann.set_profiling(False)
+        t = ann.timings()
+        if base is None:
+            base = first
+        print(json.dumps({"corr_pair": pair, "corr_gm": gm, "score_chunk_mb": mb, "select_form": sel,
+                          "score_step_ms": ev0.elapsed_time(ev1) / args.steps,
+                          **{k: t[k] / args.steps for k in ("rank_ms", "corr_ms", "select_ms")},
+                          "first_labels_unchanged": bool(np.array_equal(first, base))}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -317,6 +346,9 @@ def main():
     ap.add_argument("--batch-cells", type=int, default=65536)
     ap.add_argument("--distinct-batches", type=int, default=8)
     ap.add_argument("--stream-passes", type=int, default=2)
+    ap.add_argument("--sweep", action="store_true",
+                    help="time the score step for every score-step shape on the batch (device stage times, one "
+                         "JSON line per shape) instead of the bench line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -371,6 +403,11 @@ def main():
         t = torch.tensor([v], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if args.sweep:
+        sweep(args, ann, abi, torch, csr_dev, stream)
+        ann.close()
+        return
 
     use_learned = args.form in ("learned", "both") and mode == abi.MODE_EXACT
     mlp_info = None

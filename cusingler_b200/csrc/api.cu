@@ -141,7 +141,7 @@ struct sgr_ctx {
     int corr_f16 = 0;              // tuning: score-step correlation on FP16 operands (not exact)
     int corr_pair = 0;             // tuning: exact correlation on SM pairs (cta_group::2, 256-row tiles)
     int corr_gm = 1;               // tuning: row bands per group of the correlation's tile order
-    int select_warps = 16;         // tuning: score-step selection, 8 or 16 warps per row-staging CTA, 0 a warp per row
+    int select_warps = 16;         // tuning: score-step selection, 8 or 16 warps per row-staging CTA, 0 / 1 a warp per row
     int host_training = 0;         // tuning: marker medians and pair lists on the host instead of the device
     int pipeline = 0;              // tuning: fine-tune each score block on its own stream while the next is scored
     cudaStream_t ft_s = nullptr;   // the pipelined fine-tune's stream
@@ -1800,7 +1800,7 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
     // phase 1: score-step shapes (correlation form and tile order, score block, selection CTA width),
     // each timed on the score step of the sample; first labels must not change
     const bool exact = ctx->mode == SGR_MODE_EXACT;
-    const int pairs[] = {0, 1}, gms[] = {1, 16}, chunk_mb[] = {256, 1024}, sel_w[] = {0, 16};
+    const int pairs[] = {0, 1}, gms[] = {1, 16}, chunk_mb[] = {256, 1024}, sel_w[] = {0, 1, 16};
     double score_best = 1e300;
     for (int pr : pairs)
         for (int gm : gms) {
@@ -1914,7 +1914,7 @@ sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value) {
         return SGR_OK;
     }
     if (what == 7) {
-        if (value != 0 && value != 8 && value != 16) return SGR_ERR_INVALID_ARGUMENT;
+        if (value != 0 && value != 1 && value != 8 && value != 16) return SGR_ERR_INVALID_ARGUMENT;
         ctx->select_warps = value;
         return SGR_OK;
     }

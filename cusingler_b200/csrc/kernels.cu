@@ -573,8 +573,10 @@ __global__ void __launch_bounds__(NW * 32) select_first_kernel(const float* scor
 // (global memory; a label's second pass hits L1 / L2), so no block barrier waits for a row's longest
 // label, and a CTA needs only a histogram per warp (up to 64 warps per SM).  Every row has the same
 // labels, so the warps' work is balanced by construction.  Each warp prefetches its next row into L2.
-template <int NW>
-__global__ void __launch_bounds__(NW * 32) select_rows_kernel(const float* scores, int64_t ld, int nq, int L,
+// MINB: CTAs per SM the register allocation is sized for (2: 64 registers, 4: 32 registers and 64
+// warps per SM).
+template <int NW, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) select_rows_kernel(const float* scores, int64_t ld, int nq, int L,
                                                            const LabelQ* lq, float p, float thre,
                                                            const int64_t* qn2, float* label_scores, int32_t* first,
                                                            uint8_t* flags, float* scratch, int64_t spw, int* status,
@@ -952,13 +954,14 @@ void launch_select_first(const float* scores, int64_t ld, int nq, int L, const L
                          const uint32_t* ext_min, const uint32_t* ext_max, int warps) {
     if (nq <= 0) return;
     const size_t stage_bytes = (((size_t)std::max(row_len, 1) * 4 + 15) & ~size_t(15));
-    if (lorder && warps == 0) {  // one warp per row, 16 warps per CTA, up to 4 CTAs per SM
+    if (lorder && (warps == 0 || warps == 1)) {  // one warp per row, 16 warps per CTA
+        auto kern = warps == 1 ? select_rows_kernel<16, 4> : select_rows_kernel<16, 2>;
         int per_sm = 0;
-        SGR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, select_rows_kernel<16>, 512, 0));
+        SGR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 512, 0));
         per_sm = std::max(1, std::min(per_sm, 4));  // scratch is sized for 64 warps per SM
         const unsigned blocks = (unsigned)std::min<long>((nq + 15) / 16, (long)sm_count() * per_sm);
-        select_rows_kernel<16><<<blocks, 512, 0, s>>>(scores, ld, nq, L, lq, p, thre, qn2, label_scores, first, flags,
-                                                      scratch, spw, status, row_len, lorder, ext_min, ext_max);
+        kern<<<blocks, 512, 0, s>>>(scores, ld, nq, L, lq, p, thre, qn2, label_scores, first, flags, scratch, spw,
+                                    status, row_len, lorder, ext_min, ext_max);
     } else if (lorder && stage_bytes <= 200 * 1024) {
         auto kern = warps == 8 ? select_first_kernel<true, 8> : select_first_kernel<true, 16>;
         const int threads = 32 * (warps == 8 ? 8 : 16);

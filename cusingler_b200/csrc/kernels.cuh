@@ -130,7 +130,8 @@ LabelQ make_lq(int start, int len, float p);
 // and rows of at most 200 KB, each block stages its row in shared memory before selecting.
 // ext_min / ext_max (optional, staged path): per (row, label) extreme order keys from the
 // correlation epilogue, used instead of a min / max pass for lists that cannot hold NaN.  warps: 8 or 16
-// warps per CTA of the staged form (a block per row), 0 the warp-per-row form (with `lorder`).
+// warps per CTA of the staged form (a block per row), 0 the warp-per-row form (with `lorder`), 1 the
+// warp-per-row form with 32 registers per thread (64 warps per SM).
 void launch_select_first(const float* scores, int64_t ld, int nq, int L, const LabelQ* lq, float p,
                          float thre, const int64_t* qn2, float* label_scores, int32_t* first, uint8_t* flags,
                          float* scratch, int64_t scratch_per_warp, int* status, int row_len, const int32_t* lorder,

@@ -147,7 +147,8 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
  * tiles), 0 one CTA per 128-row tile; what 6: row bands per group of the correlation's tile order
  * (1 to 4096; the bands of a group sweep the reference together so that the CTAs at work share
  * operand tiles in L2); what 7: the score-step selection's form: 8 or 16 warps per CTA that stages
- * a query row in shared memory, or 0 for one warp per query row reading the scores directly;
+ * a query row in shared memory, 0 for one warp per query row reading the scores directly, 1 the
+ * same with 32 registers per thread (twice the warps per SM);
  * what 8: 1 trains the markers on the host instead of the device; what 9 (exact mode): 1 fine-tunes
  * each score block on a second stream while the next block is scored.
  * No choice above changes any result.  what 4 (exact mode only; no counterpart in the reference):
@@ -160,8 +161,8 @@ sgr_status sgr_reset_timings(sgr_ctx* ctx);
 /* Autotuner (no counterpart in the reference).  A host `sample` is first copied to the device once
  * (the trials then time the kernels, not the copy).  Phase 1 times the score step of `sample` for
  * every score-step shape -- correlation on one CTA or an SM pair per tile x tile
- * order of 1 or 16 bands per group x score block {256, 1024} MiB x selection form {warp per row,
- * 16-warp row-staging CTA}
+ * order of 1 or 16 bands per group x score block {256, 1024} MiB x selection form {warp per row at
+ * 64 or 32 registers, 16-warp row-staging CTA}
  * (exact mode; fp32ref mode tunes the last two) -- and keeps the fastest; phase 2 then times the
  * whole annotation for every fine-tune shape -- pipelined or not (exact mode) x warps per CTA
  * {8, 32} x split-path threshold {4, 6, 9, 16, off} -- and keeps the fastest by wall time.  All choices stay set in the context.

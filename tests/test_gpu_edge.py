@@ -126,7 +126,7 @@ def test_dense_rows_take_the_large_sort_tier(mode):
         assert np.array_equal(d_ref[i], orc.rank_row(0, i)), i
 
 
-@pytest.mark.parametrize("select_form", [0, 16])
+@pytest.mark.parametrize("select_form", [0, 1, 16])
 def test_long_labels_ties_and_nan_lists(select_form):
     """Long score lists in exact mode.  Five labels, four of them over 1,024 reference cells: one long
     label holds an empty reference row (its lists hold NaN and are sorted exactly), one holds 1,000
@@ -255,10 +255,10 @@ def test_autotune_keeps_results():
     a = abi.Annotator(gpuid=0)
     a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
     t = a.autotune(prob.qry)
-    assert t["trials"] == 20 and t["score_trials"] == 16 and t["pipeline"] in (0, 1)
+    assert t["trials"] == 20 and t["score_trials"] == 24 and t["pipeline"] in (0, 1)
     assert t["ft_warps"] in (8, 32) and t["ft_heavy"] in (4, 6, 9, 16, 1 << 30)
     assert t["score_chunk_mb"] in (256, 1024) and 0 < t["best_ms"] <= t["worst_ms"]
-    assert t["corr_pair"] in (0, 1) and t["corr_gm"] in (1, 16) and t["select_warps"] in (0, 16)
+    assert t["corr_pair"] in (0, 1) and t["corr_gm"] in (1, 16) and t["select_warps"] in (0, 1, 16)
     first, final = a.annotate(prob.qry)
     o = H.oracle_run("families", 1)
     assert np.array_equal(first, o["first"]) and np.array_equal(final, o["final"])

@@ -148,7 +148,7 @@ def test_correlation_forms_bit_exact(kind, pair, gm):
 
 
 @pytest.mark.parametrize("kind", ["tiny", "families", "small"])
-@pytest.mark.parametrize("form", [0, 8])
+@pytest.mark.parametrize("form", [0, 1, 8])
 def test_selection_forms(kind, form):
     """The score-step selection as one warp per query row (form 0) and as 8-warp row-staging CTAs
     gives the oracle's label scores (ulp-equal), first labels and flags."""
