@@ -131,7 +131,8 @@ struct sgr_ctx {
     DevBuf<int32_t> d_ell_off;     // fine-tune lists: start of each 32-row block in ref_sorted
     uint32_t R32 = 0;              // reference rows with each label's range padded to a multiple of 32
     int pack_shift = 0;            // packed fine-tune row scan (0: not representable, plain scan)
-    int pack_scan = 1;             // tuning: use the packed scan when representable
+    int pack_scan = 2;             // tuning: packed scan when representable (2: and narrow when representable)
+    bool pack_narrow = false;      // the trained reference allows 32-bit run sums
     DevBuf<uint32_t> ref_sorted;       // thre-pool entries of each reference row, by value
     DevBuf<uint32_t> d_ctidx, d_ft_genes, d_ft_idx;
     DevBuf<int32_t> d_gene_thre;
@@ -589,6 +590,10 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
         const int shift = 32 - cbits;
         ctx->pack_shift = (shift > 0 && max_row * 2 * (int64_t)std::max<uint32_t>(ctx->Wt, 1) < (int64_t(1) << shift))
                               ? shift : 0;
+        // 32-bit run sums: X <= 4 k^2 Wt and sum b^3 <= k^3 for the longest row k
+        const int64_t wt = std::max<uint32_t>(ctx->Wt, 1);
+        ctx->pack_narrow = ctx->pack_shift > 0 && 4 * max_row * max_row * wt < (int64_t(1) << 32) &&
+                           max_row * max_row * max_row < (int64_t(1) << 32);
     }
     ctx->d_blk_base.upload(blk_base, s);
     ctx->d_ell_off.upload(ell_off, s);
@@ -1148,6 +1153,7 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     FtPersistentArgs a{};
     a.ref_sorted = ctx->ref_sorted.p;
     a.pack_shift = ctx->pack_scan ? ctx->pack_shift : 0;
+    a.narrow = ctx->pack_scan == 2 && ctx->pack_narrow ? 1 : 0;
     a.blk_base = ctx->d_blk_base.p;
     a.ell_off = ctx->d_ell_off.p;
     a.ctidx = ctx->d_ctidx.p;
@@ -1899,7 +1905,7 @@ sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value) {
         return SGR_OK;
     }
     if (what == 3) {
-        if (value != 0 && value != 1) return SGR_ERR_INVALID_ARGUMENT;
+        if (value < 0 || value > 2) return SGR_ERR_INVALID_ARGUMENT;
         ctx->pack_scan = value;
         return SGR_OK;
     }

@@ -337,21 +337,47 @@ __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const 
         const int sh = a.pack_shift;
         const uint32_t low = (1u << sh) - 1u;
         uint32_t acc = 0;
-        for (int t = 0; t < n4; ++t) {
-            const uint4 w4 = nxt;
-            if (t + 1 < n4) nxt = __ldg(p + 32 * (t + 1));
-            const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
+        if (a.narrow) {
+            // X, sum b^3 fit 32 bits (the host checked 4 k^2 Wt < 2^32 and k^3 < 2^32 for the longest
+            // row k): a run end is applied with masks, the same instructions for every lane, and
+            // T = sum b^3 - k_r at the end
+            uint32_t X32 = 0, B3 = 0;
+            for (int t = 0; t < n4; ++t) {
+                const uint4 w4 = nxt;
+                if (t + 1 < n4) nxt = __ldg(p + 32 * (t + 1));
+                const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const uint32_t ent = ws[u];
-                acc += ep[ent & 0xffffu];
-                if ((int32_t)ent < 0) {  // last entry of its value run
-                    const uint32_t b = acc >> sh, sum = acc & low;
-                    X += (uint64_t)(2 * ka + b) * sum;
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t ent = ws[u];
+                    acc += ep[ent & 0xffffu];
+                    const uint32_t m = (uint32_t)((int32_t)ent >> 31);  // all ones at a run's last entry
+                    const uint32_t b = (acc >> sh) & m, sum = acc & low & m;
+                    X32 += (2 * ka + b) * sum;
                     Y += sum;
-                    T += (uint64_t)b * (b * b - 1u);
+                    B3 += b * b * b;
                     ka += b;
-                    acc = 0;
+                    acc &= ~m;
+                }
+            }
+            X = X32;
+            T = (uint64_t)(B3 - ka);
+        } else {
+            for (int t = 0; t < n4; ++t) {
+                const uint4 w4 = nxt;
+                if (t + 1 < n4) nxt = __ldg(p + 32 * (t + 1));
+                const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t ent = ws[u];
+                    acc += ep[ent & 0xffffu];
+                    if ((int32_t)ent < 0) {  // last entry of its value run
+                        const uint32_t b = acc >> sh, sum = acc & low;
+                        X += (uint64_t)(2 * ka + b) * sum;
+                        Y += sum;
+                        T += (uint64_t)b * (b * b - 1u);
+                        ka += b;
+                        acc = 0;
+                    }
                 }
             }
         }

@@ -220,6 +220,7 @@ struct FtPersistentArgs {
     int max_rcand, max_label, capq;
     int* status;
     int pack_shift;               // > 0: row scan on packed e-values (count << shift | e-sum); 0: plain
+    int narrow;                   // with pack_shift: 32-bit run sums and masked run ends (bounds checked)
 };
 
 // Split path for heavy cells: state arrays of H cells (device), one round per launch_split_round.

@@ -141,8 +141,9 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
  * what 1: candidate count from which a cell's fine-tune rounds are spread over the whole GPU
  * instead of one CTA (>= 2; large values disable the split path); what 2: MiB of score-step
  * correlations per block of queries (small blocks are read back from L2 by the selection); what 3:
- * 1 (default) lets the fine-tune row scan keep each value run's count and e-sum in one packed
- * 32-bit word when the trained reference allows it, 0 always uses the two-register scan; what 5:
+ * 1 lets the fine-tune row scan keep each value run's count and e-sum in one packed 32-bit word when
+ * the trained reference allows it, 2 (default) also keeps the run sums in 32 bits and applies run
+ * ends with masks when the row lengths allow it, 0 always uses the two-register scan; what 5:
  * 1 runs the exact correlation on SM pairs (clusters of two CTAs, tcgen05 cta_group::2, 256-row
  * tiles), 0 one CTA per 128-row tile; what 6: row bands per group of the correlation's tile order
  * (1 to 4096; the bands of a group sweep the reference together so that the CTAs at work share

@@ -97,11 +97,11 @@ def test_annotate_matches_steps():
     assert len(H.unexplained_flips(final, fp["final"], fp["margin_final"])) == 0
 
 
-@pytest.mark.parametrize("kind", ["tiny", "families"])
-@pytest.mark.parametrize("packed", [0, 1])
+@pytest.mark.parametrize("kind", ["tiny", "families", "small"])
+@pytest.mark.parametrize("packed", [0, 1, 2])
 def test_final_labels_both_row_scans(kind, packed):
-    """The fine-tune row scan on packed (count, e-sum) words and on two registers give the oracle's
-    final labels and round counts."""
+    """The fine-tune row scan on two registers, on packed (count, e-sum) words, and on packed words
+    with 32-bit run sums and masked run ends gives the oracle's final labels and round counts."""
     a, prob = annotator(kind, abi.MODE_EXACT)
     a.set_tuning(3, packed)
     res = H.oracle_run(kind, 1)
