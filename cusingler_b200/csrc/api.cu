@@ -128,6 +128,7 @@ struct sgr_ctx {
     DevBuf<float> reff_data;
     DevBuf<int32_t> reff_indices, reff_indptr;
     DevBuf<int32_t> d_blk_base;    // fine-tune lists: first 32-row block of each label
+    DevBuf<uint32_t> d_row_perm;   // fine-tune lists: block position -> position in the label's rows
     DevBuf<int32_t> d_ell_off;     // fine-tune lists: start of each 32-row block in ref_sorted
     uint32_t R32 = 0;              // reference rows with each label's range padded to a multiple of 32
     int pack_shift = 0;            // packed fine-tune row scan (0: not representable, plain scan)
@@ -561,18 +562,31 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     std::vector<int32_t> blk_base(L + 1), ell_base(std::max<uint32_t>(ctx->R, 1)), ell_len(std::max<uint32_t>(ctx->R, 1));
     std::vector<int32_t> ell_off{0};
     ctx->R32 = 0;
+    // inside each label the rows are laid out longest first, so that a block's rows are of similar
+    // length (less padding); row_perm maps a row's block position back to its position in the label
+    std::vector<uint32_t> row_perm(std::max<uint32_t>(ctx->R, 1));
     for (uint32_t l = 0; l < L; ++l) {
         const uint32_t start = mk.ctidx[2 * l], len = mk.ctidx[2 * l + 1];
+        std::vector<uint32_t> order(len);
+        for (uint32_t j = 0; j < len; ++j) order[j] = j;
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+            return fptr[start + x + 1] - fptr[start + x] > fptr[start + y + 1] - fptr[start + y];
+        });
+        for (uint32_t j = 0; j < len; ++j) row_perm[start + j] = order[j];
         blk_base[l] = (int32_t)ell_off.size() - 1;
         ctx->R32 += (len + 31) & ~31u;
         for (uint32_t b0 = 0; b0 < len; b0 += 32) {
             const uint32_t nb = std::min<uint32_t>(32, len - b0);
             int mx = 0;
-            for (uint32_t t = 0; t < nb; ++t) mx = std::max(mx, fptr[start + b0 + t + 1] - fptr[start + b0 + t]);
+            for (uint32_t t = 0; t < nb; ++t) {
+                const uint32_t r = start + order[b0 + t];
+                mx = std::max(mx, fptr[r + 1] - fptr[r]);
+            }
             const int len4 = (mx + 3) & ~3;
             for (uint32_t t = 0; t < nb; ++t) {
-                ell_base[start + b0 + t] = ell_off.back() + 4 * (int32_t)t;
-                ell_len[start + b0 + t] = len4;
+                const uint32_t r = start + order[b0 + t];
+                ell_base[r] = ell_off.back() + 4 * (int32_t)t;
+                ell_len[r] = len4;
             }
             const int64_t next = (int64_t)ell_off.back() + 32ll * len4;
             if (next > INT32_MAX) fail(SGR_ERR_UNSUPPORTED, "fine-tune reference lists exceed 2^31 entries");
@@ -595,6 +609,7 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
         ctx->pack_narrow = ctx->pack_shift > 0 && 4 * max_row * max_row * wt < (int64_t(1) << 32) &&
                            max_row * max_row * max_row < (int64_t(1) << 32);
     }
+    ctx->d_row_perm.upload(row_perm, s);
     ctx->d_blk_base.upload(blk_base, s);
     ctx->d_ell_off.upload(ell_off, s);
     DevBuf<int32_t> d_base, d_len;
@@ -1154,6 +1169,7 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     a.ref_sorted = ctx->ref_sorted.p;
     a.pack_shift = ctx->pack_scan ? ctx->pack_shift : 0;
     a.narrow = ctx->pack_scan == 2 && ctx->pack_narrow ? 1 : 0;
+    a.row_perm = ctx->d_row_perm.p;
     a.blk_base = ctx->d_blk_base.p;
     a.ell_off = ctx->d_ell_off.p;
     a.ctidx = ctx->d_ctidx.p;

@@ -311,8 +311,11 @@ __device__ void label_offsets(const FtPersistentArgs& a, const uint8_t* top, int
 
 // Exact correlation over S of the query (eqv, kq, nq) with reference row slot f of the list.
 // One thread: one pass over the row's value-sorted entries (see the top of this file).
+// The rows of a label are scanned in the order of their 32-row blocks (rows sorted by length inside
+// the label, so that a block's rows are of similar length); *dest receives the score's slot in the
+// label's original row order, which the quantile's NaN-order rules depend on.
 __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const int* off, int ntop, int f,
-                           const int* eqv, int nS, int kq, int64_t nq, double rq) {
+                           const int* eqv, int nS, int kq, int64_t nq, double rq, int* dest) {
     int lo = 0, hi = ntop - 1;  // label slot: off[lo] <= f < off[lo+1]
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -320,7 +323,9 @@ __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const 
         else hi = mid - 1;
     }
     const int lab = top[lo], j = f - off[lo];
+    *dest = f;
     if (j >= (int)a.ctidx[2 * lab + 1]) return 0.f;  // padding slot of the label's range
+    if (a.row_perm) *dest = off[lo] + (int)a.row_perm[a.ctidx[2 * lab] + j];
     const int blk = a.blk_base[lab] + (j >> 5);
     const int beg = a.ell_off[blk], n4 = (a.ell_off[blk + 1] - beg) >> 7;
     const uint4* p = reinterpret_cast<const uint4*>(a.ref_sorted + beg) + (j & 31);
@@ -516,8 +521,11 @@ __global__ void __launch_bounds__(NW * 32) ft_persistent_kernel(FtPersistentArgs
             const int kq = sh.kq;
             const int64_t nq = sh.nq;
             const double rq = sh.rq;
-            for (int f = tid; f < total; f += NW * 32)
-                scores[f] = row_score(a, top, off, ntop, f, eqv, nS, kq, nq, rq);
+            for (int f = tid; f < total; f += NW * 32) {
+                int dst;
+                const float v = row_score(a, top, off, ntop, f, eqv, nS, kq, nq, rq, &dst);
+                scores[dst] = v;
+            }
             __syncthreads();
             cta_label_quantiles<NW>(a, top, off, ntop, scores, lsc, hist, nan_scratch);
             if (tid == 0) sh.ntop = decide_top(lsc, ntop, top, ntopv, a.thre);
@@ -635,9 +643,11 @@ __global__ void __launch_bounds__(256) split_scan_kernel(FtPersistentArgs a, FtS
     for (int t = threadIdx.x; t <= ntop; t += 256) off[t] = sp.off[(size_t)i * 257 + t];
     for (int t = threadIdx.x; t < ntop; t += 256) top[t] = sp.top[(size_t)i * 256 + t];
     __syncthreads();
-    if (f < total)
-        sp.scores[(size_t)i * sp.max_rcand + f] =
-            row_score(a, top, off, ntop, f, eqv, sp.nS[i], sp.kq[i], sp.nq[i], sp.rq[i]);
+    if (f < total) {
+        int dst;
+        const float v = row_score(a, top, off, ntop, f, eqv, sp.nS[i], sp.kq[i], sp.nq[i], sp.rq[i], &dst);
+        sp.scores[(size_t)i * sp.max_rcand + dst] = v;
+    }
 }
 
 // Per-label quantiles and the keep / drop rule per heavy cell.  grid = H.

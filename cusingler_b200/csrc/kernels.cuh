@@ -221,6 +221,7 @@ struct FtPersistentArgs {
     int* status;
     int pack_shift;               // > 0: row scan on packed e-values (count << shift | e-sum); 0: plain
     int narrow;                   // with pack_shift: 32-bit run sums and masked run ends (bounds checked)
+    const uint32_t* row_perm;     // per reference row slot in block order: its position in the label's row order
 };
 
 // Split path for heavy cells: state arrays of H cells (device), one round per launch_split_round.
