@@ -174,6 +174,35 @@ def cpu_reference(args, wl, ref, qry, steps, warmup, sample):
     return sample / per_step, cores, per_step
 
 
+def reference_prep(ref, qry, names, genes, sample=256):
+    """The reference's own host preparation (its io.cpp compiled from the reference sources into
+    oracle/_ref): gene intersection, marker training, and the marker-column filter of the full
+    reference and of `sample` query cells, all host threads.  The counterpart of ref_prep_s; None
+    when oracle/_ref was not built."""
+    from oracle import oracle as O
+
+    if O.ref_lib() is None:
+        return None
+    cores = os.cpu_count() or 1
+    sub = qry.rows(0, min(sample, qry.n_rows))
+    prob = O.Problem(ref, sub, names, ref.labels, genes, genes)
+    sys.stdout.flush()
+    saved = os.dup(1)
+    try:  # the reference prints its matrix shapes on stdout; keep the bench line alone there
+        with open(os.devnull, "w") as null:
+            os.dup2(null.fileno(), 1)
+            t0 = time.perf_counter()
+            host = O.RefHost(prob, cores)
+            dt = time.perf_counter() - t0
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+    del host
+    return {"seconds": dt, "cores": cores, "kind": "reference",
+            "stages": f"prepareData .. trainData .. generateDenseMatrix, full reference and {sub.n_rows} "
+                      "query cells"}
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -609,6 +638,9 @@ def main():
         v, cores, per = cpu_reference(args, wl, ref, qry, 1, 0, args.cpu_sample)
         cpu = {"value": v, "unit": "cells/s", "cores": cores, "kind": "port",
                "sample": f"{args.cpu_sample} query cells of the same batch, full reference, {per:.1f} s"}
+    ref_prep_cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        ref_prep_cpu = reference_prep(ref, qry, names, genes)
 
     if rank == 0:
         line = {
@@ -626,7 +658,8 @@ def main():
             "e2e_labels_equal_device_input": e2e_labels_equal,
             "gpu_launches": int(tm["launches"]),
             "roofline": dominant, "rooflines": [roof_corr, roof_rank, roof_sel],
-            "stages_ms": stages, "ref_prep_s": ref_prep_s, "forms": form_lines, "mlp": mlp_info,
+            "stages_ms": stages, "ref_prep_s": ref_prep_s, "ref_prep_reference": ref_prep_cpu,
+            "forms": form_lines, "mlp": mlp_info,
             "tuning": tuning, "fp16_variant": fp16, "parity": parity, "stream": stream_out,
             **ft_stats(tm, steps),
             "clocks": clk, "cpu_baseline": cpu,

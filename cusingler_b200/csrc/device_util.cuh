@@ -157,7 +157,9 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
     const float span = fmax - fmin;
     if (!(span > 1e-30f) || !(span < 1e30f)) return false;
     const float scale = 256.0f / span;
-    auto bin_of = [&](float x) { return min(255, (int)((x - fmin) * scale)); };
+    // clamped both ways, so that a value outside [min, max] (extremes supplied by the caller that do
+    // not match the list) still lands in a bin rather than outside the histogram
+    auto bin_of = [&](float x) { return max(0, min(255, (int)((x - fmin) * scale))); };
     for (int b = lane; b < 256; b += 32) hist[b] = 0;
     __syncwarp();
     int i = lane;
