@@ -127,6 +127,8 @@ struct sgr_ctx {
     std::vector<int64_t> h_ref_n2;
     DevBuf<float> reff_data;
     DevBuf<int32_t> reff_indices, reff_indptr;
+    DevBuf<int> sp_items;          // split path: two chunk lists
+    DevBuf<int> sp_nitems;         // split path: their lengths
     DevBuf<int32_t> d_blk_base;    // fine-tune lists: first 32-row block of each label
     DevBuf<uint32_t> d_row_perm;   // fine-tune lists: block position -> position in the label's rows
     DevBuf<int32_t> d_ell_off;     // fine-tune lists: start of each 32-row block in ref_sorted
@@ -1291,11 +1293,16 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
         SGR_CUDA(cudaMemsetAsync(ctx->sp_state.p, 0, H * sizeof(int), s));
         ctx->sp_rows.ensure(1);
         SGR_CUDA(cudaMemsetAsync(ctx->sp_rows.p, 0, sizeof(unsigned long long), s));
+        const int max_chunks = (int)((ctx->R32 + 255) / 256);
+        ctx->sp_items.ensure((size_t)2 * H * max_chunks);
+        ctx->sp_nitems.ensure(2);
+        SGR_CUDA(cudaMemsetAsync(ctx->sp_nitems.p, 0, 2 * sizeof(int), s));
         FtSplit sp{ctx->sp_cells.p, ctx->sp_top.p, ctx->sp_ntop.p, ctx->sp_rounds.p, ctx->sp_times.p,
                    ctx->sp_state.p, ctx->sp_nS.p, ctx->sp_kq.p, ctx->sp_nq.p, ctx->sp_rq.p, ctx->sp_total.p,
-                   ctx->sp_off.p, ctx->sp_eqv.p, ctx->sp_scores.p, ctx->sp_nan.p, (int)ctx->R32, ctx->sp_rows.p};
-        const int max_chunks = (int)((ctx->R32 + 255) / 256);
+                   ctx->sp_off.p, ctx->sp_eqv.p, ctx->sp_scores.p, ctx->sp_nan.p, (int)ctx->R32, ctx->sp_rows.p,
+                   ctx->sp_items.p, ctx->sp_nitems.p, H * max_chunks, max_chunks};
         split_round_setup(a);
+        launch_split_first(a, sp, H, s);
         // Rounds run kRoundsPerGraph at a time from one CUDA graph (rounds of finished cells do
         // nothing), with one host check of the cells' states per graph launch; a stream that
         // cannot be captured runs the same rounds as plain launches.
@@ -1305,7 +1312,7 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
             const uint64_t before = launch_count();
             cudaGraph_t graph = nullptr;
             try {
-                for (int r = 0; r < kRoundsPerGraph; ++r) launch_split_round(a, sp, H, max_chunks, s);
+                for (int r = 0; r < kRoundsPerGraph; ++r) launch_split_round(a, sp, H, r & 1, s);
             } catch (...) {
                 cudaStreamEndCapture(s, &graph);
                 if (graph) cudaGraphDestroy(graph);
@@ -1332,10 +1339,10 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
                     cudaGraphExecDestroy(exec);
                     SGR_CUDA(e);
                 }
-                count_launch(3 * kRoundsPerGraph);
+                count_launch(2 * kRoundsPerGraph);
                 rounds_run += kRoundsPerGraph;
             } else {
-                launch_split_round(a, sp, H, max_chunks, s);
+                launch_split_round(a, sp, H, (int)(rounds_run & 1), s);
                 rounds_run += 1;
             }
             const int cur = launched & 1;

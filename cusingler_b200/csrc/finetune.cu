@@ -142,9 +142,28 @@ __device__ int cta_gene_set(const FtPersistentArgs& a, const uint8_t* top, int n
     for (int w = tid; w < nwords; w += NW * 32) bits[w] = 0u;
     __syncthreads();
     const int gthre = a.gene_thre[ntop];
-    // a warp takes 32 ordered pairs at a time: each lane fetches one pair's list, then the warp
-    // walks the 32 lists together so that the gene loads of several pairs are in flight at once
-    for (int base = warp * 32; base < ntop * ntop; base += NW * 32) {
+    const int np = ntop * ntop;
+    if (np <= 4 * NW) {
+        // few pairs: warps take pairs round robin, and with more warps than pairs each pair's list is
+        // cut into interleaved segments, so that every warp has loads in flight
+        const int segs = max(1, NW / np);
+        for (int u = warp; u < np * segs; u += NW) {
+            const int pr = u % np, seg = u / np;
+            const int i = pr / ntop, j = pr % ntop;
+            if (i == j) continue;
+            const size_t pi = (size_t)top[i] * a.L + top[j];
+            const uint32_t pos = a.ft_idx[2 * pi];
+            const int len = min((int)a.ft_idx[2 * pi + 1], gthre);
+#pragma unroll 4
+            for (int e = seg * 32 + lane; e < len; e += 32 * segs) {
+                const uint32_t g = __ldg(a.ft_genes + pos + e);
+                atomicOr(&bits[g >> 5], 1u << (g & 31));
+            }
+        }
+    }
+    // many pairs: a warp takes 32 ordered pairs at a time: each lane fetches one pair's list, then the
+    // warp walks the 32 lists together so that the gene loads of several pairs are in flight at once
+    for (int base = warp * 32; np > 4 * NW && base < np; base += NW * 32) {
         const int pr = base + lane;
         uint32_t pos = 0;
         int len = 0;
@@ -189,31 +208,27 @@ __device__ void cta_query_ranks(const FtPersistentArgs& a, int cell, int nS, con
                                 uint64_t* qkeys, uint32_t* qvals, int* qhist, int* kq_out, int64_t* nq_out,
                                 double* rq_out) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int beg = a.qf_ptr[cell], end = a.qf_ptr[cell + 1];
     for (int g = tid; g < a.Wt; g += NW * 32) eqv[g] = (bits[g >> 5] >> (g & 31)) & 1u ? 0 : SENT;
-    if (tid == 0) eqv[a.Wt] = SENT;  // the pad entries' gene id
+    if (tid == 0) {
+        eqv[a.Wt] = SENT;  // the pad entries' gene id
+        qhist[0] = 0;
+    }
     __syncthreads();
-    if (warp == 0) {
-        const int beg = a.qf_ptr[cell], end = a.qf_ptr[cell + 1];
-        int k = 0;
-        for (int base = beg; base < end; base += 32) {
-            const int i = base + lane;
-            bool hit = false;
-            uint64_t key = 0;
-            if (i < end) {
-                const int g = a.qf_idx[i];
-                if ((bits[g >> 5] >> (g & 31)) & 1u) {
-                    hit = true;
-                    key = ((uint64_t)ord_key(canon_zero(a.qf_data[i])) << 32) | (uint32_t)g;
-                }
-            }
-            const unsigned m = __ballot_sync(FULL, hit);
-            if (hit) {
-                const int o = k + __popc(m & ((1u << lane) - 1u));
-                if (o < a.capq) qkeys[o] = key;
-            }
-            k += __popc(m);
+    // the query's stored entries inside S, gathered by the whole CTA in any order (the ranks below
+    // count #less / #equal, which do not depend on it)
+    for (int i = beg + tid; i < end; i += NW * 32) {
+        const int g = a.qf_idx[i];
+        if ((bits[g >> 5] >> (g & 31)) & 1u) {
+            const uint64_t key = ((uint64_t)ord_key(canon_zero(a.qf_data[i])) << 32) | (uint32_t)g;
+            const int o = atomicAdd(&qhist[0], 1);
+            if (o < a.capq) qkeys[o] = key;
         }
-        __syncwarp();
+    }
+    __syncthreads();
+    const int k = qhist[0];
+    __syncthreads();  // qhist is the ranking's scratch below
+    if (warp == 0) {
         int64_t sq = 0;
         if (k <= a.capq) {
             // #less / #equal through 256 value buckets (as in the score step's rank kernel)
@@ -309,11 +324,33 @@ __device__ void label_offsets(const FtPersistentArgs& a, const uint8_t* top, int
     off[ntop] = o;
 }
 
+// Walks a row's n4 16-byte entry vectors (32 vectors apart: the rows of a block are interleaved)
+// with PF loads in flight: PF = 1 where many warps hide the latency (the work queue), deeper where
+// few rows are scored at once (the late rounds of the spread path).
+template <int PF, class F>
+__device__ __forceinline__ void scan_words(const uint4* p, int n4, F&& fn) {
+    uint4 buf[PF];
+#pragma unroll
+    for (int u = 0; u < PF; ++u) buf[u] = u < n4 ? __ldg(p + 32 * u) : make_uint4(0u, 0u, 0u, 0u);
+    for (int t0 = 0; t0 < n4; t0 += PF) {
+#pragma unroll
+        for (int u = 0; u < PF; ++u) {
+            const int t = t0 + u;
+            if (t < n4) {
+                const uint4 w4 = buf[u];
+                if (t + PF < n4) buf[u] = __ldg(p + 32 * (t + PF));
+                fn(w4);
+            }
+        }
+    }
+}
+
 // Exact correlation over S of the query (eqv, kq, nq) with reference row slot f of the list.
 // One thread: one pass over the row's value-sorted entries (see the top of this file).
 // The rows of a label are scanned in the order of their 32-row blocks (rows sorted by length inside
 // the label, so that a block's rows are of similar length); *dest receives the score's slot in the
 // label's original row order, which the quantile's NaN-order rules depend on.
+template <int PF>
 __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const int* off, int ntop, int f,
                            const int* eqv, int nS, int kq, int64_t nq, double rq, int* dest) {
     int lo = 0, hi = ntop - 1;  // label slot: off[lo] <= f < off[lo+1]
@@ -333,7 +370,6 @@ __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const 
     // Bounds (|S| <= Wt <= 40000, e <= 2|S|): sum, Y, z * sum / z < 2^32, b^3 < 2^63.
     uint32_t ka = 0, Y = 0;
     uint64_t X = 0, T = 0;
-    uint4 nxt = n4 > 0 ? __ldg(p) : make_uint4(0u, 0u, 0u, 0u);
     if (a.pack_shift) {
         // packed e-values: (1 << shift) + e at genes of S, 0 elsewhere, so one add per entry keeps
         // the run's count (high bits) and e-sum (low bits); the host chose shift so that neither
@@ -347,9 +383,7 @@ __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const 
             // row k): a run end is applied with masks, the same instructions for every lane, and
             // T = sum b^3 - k_r at the end
             uint32_t X32 = 0, B3 = 0;
-            for (int t = 0; t < n4; ++t) {
-                const uint4 w4 = nxt;
-                if (t + 1 < n4) nxt = __ldg(p + 32 * (t + 1));
+            scan_words<PF>(p, n4, [&](const uint4 w4) {
                 const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
@@ -363,13 +397,11 @@ __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const 
                     ka += b;
                     acc &= ~m;
                 }
-            }
+            });
             X = X32;
             T = (uint64_t)(B3 - ka);
         } else {
-            for (int t = 0; t < n4; ++t) {
-                const uint4 w4 = nxt;
-                if (t + 1 < n4) nxt = __ldg(p + 32 * (t + 1));
+            scan_words<PF>(p, n4, [&](const uint4 w4) {
                 const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
@@ -384,13 +416,11 @@ __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const 
                         acc = 0;
                     }
                 }
-            }
+            });
         }
     } else {
         uint32_t b = 0, sum = 0;
-        for (int t = 0; t < n4; ++t) {
-            const uint4 w4 = nxt;
-            if (t + 1 < n4) nxt = __ldg(p + 32 * (t + 1));
+        scan_words<PF>(p, n4, [&](const uint4 w4) {
             const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
@@ -407,7 +437,7 @@ __device__ float row_score(const FtPersistentArgs& a, const uint8_t* top, const 
                     sum = 0;
                 }
             }
-        }
+        });
     }
     const int64_t kr = ka;
     const int64_t N = (int64_t)X + ((int64_t)nS - kr) * (int64_t)Y - (int64_t)nS * kq * kr;
@@ -523,7 +553,7 @@ __global__ void __launch_bounds__(NW * 32) ft_persistent_kernel(FtPersistentArgs
             const double rq = sh.rq;
             for (int f = tid; f < total; f += NW * 32) {
                 int dst;
-                const float v = row_score(a, top, off, ntop, f, eqv, nS, kq, nq, rq, &dst);
+                const float v = row_score<1>(a, top, off, ntop, f, eqv, nS, kq, nq, rq, &dst);
                 scores[dst] = v;
             }
             __syncthreads();
@@ -539,18 +569,36 @@ __global__ void __launch_bounds__(NW * 32) ft_persistent_kernel(FtPersistentArgs
     }
 }
 
-// ---- split path: one round of many heavy cells spread over the whole GPU ----------------------
+// ---- split path: the rounds of many heavy cells spread over the whole GPU ----------------------
 //
 // State per heavy cell i (device arrays of FtSplit): candidate list, its length, rounds, times used,
-// active flag; per round: the query's e-values, |S|, k_q, n_q, label offsets, and the scores.
+// state; per round: the query's e-values, |S|, k_q, n_q, label offsets and the scores.  A round is
+// two launches: the scan of the 256-row chunks of every active cell (a compact chunk list, filled by
+// the previous launch), then per cell the quantiles, the keep / drop rule and the setup of its next
+// round (gene set, query ranks, its chunks appended to the other list).  The cells that take many
+// rounds keep many candidates for most of them, so the scan stays the bulk of the work: chunks are
+// spread over a grid of 16 CTAs per SM, rows scanned with four loads in flight, and the scores of a
+// round are staged in shared memory for the quantiles.
 
-// Round setup per heavy cell: round condition, gene set, query ranks, label offsets.  grid = H.
-__global__ void __launch_bounds__(256) split_prepare_kernel(FtPersistentArgs a, FtSplit sp) {
-    extern __shared__ __align__(16) unsigned char smem[];
+constexpr int SPLIT_STAGE = 12288;  // rows of a round whose scores are staged for the quantiles
+constexpr int SPLIT_SCAN_PF = 4;    // entry vectors in flight per row in the spread scan
+constexpr int SPLIT_SCAN_CTAS = 16; // scan CTAs per SM
+
+// Cell i is done: its first candidate is the final label.  One thread.
+__device__ void split_finish(const FtPersistentArgs& a, const FtSplit& sp, int i, int cell, int ntop) {
+    a.final_labels[cell] = ntop > 0 ? (int32_t)sp.top[(size_t)i * 256] : 0;
+    if (a.rounds) a.rounds[cell] = sp.rounds[i];
+    sp.state[i] = 2;
+    sp.total[i] = 0;
+}
+
+// Setup of cell i's next round, CTA-wide (256 threads): the round condition, gene set, the query's
+// ranks (e-values into sp.eqv), label offsets, and the round's chunks appended to chunk list q.
+// smem: split_prepare_smem bytes.
+__device__ void split_setup_round(const FtPersistentArgs& a, const FtSplit& sp, int i, int q, unsigned char* smem) {
     constexpr int NW = 8;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int i = blockIdx.x;
-    const int Wt = a.Wt, L = a.L;
+    const int tid = threadIdx.x;
+    const int Wt = a.Wt;
     const int nwords = (Wt + 31) / 32;
     int* eqv = reinterpret_cast<int*>(smem);
     uint32_t* bits = reinterpret_cast<uint32_t*>(eqv + ((Wt + 4) & ~3));
@@ -558,118 +606,143 @@ __global__ void __launch_bounds__(256) split_prepare_kernel(FtPersistentArgs a, 
     uint32_t* qvals = reinterpret_cast<uint32_t*>(qkeys + a.capq);
     int* qhist = reinterpret_cast<int*>(qvals + a.capq);  // 512
     int* red = qhist + 512;
-    __shared__ int s_ntop, s_go;
-    uint8_t* top = sp.top + (size_t)i * 256;
+    __shared__ int s_go, s_kq;
+    __shared__ int64_t s_nq;
+    __shared__ double s_rq;
     const int cell = sp.cells[i];
-    if (tid == 0) {
-        if (sp.state[i] == 0) {  // first round: candidates from the flags
-            s_ntop = -1;
-        } else {
-            s_ntop = sp.ntop[i];
-        }
-    }
-    __syncthreads();
-    if (s_ntop < 0) {
-        if (warp == 0) {
-            const int n = warp_flagged_labels(a.flags + (size_t)cell * L, L, top, lane);
-            if (lane == 0) {
-                s_ntop = n;
-                sp.ntop[i] = n;
-                sp.rounds[i] = 0;
-                sp.times[i] = 0;
-                sp.state[i] = 1;
-            }
-        }
-        __syncthreads();
-    }
-    const int ntop = s_ntop;
+    const uint8_t* top = sp.top + (size_t)i * 256;
+    const int ntop = sp.ntop[i];
     if (tid == 0) {
         bool go = sp.state[i] == 1 && ntop > 1;
         if (go && a.times != 0) go = sp.times[i]++ < a.times;
-        if (!go) {
-            if (sp.state[i] == 1) {
-                a.final_labels[cell] = ntop > 0 ? (int32_t)top[0] : 0;
-                if (a.rounds) a.rounds[cell] = sp.rounds[i];
-            }
-            sp.state[i] = 2;  // finished
-        } else {
-            sp.rounds[i]++;
-        }
+        if (go) sp.rounds[i]++;
+        else split_finish(a, sp, i, cell, ntop);
         s_go = go;
-        sp.total[i] = 0;
     }
     __syncthreads();
     if (!s_go) return;
     const int nS = cta_gene_set<NW>(a, top, ntop, bits, red);
-    if (nS < 20) {  // keep the first candidate
-        if (tid == 0) sp.ntop[i] = 1;
+    if (nS < 20) {  // keep the first candidate (src/cusingler.cu:1158-1159)
+        if (tid == 0) {
+            sp.ntop[i] = 1;
+            split_finish(a, sp, i, cell, 1);
+        }
         return;
     }
-    __shared__ int s_kq;
-    __shared__ int64_t s_nq;
-    __shared__ double s_rq;
     cta_query_ranks<NW>(a, cell, nS, bits, eqv, qkeys, qvals, qhist, &s_kq, &s_nq, &s_rq);
     int* geqv = sp.eqv + (size_t)i * Wt;
     for (int g = tid; g < Wt; g += NW * 32) geqv[g] = eqv[g];
     if (tid == 0) {
-        label_offsets(a, top, ntop, sp.off + (size_t)i * 257);
+        int* off = sp.off + (size_t)i * 257;
+        label_offsets(a, top, ntop, off);
+        const int total = off[ntop];
         sp.nS[i] = nS;
         sp.kq[i] = s_kq;
         sp.nq[i] = s_nq;
         sp.rq[i] = s_rq;
-        sp.total[i] = sp.off[(size_t)i * 257 + ntop];
-        atomicAdd(sp.rows_scored, (unsigned long long)sp.total[i]);
+        sp.total[i] = total;
+        atomicAdd(sp.rows_scored, (unsigned long long)total);
+        const int nch = (total + 255) / 256;
+        const int base = atomicAdd(sp.n_items + q, nch);
+        int* items = sp.items + (size_t)q * sp.max_items;
+        for (int c = 0; c < nch; ++c) items[base + c] = i * sp.max_chunks + c;
     }
 }
 
-// Scores of 256-row chunks of every heavy cell's candidate rows.  grid = (chunks, H).
-__global__ void __launch_bounds__(256) split_scan_kernel(FtPersistentArgs a, FtSplit sp) {
+// First round of every heavy cell: candidates from the flags, then the round's setup (chunk list 0).
+// grid = H.
+__global__ void __launch_bounds__(256) split_first_kernel(FtPersistentArgs a, FtSplit sp) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int i = blockIdx.y;
-    const int total = sp.total[i];
-    const int f = blockIdx.x * 256 + threadIdx.x;
-    if ((int)blockIdx.x * 256 >= total) return;
+    const int i = blockIdx.x, lane = threadIdx.x & 31;
+    if (threadIdx.x < 32) {
+        const int n = warp_flagged_labels(a.flags + (size_t)sp.cells[i] * a.L, a.L, sp.top + (size_t)i * 256, lane);
+        if (lane == 0) {
+            sp.ntop[i] = n;
+            sp.rounds[i] = 0;
+            sp.times[i] = 0;
+            sp.state[i] = 1;
+            sp.total[i] = 0;
+        }
+    }
+    __syncthreads();
+    split_setup_round(a, sp, i, 0, smem);
+}
+
+// Scores of the chunks on list q (item i * max_chunks + c: rows [256 c, 256 c + 256) of cell i's
+// round); also clears the other list's count for the setups that follow.  Fixed grid striding over
+// the items; a CTA reloads the cell's tables (e-values, offsets, candidates) when the cell changes.
+__global__ void __launch_bounds__(256) split_scan_kernel(FtPersistentArgs a, FtSplit sp, int q) {
+    extern __shared__ __align__(16) unsigned char smem[];
     int* eqv = reinterpret_cast<int*>(smem);
     int* off = eqv + ((a.Wt + 4) & ~3);
     uint8_t* top = reinterpret_cast<uint8_t*>(off + 260);
-    const int* geqv = sp.eqv + (size_t)i * a.Wt;
-    const int ntop = sp.ntop[i];
-    if (a.pack_shift) {
-        for (int g = threadIdx.x; g < a.Wt; g += 256) eqv[g] = pack_e(geqv[g], a.pack_shift);
-    } else {
-        for (int g = threadIdx.x; g < a.Wt; g += 256) eqv[g] = geqv[g];
-    }
-    if (threadIdx.x == 0) eqv[a.Wt] = a.pack_shift ? 0 : SENT;
-    for (int t = threadIdx.x; t <= ntop; t += 256) off[t] = sp.off[(size_t)i * 257 + t];
-    for (int t = threadIdx.x; t < ntop; t += 256) top[t] = sp.top[(size_t)i * 256 + t];
-    __syncthreads();
-    if (f < total) {
-        int dst;
-        const float v = row_score(a, top, off, ntop, f, eqv, sp.nS[i], sp.kq[i], sp.nq[i], sp.rq[i], &dst);
-        sp.scores[(size_t)i * sp.max_rcand + dst] = v;
+    __shared__ int s_ntop;
+    if (blockIdx.x == 0 && threadIdx.x == 0) sp.n_items[q ^ 1] = 0;
+    const int n = sp.n_items[q];
+    const int* items = sp.items + (size_t)q * sp.max_items;
+    int cur = -1;
+    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+        const int it = items[t];
+        const int i = it / sp.max_chunks, c = it % sp.max_chunks;
+        if (i != cur) {
+            __syncthreads();  // the previous cell's tables are no longer read
+            const int* geqv = sp.eqv + (size_t)i * a.Wt;
+            const int ntop = sp.ntop[i];
+            if (a.pack_shift) {
+                for (int g = threadIdx.x; g < a.Wt; g += 256) eqv[g] = pack_e(geqv[g], a.pack_shift);
+            } else {
+                for (int g = threadIdx.x; g < a.Wt; g += 256) eqv[g] = geqv[g];
+            }
+            if (threadIdx.x == 0) {
+                eqv[a.Wt] = a.pack_shift ? 0 : SENT;
+                s_ntop = ntop;
+            }
+            for (int u = threadIdx.x; u <= ntop; u += 256) off[u] = sp.off[(size_t)i * 257 + u];
+            for (int u = threadIdx.x; u < ntop; u += 256) top[u] = sp.top[(size_t)i * 256 + u];
+            __syncthreads();
+            cur = i;
+        }
+        const int f = c * 256 + (int)threadIdx.x;
+        if (f < sp.total[i]) {
+            int dst;
+            const float v = row_score<SPLIT_SCAN_PF>(a, top, off, s_ntop, f, eqv, sp.nS[i], sp.kq[i], sp.nq[i],
+                                                     sp.rq[i], &dst);
+            sp.scores[(size_t)i * sp.max_rcand + dst] = v;
+        }
     }
 }
 
-// Per-label quantiles and the keep / drop rule per heavy cell.  grid = H.
-__global__ void __launch_bounds__(256) split_decide_kernel(FtPersistentArgs a, FtSplit sp) {
+// Per cell scanned this round: quantiles (from shared memory when the round's scores fit), the keep /
+// drop rule, then the setup of its next round (chunks appended to list q).  grid = H.
+__global__ void __launch_bounds__(256) split_decide_kernel(FtPersistentArgs a, FtSplit sp, int q) {
+    extern __shared__ __align__(16) unsigned char smem[];
     constexpr int NW = 8;
     __shared__ int hist[NW * 256];
     __shared__ float lsc[256];
     __shared__ int off[257];
     __shared__ uint8_t top[256], tmp[256];
     const int i = blockIdx.x;
-    if (sp.total[i] == 0) return;  // finished, or kept its first candidate this round
+    const int total = sp.total[i];
+    if (total == 0) return;  // finished
     const int ntop = sp.ntop[i];
     for (int t = threadIdx.x; t <= ntop; t += 256) off[t] = sp.off[(size_t)i * 257 + t];
     for (int t = threadIdx.x; t < ntop; t += 256) top[t] = sp.top[(size_t)i * 256 + t];
+    const float* scores = sp.scores + (size_t)i * sp.max_rcand;
+    if (total <= SPLIT_STAGE) {  // total is a multiple of 32 (label ranges are padded to 32 rows)
+        float4* st = reinterpret_cast<float4*>(smem);
+        const float4* src = reinterpret_cast<const float4*>(scores);
+        for (int t = threadIdx.x; t < total / 4; t += 256) st[t] = src[t];
+        scores = reinterpret_cast<const float*>(smem);
+    }
     __syncthreads();
-    cta_label_quantiles<NW>(a, top, off, ntop, sp.scores + (size_t)i * sp.max_rcand, lsc, hist,
-                            sp.nan_scratch + (size_t)i * NW * a.max_label);
+    cta_label_quantiles<NW>(a, top, off, ntop, scores, lsc, hist, sp.nan_scratch + (size_t)i * NW * a.max_label);
     if (threadIdx.x == 0) {
         const int n = decide_top(lsc, ntop, top, tmp, a.thre);
         for (int t = 0; t < n; ++t) sp.top[(size_t)i * 256 + t] = top[t];
         sp.ntop[i] = n;
     }
+    __syncthreads();
+    split_setup_round(a, sp, i, q, smem);
 }
 
 }  // namespace
@@ -680,23 +753,34 @@ size_t split_prepare_smem(int Wt, int capq) {
            sizeof(uint32_t) * capq + sizeof(int) * (512 + 16);
 }
 
+namespace {
+size_t split_decide_smem(int Wt, int capq) {
+    return std::max(split_prepare_smem(Wt, capq), sizeof(float) * SPLIT_STAGE);
+}
+size_t split_scan_smem(int Wt) { return sizeof(int) * (((Wt + 4) & ~3) + 260) + 256; }
+}  // namespace
+
 void split_round_setup(const FtPersistentArgs& a) {
-    const size_t sm1 = split_prepare_smem(a.Wt, a.capq);
-    SGR_CUDA(cudaFuncSetAttribute(split_prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-    const size_t sm2 = sizeof(int) * (((a.Wt + 4) & ~3) + 260) + 256;
-    SGR_CUDA(cudaFuncSetAttribute(split_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    SGR_CUDA(cudaFuncSetAttribute(split_first_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)split_prepare_smem(a.Wt, a.capq)));
+    SGR_CUDA(cudaFuncSetAttribute(split_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)split_scan_smem(a.Wt)));
+    SGR_CUDA(cudaFuncSetAttribute(split_decide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)split_decide_smem(a.Wt, a.capq)));
 }
 
-void launch_split_round(const FtPersistentArgs& a, const FtSplit& sp, int H, int max_chunks, cudaStream_t s) {
-    const size_t sm1 = split_prepare_smem(a.Wt, a.capq);
-    split_prepare_kernel<<<H, 256, sm1, s>>>(a, sp);
+void launch_split_first(const FtPersistentArgs& a, const FtSplit& sp, int H, cudaStream_t s) {
+    split_first_kernel<<<H, 256, split_prepare_smem(a.Wt, a.capq), s>>>(a, sp);
     SGR_LAUNCH_CHECK();
-    const size_t sm2 = sizeof(int) * (((a.Wt + 4) & ~3) + 260) + 256;
-    split_scan_kernel<<<dim3(max_chunks, H), 256, sm2, s>>>(a, sp);
+    count_launch(1);
+}
+
+void launch_split_round(const FtPersistentArgs& a, const FtSplit& sp, int H, int q, cudaStream_t s) {
+    split_scan_kernel<<<SPLIT_SCAN_CTAS * device_sm_count(), 256, split_scan_smem(a.Wt), s>>>(a, sp, q);
     SGR_LAUNCH_CHECK();
-    split_decide_kernel<<<H, 256, 0, s>>>(a, sp);
+    split_decide_kernel<<<H, 256, split_decide_smem(a.Wt, a.capq), s>>>(a, sp, q ^ 1);
     SGR_LAUNCH_CHECK();
-    count_launch(3);
+    count_launch(2);
 }
 
 void launch_ft_keys(int n, const int32_t* list, int L, const uint8_t* flags, const uint32_t* ctidx, int64_t* keys,

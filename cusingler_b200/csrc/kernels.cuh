@@ -243,12 +243,19 @@ struct FtSplit {
     float* nan_scratch;     // H x 8 x max_label
     int max_rcand;
     unsigned long long* rows_scored;  // device counter: reference rows scored, summed over rounds
+    int* items;             // 2 x max_items chunk lists (i * max_chunks + c)
+    int* n_items;           // 2 list lengths
+    int max_items;          // H * max_chunks
+    int max_chunks;         // 256-row chunks of the longest possible round
 };
 
-// Function attributes of the split-round kernels; call once before launch_split_round (and before
+// Function attributes of the split-round kernels; call once before launch_split_first (and before
 // capturing rounds into a CUDA graph).
 void split_round_setup(const FtPersistentArgs& a);
-void launch_split_round(const FtPersistentArgs& a, const FtSplit& sp, int H, int max_chunks, cudaStream_t s);
+// First round's setup of the H cells (chunk list 0; n_items must be zero).
+void launch_split_first(const FtPersistentArgs& a, const FtSplit& sp, int H, cudaStream_t s);
+// One round: scan of chunk list q, then the decisions and the next round's setup (list q ^ 1).
+void launch_split_round(const FtPersistentArgs& a, const FtSplit& sp, int H, int q, cudaStream_t s);
 
 size_t ft_persistent_smem(int Wt, int capq, int nw);
 void launch_ft_keys(int n, const int32_t* list, int L, const uint8_t* flags, const uint32_t* ctidx, int64_t* keys,

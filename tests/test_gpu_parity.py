@@ -110,6 +110,21 @@ def test_final_labels_both_row_scans(kind, packed):
     assert np.array_equal(rounds, res["rounds"])
 
 
+@pytest.mark.parametrize("kind", ["tiny", "families", "small"])
+@pytest.mark.parametrize("heavy", [2, 1 << 30])
+@pytest.mark.parametrize("times", [0, 2])
+def test_final_labels_spread_and_queue_paths(kind, heavy, times):
+    """Every cell on the spread path (rounds spread over the GPU, two launches per round) or every
+    cell on the work-queue kernel: the oracle's final labels and round counts either way."""
+    a, prob = annotator(kind, abi.MODE_EXACT)
+    a.set_tuning(1, heavy)
+    res = H.oracle_run(kind, 1, times)
+    final, rounds = a.finetune(prob.qry, res["flags"].astype(np.uint8), times=times)
+    a.set_tuning(1, 6)
+    assert np.array_equal(final, res["final"])
+    assert np.array_equal(rounds, res["rounds"])
+
+
 @pytest.mark.parametrize("kind", ["tiny", "small"])
 def test_fp16_variant_close_to_exact(kind):
     """The FP16-operand correlation variant (FP32 accumulation, not exact): every score within 1e-4
