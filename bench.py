@@ -473,7 +473,7 @@ def main():
             tuning["learned" if learned else "plain"] = {"pinned": True, "ft_warps": args.ft_warps,
                                                           "ft_heavy": args.ft_heavy, "score_chunk_mb": 1024,
                                                           "corr_pair": 0, "corr_gm": 1, "select_warps": 16,
-                                                          "pipeline": 0}
+                                                          "pipeline": 0, "corr_wide": 16}
             return
         tuning["learned" if learned else "plain"] = ann.autotune(
             tune_sample, learned=learned, min_confidence=args.min_confidence, check_fraction=args.check_fraction)
@@ -490,6 +490,7 @@ def main():
             ann.set_tuning(7, t["select_warps"])
             if mode == abi.MODE_EXACT:
                 ann.set_tuning(9, t["pipeline"])
+                ann.set_tuning(10, t["corr_wide"])
 
     def timed(fn, csr, steps, name):
         for _ in range(args.warmup):

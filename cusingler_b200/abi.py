@@ -63,7 +63,7 @@ class SgrTuning(C.Structure):
                 ("trials", C.c_int32), ("best_ms", C.c_double), ("worst_ms", C.c_double),
                 ("corr_pair", C.c_int32), ("corr_gm", C.c_int32), ("select_warps", C.c_int32),
                 ("score_trials", C.c_int32), ("score_best_ms", C.c_double), ("pipeline", C.c_int32),
-                ("pad", C.c_int32)]
+                ("corr_wide", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -158,6 +158,9 @@ struct sgr_ctx {
     DevBuf<uint32_t> ext_min, ext_max;  // per (query, label) score extremes of a score block
     DevBuf<RankItem> rank_overflow;  // rows ranked by the rank kernel's large-buffer tier
     DevBuf<int> rank_n_overflow;
+    int limb_w = 0;              // split of the exact limbs (split_limbs), chosen at training
+    int limb_base128 = 0;        // tuning: train with the base-128 split
+    int corr_wide = 16;          // tuning: 8 / 16 epilogue warps of the 128 x 256 form, 0 the 128 x 160 form
     int ft_warps = 8;            // warps per CTA of the persistent fine-tune (8 or 32)
     int ft_heavy = 6;            // candidates from which a cell takes the split path
     size_t score_chunk_bytes = (size_t)1 << 30;  // score-step correlation block (queries x reference)
@@ -528,6 +531,8 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     ctx->Wt = (uint32_t)mk.thre.size();
     ctx->markers_ready = true;
     if (ctx->G > 8128) fail(SGR_ERR_UNSUPPORTED, "more than 8128 score-step marker genes");
+    // the exact limbs' split: the two-accumulator split where it keeps every limb in int8
+    ctx->limb_w = ctx->limb_base128 ? 0 : pick_limb_w(ctx->G);
     if (ctx->Wt > 40000) fail(SGR_ERR_UNSUPPORTED, "fine-tune gene pool above 40000 genes");
     {
         const std::vector<int32_t> rmap = position_map(mk.ref_colmap, mk.common, mk.W);
@@ -549,7 +554,7 @@ void train(sgr_ctx* ctx, const sgr_csr* ref, const int32_t* celltypes, const cha
     ctx->ref_f32.ensure(ctx->R);
     DevCsr rm{ctx->ref_data.p, ctx->ref_indices.p, ctx->ref_indptr.p, ctx->R, ctx->ref_cols, (int64_t)indptr[ctx->R]};
     RankGroup g{ctx->ref_map_common.p, ctx->G, ctx->Kp, ctx->ref_limbs.p, ctx->ref_n2.p, ctx->ref_rinv.p,
-                ctx->ref_f32.p};
+                ctx->ref_f32.p, ctx->limb_w};
     rank_rows(ctx, rm, g, RANK_LIMBS, NORM_SEQ, ctx->ref_bits.p, ctx->ref_prefix.p);
     ctx->h_ref_n2.resize(ctx->R);
     SGR_CUDA(cudaMemcpyAsync(ctx->h_ref_n2.data(), ctx->ref_n2.p, ctx->R * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -678,11 +683,11 @@ void correlate(sgr_ctx* ctx, bool fp32, const int8_t* A, int nq, uint32_t q0, fl
     if (fp32 || exact_simt())
         launch_corr_simt(fp32, A, ctx->ref_limbs.p, nq, (int)ctx->R, ctx->G, ctx->Kp, ctx->q_f32.p + q0,
                          ctx->ref_f32.p, ctx->q_rinv.p + q0, ctx->ref_rinv.p, ctx->q_n2.p + q0, ctx->ref_n2.p, out,
-                         ld, ctx->stream);
+                         ld, ctx->limb_w, ctx->stream);
     else
         launch_corr_tc(A, ctx->ref_limbs.p, nq, (int)ctx->R, ctx->Kp, ctx->q_rinv.p + q0, ctx->ref_rinv.p,
                        ctx->q_n2.p + q0, ctx->ref_n2.p, out, ld, ctx->status.p, ctx->stream, false, ext,
-                       ctx->corr_pair != 0, ctx->corr_gm);
+                       ctx->corr_pair != 0, ctx->corr_gm, ctx->limb_w, ctx->corr_wide);
 }
 
 // A score step in progress: the query's rows are ranked and scored in blocks of `chunk` rows.
@@ -727,7 +732,7 @@ ScorePlan score_begin(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const 
         const size_t r0 = (size_t)c * pl.chunk;
         groups[c] = RankGroup{ctx->qry_map_common.p, ctx->G,          ctx->Kp,
                               ctx->q_limbs.p + r0 * row_bytes, ctx->q_n2.p + r0, ctx->q_rinv.p + r0,
-                              ctx->q_f32.p + r0};
+                              ctx->q_f32.p + r0, ctx->limb_w};
     }
     ctx->rank_groups.upload(groups, s);
     pl.rank_out = pl.f16 ? RANK_F16 : RANK_LIMBS;
@@ -1807,7 +1812,7 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
     };
     // every knob is restored if a candidate fails or changes a label
     const int keep_w = ctx->ft_warps, keep_h = ctx->ft_heavy, keep_pair = ctx->corr_pair, keep_gm = ctx->corr_gm,
-              keep_sw = ctx->select_warps, keep_pipe = ctx->pipeline;
+              keep_sw = ctx->select_warps, keep_pipe = ctx->pipeline, keep_wide = ctx->corr_wide;
     const size_t keep_c = ctx->score_chunk_bytes;
     auto restore = [&]() {
         ctx->ft_warps = keep_w;
@@ -1817,6 +1822,7 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
         ctx->corr_gm = keep_gm;
         ctx->select_warps = keep_sw;
         ctx->pipeline = keep_pipe;
+        ctx->corr_wide = keep_wide;
     };
     sgr_tuning best{};
     best.best_ms = 1e300;
@@ -1827,16 +1833,19 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
     fin0 = fin;
 
     // phase 1: score-step shapes (correlation form and tile order, score block, selection CTA width),
-    // each timed on the score step of the sample; first labels must not change
+    // each timed on the score step of the sample; first labels must not change.  Forms: 0 the
+    // 128 x 160 tiles, 1 their SM-pair form, 8 / 16 the 128 x 256 tiles with 8 / 16 epilogue warps.
     const bool exact = ctx->mode == SGR_MODE_EXACT;
-    const int pairs[] = {0, 1}, gms[] = {1, 16}, chunk_mb[] = {256, 1024}, sel_w[] = {0, 1, 16};
+    const int forms[] = {0, 1, 8, 16}, gms[] = {1, 16}, chunk_mb[] = {256, 1024}, sel_w[] = {0, 1, 16};
     double score_best = 1e300;
-    for (int pr : pairs)
+    for (int form : forms)
         for (int gm : gms) {
-            if (!exact && (pr || gm != 1)) continue;  // the FP32-order correlation runs on CUDA cores
+            if (!exact && (form || gm != 1)) continue;  // the FP32-order correlation runs on CUDA cores
+            if (form >= 8 && ctx->limb_w == 0) continue;  // the base-128 split has three accumulators
             for (int c : chunk_mb)
                 for (int w : sel_w) {
-                    ctx->corr_pair = pr;
+                    ctx->corr_pair = form == 1;
+                    ctx->corr_wide = form >= 8 ? form : 0;
                     ctx->corr_gm = gm;
                     ctx->score_chunk_bytes = (size_t)c << 20;
                     ctx->select_warps = w;
@@ -1853,7 +1862,8 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
                     best.score_trials++;
                     if (ms < score_best) {
                         score_best = ms;
-                        best.corr_pair = pr;
+                        best.corr_pair = form == 1;
+                        best.corr_wide = form >= 8 ? form : 0;
                         best.corr_gm = gm;
                         best.score_chunk_mb = c;
                         best.select_warps = w;
@@ -1861,6 +1871,7 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
                 }
         }
     ctx->corr_pair = best.corr_pair;
+    ctx->corr_wide = best.corr_wide;
     ctx->corr_gm = best.corr_gm;
     ctx->score_chunk_bytes = (size_t)best.score_chunk_mb << 20;
     ctx->select_warps = best.select_warps;
@@ -1955,6 +1966,16 @@ sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value) {
     if (what == 9) {
         if (value != 0 && value != 1) return SGR_ERR_INVALID_ARGUMENT;
         ctx->pipeline = value;
+        return SGR_OK;
+    }
+    if (what == 10) {
+        if (value != 0 && value != 8 && value != 16) return SGR_ERR_INVALID_ARGUMENT;
+        ctx->corr_wide = value;
+        return SGR_OK;
+    }
+    if (what == 11) {
+        if (value != 0 && value != 1) return SGR_ERR_INVALID_ARGUMENT;
+        ctx->limb_base128 = value;
         return SGR_OK;
     }
     return SGR_ERR_INVALID_ARGUMENT;
@@ -2097,7 +2118,8 @@ sgr_status sgr_debug_ranks(sgr_ctx* ctx, const sgr_csr* rows, int which, int32_t
             ctx->q_n2.ensure(n);
             ctx->q_rinv.ensure(n);
             ctx->q_f32.ensure(n);
-            RankGroup g{ctx->qry_map_common.p, G, Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p};
+            RankGroup g{ctx->qry_map_common.p, G, Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p,
+                        ctx->limb_w};
             rank_rows(ctx, q, g, RANK_LIMBS, NORM_NONE, ctx->qry_bits.p, ctx->qry_prefix.p);
             limbs.resize((size_t)n * 3 * Kp);
             SGR_CUDA(cudaMemcpyAsync(limbs.data(), ctx->q_limbs.p, limbs.size(), cudaMemcpyDeviceToHost, s));
@@ -2107,9 +2129,10 @@ sgr_status sgr_debug_ranks(sgr_ctx* ctx, const sgr_csr* rows, int which, int32_t
         for (uint32_t r = 0; r < n; ++r) {
             const int8_t* row = limbs.data() + (size_t)r * 3 * Kp;
             for (int i = 0; i < G; ++i) {
-                const int h = row[i], l = row[Kp + i], sm = row[2 * Kp + i];
-                if (sm != h + l) fail(SGR_ERR_STATE, "limb planes disagree");
-                d_out[(size_t)r * G + i] = 128 * h + l;
+                const int p0 = row[i], l = row[Kp + i], sm = row[2 * Kp + i], w = ctx->limb_w;
+                const int h = w ? p0 / w : p0;
+                if ((w && p0 != w * h) || sm != h + l) fail(SGR_ERR_STATE, "limb planes disagree");
+                d_out[(size_t)r * G + i] = limb_mult(w) * p0 + sm;
             }
         }
     });
@@ -2129,7 +2152,8 @@ sgr_status sgr_debug_scores(sgr_ctx* ctx, const sgr_csr* qry, float* out) {
         ctx->q_f32.ensure(Q);
         const bool f16 = ctx->corr_f16 && !fp32;
         if (f16) ensure_ref_f16(ctx);
-        RankGroup g{ctx->qry_map_common.p, ctx->G, ctx->Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p};
+        RankGroup g{ctx->qry_map_common.p, ctx->G, ctx->Kp, ctx->q_limbs.p, ctx->q_n2.p, ctx->q_rinv.p, ctx->q_f32.p,
+                    ctx->limb_w};
         rank_rows(ctx, q, g, f16 ? RANK_F16 : RANK_LIMBS, fp32 ? NORM_SEQ : NORM_NONE, ctx->qry_bits.p,
                   ctx->qry_prefix.p);
         DevBuf<float> sc;

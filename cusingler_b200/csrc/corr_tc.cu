@@ -43,6 +43,8 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdlib>
 #include <cstdint>
 
 #include "kernels.cuh"
@@ -305,7 +307,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     corr_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nq, int R,
                    int Kp, const double* __restrict__ rq, const double* __restrict__ rr,
                    const int64_t* __restrict__ nq2, const int64_t* __restrict__ nr2, float* __restrict__ out,
-                   int64_t ld, int* status, LabelExtremes ext, int gm) {
+                   int64_t ld, int* status, LabelExtremes ext, int gm, int k1, int cbase) {
     static_assert(!(F16 && PAIR), "the SM-pair form is exact only");
     constexpr int NST = PAIR ? PAIR_STAGES : STAGES;
     constexpr int SBYTES = PAIR ? PAIR_STAGE_BYTES : STAGE_BYTES;
@@ -532,7 +534,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                         tmem_ld16(lane_base + half * HALF + c * 16, pa);
                         tmem_wait_ld();
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) T[c][j] = 127 * (int)pa[j];
+                        for (int j = 0; j < 16; ++j) T[c][j] = k1 * (int)pa[j];
                     }
                     release(0);
                     got = acquire(1, par);
@@ -585,7 +587,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     const double N = F16 ? (double)__uint_as_float(p2[c & 1][j])
-                                         : (double)(128ll * T[c][j] - 127ll * (int)p2[c & 1][j]);
+                                         : (double)((int64_t)cbase * T[c][j] -
+                                                    (int64_t)(cbase - 1) * (int)p2[c & 1][j]);
                     const double rrj = __shfl_sync(0xffffffffu, rrv[c], j);
                     v[j] = (float)((N * rqv) * rrj);
                 }
@@ -667,6 +670,291 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
 }
 
+// ---- wide form: 128 x 256 tiles, two accumulators ----------------------------------------------
+//
+// With the split d = C h + l, C = w^2 + 1 (split_limbs with w > 0; planes P0 = w h, L = l, S = h + l):
+//     A1 = P0_q . P0_r + S_q . S_r,   A2 = L_q . L_r,   N = C A1 - (C - 1) A2   (exact in int64).
+// The two 256-column accumulators fill TMEM's 512 columns, so every tcgen05.mma has N = 256: the
+// time of one M = 128, K = 32 instruction measured the same at N = 128, 160 and 256, so this tile
+// gets the most products out of each.  Per tile the K loop multiplies the P0 and S planes into A1,
+// then the L plane into A2.  No second accumulator set fits, so the epilogue's walk over the tile
+// (TMEM loads one 16-column chunk ahead of the arithmetic) holds up the next tile's MMAs until its
+// last loads; EW epilogue warps (8 or 16: two or four per TMEM lane quadrant) shorten that walk.
+constexpr int WBN = 256;
+constexpr int WSTAGES = 4;
+constexpr int WSTAGE_BYTES = A_BYTES + WBN * BK;  // 48 KB, a multiple of 1024
+static_assert(WSTAGES <= MAX_STAGES, "barrier arrays");
+
+template <int EW>
+__global__ void __launch_bounds__(32 * (4 + EW), 1)
+    corr_wide_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nq, int R,
+                     int Kp, const double* __restrict__ rq, const double* __restrict__ rr, float* __restrict__ out,
+                     int64_t ld, int* status, LabelExtremes ext, int gm, int cbase) {
+    constexpr int QW = EW / 4;         // epilogue warps per TMEM lane quadrant
+    constexpr int WCOLS = WBN / QW;    // columns per epilogue warp
+    constexpr int WCH = WCOLS / 16;    // 16-column chunks per epilogue warp
+    static_assert(EW == 8 || EW == 16, "two or four epilogue warps per lane quadrant");
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ TcShared sh;
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tiles_n = (R + WBN - 1) / WBN, tiles_m = (nq + BM - 1) / BM;
+    const int n_tiles = tiles_m * tiles_n;
+    const int segb = Kp / BK, kblocks = 3 * segb;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < WSTAGES; ++s) {
+            mbar_init(smem_u32(&sh.full[s]), 1);
+            mbar_init(smem_u32(&sh.empty[s]), 1);
+        }
+        for (int g = 0; g < 2; ++g) {
+            mbar_init(smem_u32(&sh.acc_full[g]), 1);
+            mbar_init(smem_u32(&sh.acc_empty[g]), EW);
+        }
+        mbar_init(smem_u32(&sh.drain), 1);
+        sh.abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh.tmem_base)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sh.tmem_base;
+    volatile int* abort_flag = &sh.abort_flag;
+    auto give_up = [&]() {
+        atomicOr(status, SGR_TC_TIMEOUT);
+        sh.abort_flag = 1;
+    };
+
+    if (warp == 0) {
+        // ---- TMA producer ------------------------------------------------------------------
+        if (lane == 0) {
+            const uint64_t keep = policy_evict_last();  // the reference operand is read by every band
+            uint32_t it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+                int mb, nb;
+                tile_coords(t, tiles_m, tiles_n, gm, mb, nb);
+                const int m0 = mb * BM, n0 = nb * WBN;
+                for (int kb = 0; kb < kblocks; ++kb, ++it) {
+                    const int s = it % WSTAGES;
+                    const uint32_t ph = (it / WSTAGES) & 1;
+                    if (!mbar_wait(smem_u32(&sh.empty[s]), ph ^ 1, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t a_dst = smem_u32(smem + s * WSTAGE_BYTES);
+                    const uint32_t b_dst = a_dst + A_BYTES;
+                    // planes in the MMA's order: P0 and S (into A1), then L (into A2)
+                    const int grp = kb / segb, plane = grp == 0 ? 0 : (grp == 1 ? 2 : 1);
+                    const int kx = (plane * segb + kb % segb) * BK;
+                    const uint32_t fb = smem_u32(&sh.full[s]);
+                    mbar_expect_tx(fb, WSTAGE_BYTES);
+                    tma_load_2d(a_dst, &tmA, kx, m0, fb);
+                    tma_load_2d_hint(b_dst, &tmB, kx, n0, fb, keep);
+                }
+            }
+            if (!ok) give_up();
+            // drain: every issued stage's copies land before the CTA can exit
+            for (uint32_t j = (it > (uint32_t)WSTAGES ? it - WSTAGES : 0); j < it; ++j) {
+                const uint32_t s = j % WSTAGES, ph = (j / WSTAGES) & 1;
+                const long long t0 = clock64();
+                while (!mbar_try(smem_u32(&sh.full[s]), ph) && clock64() - t0 < WAIT_CYCLES) {
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer --------------------------------------------------------------------------
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_i8(BM, WBN);
+            uint32_t it = 0, tile_iter = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++tile_iter) {
+                for (int kb = 0; kb < kblocks; ++kb, ++it) {
+                    const int region = kb < 2 * segb ? 0 : 1;  // A1 (P0 and S planes), A2 (L plane)
+                    const bool first = kb == 0 || kb == 2 * segb;
+                    if (first) {
+                        if (!mbar_wait(smem_u32(&sh.acc_empty[region]), (tile_iter & 1) ^ 1, abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                    }
+                    const int s = it % WSTAGES;
+                    const uint32_t ph = (it / WSTAGES) & 1;
+                    if (!mbar_wait(smem_u32(&sh.full[s]), ph, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_addr = smem_u32(smem + s * WSTAGE_BYTES);
+                    const uint64_t da = smem_desc(a_addr), db = smem_desc(a_addr + A_BYTES);
+                    const uint32_t tc = tmem + region * WBN;
+#pragma unroll
+                    for (int k = 0; k < BK / 32; ++k)
+                        umma_i8(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc,
+                                (first && k == 0) ? 0u : 1u);
+                    umma_commit(smem_u32(&sh.empty[s]));
+                    if (kb == 2 * segb - 1) umma_commit(smem_u32(&sh.acc_full[0]));
+                    if (kb == kblocks - 1) umma_commit(smem_u32(&sh.acc_full[1]));
+                }
+            }
+            if (!ok) give_up();
+            umma_commit(smem_u32(&sh.drain));  // every MMA has finished before TMEM is freed
+        }
+        if (lane == 0) {
+            const long long t0 = clock64();
+            while (!mbar_try(smem_u32(&sh.drain), 0) && clock64() - t0 < WAIT_CYCLES) {
+            }
+        }
+    } else if (warp >= 4) {
+        // ---- epilogue ------------------------------------------------------------------------
+        // Lane = tile row 32 * quarter + lane; this warp scores columns [part * WCOLS, + WCOLS) in
+        // 16-column chunks, staged through its 32 x 16 buffer as in corr_tc_kernel.
+        const int ew = warp - 4, quarter = warp & 3, part = ew >> 2;
+        float4* chunk = reinterpret_cast<float4*>(smem + WSTAGES * WSTAGE_BYTES + ew * CHUNK_BYTES);
+        const bool vec_store = (ld % 4) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+        const int row = 32 * quarter + lane;
+        const int64_t c1 = cbase, c2 = cbase - 1;
+        auto release = [&](int g) {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh.acc_empty[g]));
+        };
+        uint32_t tile_iter = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++tile_iter) {
+            int mb, nb;
+            tile_coords(t, tiles_m, tiles_n, gm, mb, nb);
+            const int m0 = mb * BM, n0 = nb * WBN;
+            const int q = m0 + row;
+            const double rqv = q < nq ? rq[q] : 0.0;  // NaN when the query row is constant
+            double rrv[WCH];
+#pragma unroll
+            for (int c = 0; c < WCH; ++c) {
+                const int r = n0 + part * WCOLS + c * 16 + lane;
+                rrv[c] = (lane < 16 && r < R) ? rr[r] : 0.0;  // NaN for a constant reference row
+            }
+            int lab = 0, lab_end = 0;
+            float mnf = __int_as_float(0x7f800000), mxf = -__int_as_float(0x7f800000);
+            bool seen = false;
+            if (ext.kmin) {
+                const int cb = n0 + part * WCOLS;
+                int lo = 0, hi = ext.L - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (__ldg(ext.lstart + mid) <= cb) lo = mid;
+                    else hi = mid - 1;
+                }
+                lab = lo;
+                lab_end = __ldg(ext.lstart + lab + 1);
+            }
+            const uint32_t par = tile_iter & 1;
+            bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh.acc_full[0]), par, abort_flag));
+            if (got) got = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh.acc_full[1]), par, abort_flag));
+            if (!got) {
+                if (lane == 0) give_up();
+                break;
+            }
+            tc_fence_after();
+            const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
+            const uint32_t b1 = lane_base + part * WCOLS, b2 = lane_base + WBN + part * WCOLS;
+            uint32_t x1[2][16], x2[2][16];
+            tmem_ld16(b1, x1[0]);
+            tmem_ld16(b2, x2[0]);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < WCH; ++c) {
+                const int col0 = part * WCOLS + c * 16;
+                if (c + 1 < WCH) {
+                    tmem_ld16(b1 + 16 * (c + 1), x1[(c + 1) & 1]);
+                    tmem_ld16(b2 + 16 * (c + 1), x2[(c + 1) & 1]);
+                } else {
+                    release(0);  // every TMEM read of this warp has completed
+                    release(1);
+                }
+                float v[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const double N = (double)(c1 * (int)x1[c & 1][j] - c2 * (int)x2[c & 1][j]);
+                    const double rrj = __shfl_sync(0xffffffffu, rrv[c], j);
+                    v[j] = (float)((N * rqv) * rrj);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    chunk[lane * 4 + (u ^ ((lane >> 1) & 3))] =
+                        make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+                if (ext.kmin && n0 + col0 + 16 <= min(lab_end, R)) {  // the chunk lies in one label
+                    float a0 = fminf(fminf(v[0], v[1]), fminf(v[2], v[3]));
+                    float b0 = fmaxf(fmaxf(v[0], v[1]), fmaxf(v[2], v[3]));
+#pragma unroll
+                    for (int j = 4; j < 16; j += 4) {
+                        a0 = fminf(a0, fminf(fminf(v[j], v[j + 1]), fminf(v[j + 2], v[j + 3])));
+                        b0 = fmaxf(b0, fmaxf(fmaxf(v[j], v[j + 1]), fmaxf(v[j + 2], v[j + 3])));
+                    }
+                    mnf = fminf(mnf, a0);
+                    mxf = fmaxf(mxf, b0);
+                    seen = true;
+                } else if (ext.kmin) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int col = n0 + col0 + j;
+                        if (col >= R) break;
+                        if (col >= lab_end) {  // label boundary
+                            if (seen && q < nq) {
+                                atomicMin(ext.kmin + (size_t)q * ext.L + lab, ord_key(mnf));
+                                atomicMax(ext.kmax + (size_t)q * ext.L + lab, ord_key(mxf));
+                            }
+                            mnf = __int_as_float(0x7f800000);
+                            mxf = -__int_as_float(0x7f800000);
+                            do {
+                                ++lab;
+                                lab_end = __ldg(ext.lstart + lab + 1);
+                            } while (col >= lab_end);
+                        }
+                        mnf = fminf(mnf, v[j]);
+                        mxf = fmaxf(mxf, v[j]);
+                        seen = true;
+                    }
+                }
+                // the chunk's 32 rows x 16 columns: lane l stores piece l % 4 of row l / 4 (+ 8 i)
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = 8 * i + (lane >> 2), u = lane & 3;
+                    const int qq = m0 + 32 * quarter + r, col = n0 + col0 + 4 * u;
+                    const float4 val = chunk[r * 4 + (u ^ ((r >> 1) & 3))];
+                    if (qq >= nq || col >= R) continue;
+                    float* dst = out + (size_t)qq * ld + col;
+                    if (vec_store && col + 3 < R) {
+                        *reinterpret_cast<float4*>(dst) = val;
+                    } else {
+                        dst[0] = val.x;
+                        if (col + 1 < R) dst[1] = val.y;
+                        if (col + 2 < R) dst[2] = val.z;
+                        if (col + 3 < R) dst[3] = val.w;
+                    }
+                }
+                __syncwarp();  // the next chunk may overwrite the staging buffer
+                if (c + 1 < WCH) tmem_wait_ld();
+            }
+            if (ext.kmin && seen && q < nq) {
+                atomicMin(ext.kmin + (size_t)q * ext.L + lab, ord_key(mnf));
+                atomicMax(ext.kmax + (size_t)q * ext.L + lab, ord_key(mxf));
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -704,14 +992,45 @@ size_t corr_tc_smem(bool pair) {
                 : (size_t)STAGES * STAGE_BYTES + STAGING_BYTES + 1024;
 }
 
+size_t corr_wide_smem(int ew) { return (size_t)WSTAGES * WSTAGE_BYTES + (size_t)ew * CHUNK_BYTES + 1024; }
+
+int pick_limb_w(int G) {
+    const int D = std::max(G - 1, 0);
+    for (int w = 1; w <= 15; ++w) {
+        const int C = w * w + 1, hc = C / 2;
+        bool ok = true;
+        for (int d = -D; d <= D && ok; ++d) {
+            const int h = (int)std::floor((double)(d + hc) / C), l = d - C * h, s = h + l;
+            ok = std::abs(w * h) <= 127 && s >= -128 && s <= 127 && l >= -128 && l <= 127;
+        }
+        if (ok) return w;
+    }
+    return 0;
+}
+
 void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
                     const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s,
-                    bool f16, LabelExtremes ext, bool pair, int gm) {
+                    bool f16, LabelExtremes ext, bool pair, int gm, int limb_w, int wide_warps) {
     if (nq <= 0 || R <= 0) return;
     if (Kp % BK != 0 || (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15))
         fail(SGR_ERR_INVALID_ARGUMENT, "tensor-core correlation: misaligned operands");
     pair = pair && !f16;
     gm = std::max(gm, 1);
+    // recombination of the planes' products for the split the limbs were written with
+    const int k1 = limb_w ? 1 : 127, cbase = limb_w ? limb_w * limb_w + 1 : 128;
+    if (!f16 && !pair && limb_w > 0 && (wide_warps == 8 || wide_warps == 16)) {
+        const CUtensorMap ta = limb_map(A, nq, 3 * Kp, BM), tb = limb_map(B, R, 3 * Kp, WBN);
+        const size_t smem = corr_wide_smem(wide_warps);
+        const long tiles = (long)((nq + BM - 1) / BM) * ((R + WBN - 1) / WBN);
+        const int grid = (int)std::min<long>(tiles, device_sm_count());
+        auto kern = wide_warps == 16 ? corr_wide_kernel<16> : corr_wide_kernel<8>;
+        SGR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, 32 * (4 + wide_warps), smem, s>>>(ta, tb, nq, R, Kp, ra, rb, scores, ld, status, ext, gm,
+                                                        cbase);
+        SGR_LAUNCH_CHECK();
+        count_launch();
+        return;
+    }
     const int row_bytes = (f16 ? 2 : 3) * Kp;
     const CUtensorMap ta = limb_map(A, nq, row_bytes, BM), tb = limb_map(B, R, row_bytes, pair ? BN / 2 : BN);
     const size_t smem = corr_tc_smem(pair);
@@ -721,7 +1040,7 @@ void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, con
         auto kern = f16 ? corr_tc_kernel<true, false> : corr_tc_kernel<false, false>;
         SGR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const int grid = (int)std::min<long>(tiles, device_sm_count());
-        kern<<<grid, THREADS, smem, s>>>(ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status, ext, gm);
+        kern<<<grid, THREADS, smem, s>>>(ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status, ext, gm, k1, cbase);
         SGR_LAUNCH_CHECK();
         count_launch();
         return;
@@ -747,7 +1066,7 @@ void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, con
         max_pairs = std::max(1, device_sm_count() / 2);
     }
     cfg.gridDim = dim3(2 * (unsigned)std::min<long>(tiles, max_pairs));
-    SGR_CUDA(cudaLaunchKernelEx(&cfg, kern, ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status, ext, gm));
+    SGR_CUDA(cudaLaunchKernelEx(&cfg, kern, ta, tb, nq, R, Kp, ra, rb, na, nb, scores, ld, status, ext, gm, k1, cbase));
     count_launch();
 }
 

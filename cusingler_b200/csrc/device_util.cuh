@@ -30,11 +30,25 @@ __device__ __forceinline__ float canon_zero(float v) {
 }
 
 // d = 128*h + l with l in [-64, 63]; s = h + l (the Karatsuba limb).
-__device__ __forceinline__ void split_limbs(int d, int& h, int& l, int& s) {
-    l = ((d + 64) & 127) - 64;
-    h = (d - l) >> 7;
+// Int8 limbs of a doubled centred rank d, written as planes (p0, l, s), with d = m * p0 + s:
+//   w = 0: d = 128 h + l, l in [-64, 63], p0 = h, s = h + l (m = 127);
+//   w > 0: d = C h + l with C = w^2 + 1, l in [-C/2, C - 1 - C/2], p0 = w h, s = h + l (m = w).
+// The second split lets the exact product use two accumulators: d d' = C (p0 p0' + s s') - (C-1) l l'.
+// The host picks w so that every limb of |d| < G fits int8.
+__device__ __forceinline__ void split_limbs(int d, int w, int& p0, int& l, int& s) {
+    if (w == 0) {
+        l = ((d + 64) & 127) - 64;
+        p0 = (d - l) >> 7;
+        s = p0 + l;
+        return;
+    }
+    const int C = w * w + 1, hc = C >> 1;
+    const int h = (d + hc + 4096 * C) / C - 4096;  // floor((d + hc) / C) for |d| < 4096 C
+    l = d - C * h;
     s = h + l;
+    p0 = w * h;
 }
+
 
 __device__ __forceinline__ int64_t warp_sum_i64(int64_t v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);

@@ -29,19 +29,19 @@
 namespace sgr {
 namespace {
 
-__device__ __forceinline__ int stage_d(const unsigned char* stage, int mode, int Kp, int p) {
+__device__ __forceinline__ int stage_d(const unsigned char* stage, int mode, int Kp, int p, int w) {
     if (mode == RANK_LIMBS) {
         const int8_t* s = reinterpret_cast<const int8_t*>(stage);
-        return 128 * (int)s[p] + (int)s[Kp + p];
+        return limb_mult(w) * (int)s[p] + (int)s[2 * Kp + p];
     }
     if (mode == RANK_F16) return __half2int_rn(reinterpret_cast<const __half*>(stage)[p]);
     return reinterpret_cast<const int16_t*>(stage)[p];
 }
 
-__device__ __forceinline__ void stage_put(unsigned char* stage, int mode, int Kp, int p, int d) {
+__device__ __forceinline__ void stage_put(unsigned char* stage, int mode, int Kp, int p, int d, int w) {
     if (mode == RANK_LIMBS) {
         int h, l, s;
-        split_limbs(d, h, l, s);
+        split_limbs(d, w, h, l, s);
         int8_t* st = reinterpret_cast<int8_t*>(stage);
         st[p] = (int8_t)h;
         st[Kp + p] = (int8_t)l;
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
         const int d0 = -k;
         if (a.out_mode == RANK_LIMBS) {
             int h0, l0, s0;
-            split_limbs(d0, h0, l0, s0);
+            split_limbs(d0, g.limb_w, h0, l0, s0);
             uint32_t* st = reinterpret_cast<uint32_t*>(stage);
             const int wpp = Kp / 4;  // words per plane (Kp is a multiple of 16)
 #pragma unroll
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
                     eq += u == hv;
                 }
                 const int d = G - 2 * k + 2 * less + eq;
-                stage_put(stage, a.out_mode, Kp, (int)(uint32_t)key, d);
+                stage_put(stage, a.out_mode, Kp, (int)(uint32_t)key, d, g.limb_w);
                 sq += (int64_t)d * d;
             }
         } else {
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
                     eq += w == v;
                 }
                 const int d = G - 2 * k + 2 * less + eq;
-                stage_put(stage, a.out_mode, Kp, pos, d);
+                stage_put(stage, a.out_mode, Kp, pos, d, g.limb_w);
                 sq += (int64_t)d * d;
             }
         }
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
             if (lane == 0) {
                 float acc = 0.f;
                 for (int p = 0; p < G; ++p) {
-                    const float x = stage_d(stage, a.out_mode, Kp, p) * 0.5f;
+                    const float x = stage_d(stage, a.out_mode, Kp, p, g.limb_w) * 0.5f;
                     acc = fmaf(x, x, acc);
                 }
                 g.f32norm[it.slot] = acc;
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
                 const int ch = 4 * lane + t;
                 float acc = 0.f;
                 for (int p = ch * step; p < (ch + 1) * step && p < G; ++p) {
-                    const float x = stage_d(stage, a.out_mode, Kp, p) * 0.5f;
+                    const float x = stage_d(stage, a.out_mode, Kp, p, g.limb_w) * 0.5f;
                     acc = fmaf(x, x, acc);
                 }
                 c[t] = acc;
@@ -407,7 +407,7 @@ template <bool FP32>
 __global__ void __launch_bounds__(256) corr_simt_kernel(const int8_t* A, const int8_t* B, int nq, int R, int G,
                                                         int Kp, const float* fa, const float* fb, const double* ra,
                                                         const double* rb, const int64_t* na, const int64_t* nb,
-                                                        float* out, int64_t ld) {
+                                                        float* out, int64_t ld, int m) {
     using T = typename std::conditional<FP32, float, double>::type;
     __shared__ T As[8][132];
     __shared__ T Bs[8][132];
@@ -427,11 +427,11 @@ __global__ void __launch_bounds__(256) corr_simt_kernel(const int8_t* A, const i
             if (q < nq) {
                 const int8_t* row = A + (size_t)q * 3 * Kp;
                 h4 = *reinterpret_cast<const uint32_t*>(row + k0 + lk);
-                l4 = *reinterpret_cast<const uint32_t*>(row + Kp + k0 + lk);
+                l4 = *reinterpret_cast<const uint32_t*>(row + 2 * Kp + k0 + lk);  // the S plane
             }
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
-                const int d = 128 * (int)(int8_t)(h4 >> (8 * b)) + (int)(int8_t)(l4 >> (8 * b));
+                const int d = m * (int)(int8_t)(h4 >> (8 * b)) + (int)(int8_t)(l4 >> (8 * b));
                 As[lk + b][lr] = FP32 ? T(d * 0.5f) : T(d);
             }
         }
@@ -441,11 +441,11 @@ __global__ void __launch_bounds__(256) corr_simt_kernel(const int8_t* A, const i
             if (r < R) {
                 const int8_t* row = B + (size_t)r * 3 * Kp;
                 h4 = *reinterpret_cast<const uint32_t*>(row + k0 + lk);
-                l4 = *reinterpret_cast<const uint32_t*>(row + Kp + k0 + lk);
+                l4 = *reinterpret_cast<const uint32_t*>(row + 2 * Kp + k0 + lk);  // the S plane
             }
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
-                const int d = 128 * (int)(int8_t)(h4 >> (8 * b)) + (int)(int8_t)(l4 >> (8 * b));
+                const int d = m * (int)(int8_t)(h4 >> (8 * b)) + (int)(int8_t)(l4 >> (8 * b));
                 Bs[lk + b][lr] = FP32 ? T(d * 0.5f) : T(d);
             }
         }
@@ -906,13 +906,14 @@ void launch_filter_fill(const float* data, const int32_t* indptr, const int32_t*
 
 void launch_corr_simt(bool fp32ref, const int8_t* A, const int8_t* B, int nq, int R, int G, int Kp, const float* fa,
                       const float* fb, const double* ra, const double* rb, const int64_t* na, const int64_t* nb,
-                      float* scores, int64_t ld, cudaStream_t s) {
+                      float* scores, int64_t ld, int limb_w, cudaStream_t s) {
     if (nq <= 0 || R <= 0) return;
     dim3 grid((R + 127) / 128, (nq + 127) / 128);
+    const int m = limb_mult(limb_w);
     if (fp32ref)
-        corr_simt_kernel<true><<<grid, 256, 0, s>>>(A, B, nq, R, G, Kp, fa, fb, ra, rb, na, nb, scores, ld);
+        corr_simt_kernel<true><<<grid, 256, 0, s>>>(A, B, nq, R, G, Kp, fa, fb, ra, rb, na, nb, scores, ld, m);
     else
-        corr_simt_kernel<false><<<grid, 256, 0, s>>>(A, B, nq, R, G, Kp, fa, fb, ra, rb, na, nb, scores, ld);
+        corr_simt_kernel<false><<<grid, 256, 0, s>>>(A, B, nq, R, G, Kp, fa, fb, ra, rb, na, nb, scores, ld, m);
     SGR_LAUNCH_CHECK();
     count_launch();
 }

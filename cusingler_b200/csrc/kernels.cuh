@@ -32,10 +32,11 @@ struct RankGroup {
     const int32_t* colmap;  // input column -> position, -1 if not in the subset
     int32_t G;
     int32_t Kp;
-    void* out;              // LIMBS: int8 [rows][3*Kp] planes H|L|S; D16: int16 [rows][Kp]
+    void* out;              // LIMBS: int8 [rows][3*Kp] planes p0|L|S (split_limbs); D16: int16 [rows][Kp]
     int64_t* n2;            // per row: sum of d^2 (exact)
     double* rinv;           // per row: 1/sqrt(n2), NaN when n2 == 0
     float* f32norm;         // per row, fp32 reference-order sum of x^2 (x = d/2), or nullptr
+    int32_t limb_w = 0;     // LIMBS: the split of split_limbs (0: base 128)
 };
 
 struct RankItem {
@@ -108,7 +109,7 @@ void launch_filter_fill(const float* data, const int32_t* indptr, const int32_t*
 // exact:   FP64 accumulation of the integer products (exact), FP64 normalisation.
 void launch_corr_simt(bool fp32ref, const int8_t* A, const int8_t* B, int nq, int R, int G, int Kp,
                       const float* fa, const float* fb, const double* ra, const double* rb,
-                      const int64_t* na, const int64_t* nb, float* scores, int64_t ld, cudaStream_t s);
+                      const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int limb_w, cudaStream_t s);
 
 // ---- per-label quantile, argmax, candidate flags ------------------------------------------------
 struct LabelQ {
@@ -188,9 +189,18 @@ struct LabelExtremes {
 
 // gm: row bands per group of the tile order (the bands of a group sweep the reference tiles together,
 // so the CTAs at work share them through L2); 1 visits band after band.
+// limb_w: the split of the exact limbs (split_limbs; 0 = base 128).  wide_warps 8 or 16 (with
+// limb_w > 0, not f16 or pair) runs the 128 x 256-tile two-accumulator form with that many epilogue
+// warps; 0 the 128 x 160 three-accumulator form.
 void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
                     const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s,
-                    bool f16 = false, LabelExtremes ext = LabelExtremes{}, bool pair = false, int gm = 1);
+                    bool f16 = false, LabelExtremes ext = LabelExtremes{}, bool pair = false, int gm = 1,
+                    int limb_w = 0, int wide_warps = 0);
+// Multiplier m of the limbs' reconstruction d = m * p0 + s (split_limbs with w; 0 = base 128).
+__host__ __device__ inline int limb_mult(int w) { return w == 0 ? 127 : w; }
+// Smallest w whose split (split_limbs) keeps every limb of |d| <= G - 1 in int8; 0 if none does.
+int pick_limb_w(int G);
+size_t corr_wide_smem(int ew);
 
 // Persistent exact fine-tune (finetune.cu).
 struct FtPersistentArgs {

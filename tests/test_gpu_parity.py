@@ -17,16 +17,19 @@ pytestmark = pytest.mark.gpu
 KINDS = ["tiny", "families", "small"]
 
 
-def annotator(kind, mode):
+def annotator(kind, mode, base128=0):
     prob = H.problem(kind)
     a = abi.Annotator(gpuid=0, cores=8, mode=mode)
+    a.set_tuning(11, base128)  # the limbs' split: two-accumulator (default) or base 128
     a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
     return a, prob
 
 
 @pytest.mark.parametrize("kind", KINDS)
-def test_ranks_bit_exact(kind):
-    a, prob = annotator(kind, abi.MODE_EXACT)
+@pytest.mark.parametrize("base128", [0, 1])
+def test_ranks_bit_exact(kind, base128):
+    """Ranks reconstructed from the int8 limbs equal the oracle's, for either split of the limbs."""
+    a, prob = annotator(kind, abi.MODE_EXACT, base128)
     res = H.oracle_run(kind, 1)
     orc = res["oracle"]
     d_ref = a.debug_ranks()
@@ -38,8 +41,9 @@ def test_ranks_bit_exact(kind):
 
 
 @pytest.mark.parametrize("kind", KINDS)
-def test_scores_fp32ref_bit_exact(kind):
-    a, prob = annotator(kind, abi.MODE_FP32REF)
+@pytest.mark.parametrize("base128", [0, 1])
+def test_scores_fp32ref_bit_exact(kind, base128):
+    a, prob = annotator(kind, abi.MODE_FP32REF, base128)
     raw = a.debug_scores(prob.qry)
     ref = H.oracle_run(kind, 0)["raw"]
     assert H.ulp_diff(raw, ref).max() == 0
@@ -146,14 +150,18 @@ def test_fp16_variant_close_to_exact(kind):
 
 
 @pytest.mark.parametrize("kind", ["tiny", "small"])
-@pytest.mark.parametrize("pair,gm", [(0, 8), (1, 1), (1, 8)])
-def test_correlation_forms_bit_exact(kind, pair, gm):
-    """Both tensor-core forms of the exact correlation -- one CTA per 128-row tile, or a cluster of two
-    CTAs per 256-row tile (tcgen05 cta_group::2) -- in band-by-band or grouped tile order give the
-    oracle's exact scores bit for bit, and the oracle's labels (query and reference counts that are
-    not multiples of the tile sizes included)."""
-    a, prob = annotator(kind, abi.MODE_EXACT)
+@pytest.mark.parametrize("base128,pair,wide,gm", [(0, 0, 16, 1), (0, 0, 16, 8), (0, 0, 8, 1), (0, 0, 0, 1),
+                                                  (0, 1, 0, 8), (1, 0, 0, 8), (1, 1, 0, 1), (1, 0, 16, 1)])
+def test_correlation_forms_bit_exact(kind, base128, pair, wide, gm):
+    """Every tensor-core form of the exact correlation gives the oracle's exact scores bit for bit, and
+    the oracle's labels (query and reference counts that are not multiples of the tile sizes
+    included): 128 x 256 tiles with two accumulators (8 or 16 epilogue warps), 128 x 160 tiles with
+    three, and their SM-pair form (tcgen05 cta_group::2), on either split of the limbs (the base-128
+    split has no two-accumulator form and takes the 128 x 160 tiles), in band-by-band or grouped tile
+    order."""
+    a, prob = annotator(kind, abi.MODE_EXACT, base128)
     a.set_tuning(5, pair)
+    a.set_tuning(10, wide)
     a.set_tuning(6, gm)
     raw = a.debug_scores(prob.qry)
     res = H.oracle_run(kind, 1)
