@@ -473,7 +473,7 @@ def main():
             tuning["learned" if learned else "plain"] = {"pinned": True, "ft_warps": args.ft_warps,
                                                           "ft_heavy": args.ft_heavy, "score_chunk_mb": 1024,
                                                           "corr_pair": 0, "corr_gm": 1, "select_warps": 16,
-                                                          "pipeline": 0, "corr_wide": 16}
+                                                          "pipeline": 0, "corr_wide": 18}
             return
         tuning["learned" if learned else "plain"] = ann.autotune(
             tune_sample, learned=learned, min_confidence=args.min_confidence, check_fraction=args.check_fraction)

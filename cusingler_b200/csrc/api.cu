@@ -160,7 +160,7 @@ struct sgr_ctx {
     DevBuf<int> rank_n_overflow;
     int limb_w = 0;              // split of the exact limbs (split_limbs), chosen at training
     int limb_base128 = 0;        // tuning: train with the base-128 split
-    int corr_wide = 16;          // tuning: 8 / 16 epilogue warps of the 128 x 256 form, 0 the 128 x 160 form
+    int corr_wide = 18;          // tuning: 128 x 256 form (8 / 16 epilogue warps, 18 overlapped), 0 128 x 160
     int ft_warps = 8;            // warps per CTA of the persistent fine-tune (8 or 32)
     int ft_heavy = 6;            // candidates from which a cell takes the split path
     size_t score_chunk_bytes = (size_t)1 << 30;  // score-step correlation block (queries x reference)
@@ -1834,9 +1834,10 @@ sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, flo
 
     // phase 1: score-step shapes (correlation form and tile order, score block, selection CTA width),
     // each timed on the score step of the sample; first labels must not change.  Forms: 0 the
-    // 128 x 160 tiles, 1 their SM-pair form, 8 / 16 the 128 x 256 tiles with 8 / 16 epilogue warps.
+    // 128 x 160 tiles, 1 their SM-pair form, 8 / 16 the 128 x 256 tiles with 8 / 16 epilogue warps,
+    // 18 their overlapped form.
     const bool exact = ctx->mode == SGR_MODE_EXACT;
-    const int forms[] = {0, 1, 8, 16}, gms[] = {1, 16}, chunk_mb[] = {256, 1024}, sel_w[] = {0, 1, 16};
+    const int forms[] = {0, 1, 8, 16, 18}, gms[] = {1, 16}, chunk_mb[] = {256, 1024}, sel_w[] = {0, 1, 16};
     double score_best = 1e300;
     for (int form : forms)
         for (int gm : gms) {
@@ -1969,7 +1970,7 @@ sgr_status sgr_set_tuning(sgr_ctx* ctx, int what, int value) {
         return SGR_OK;
     }
     if (what == 10) {
-        if (value != 0 && value != 8 && value != 16) return SGR_ERR_INVALID_ARGUMENT;
+        if (value != 0 && value != 8 && value != 16 && value != 18) return SGR_ERR_INVALID_ARGUMENT;
         ctx->corr_wide = value;
         return SGR_OK;
     }

@@ -955,6 +955,272 @@ __global__ void __launch_bounds__(32 * (4 + EW), 1)
     }
 }
 
+// Overlapped wide form: the 16 epilogue warps are warps 0-15 (warp % 4 is the TMEM lane quadrant
+// again), the TMA producer warp 16 and the MMA warp 17 (registers are allocated per four warps, so
+// the CTA's 18 warps leave 96 registers per thread).  Each epilogue warp takes its 64 columns of A1
+// into registers as soon as A1 is complete (while the MMA multiplies the L plane into A2) and
+// releases A1 at once, so the next tile's P0 and S
+// planes are multiplied while the warp walks A2 and stores the scores; A2 is released when its last
+// chunk has been read, well before the next tile's L plane.
+constexpr int HOLD_THREADS = 32 * 18;
+
+__global__ void __launch_bounds__(HOLD_THREADS, 1)
+    corr_wide_hold_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nq,
+                          int R, int Kp, const double* __restrict__ rq, const double* __restrict__ rr,
+                          float* __restrict__ out, int64_t ld, int* status, LabelExtremes ext, int gm, int cbase) {
+    constexpr int EW = 16, WCOLS = 64, WCH = 4;
+    constexpr int PRODUCER = 16, ISSUER = 17;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ TcShared sh;
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tiles_n = (R + WBN - 1) / WBN, tiles_m = (nq + BM - 1) / BM;
+    const int n_tiles = tiles_m * tiles_n;
+    const int segb = Kp / BK, kblocks = 3 * segb;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < WSTAGES; ++s) {
+            mbar_init(smem_u32(&sh.full[s]), 1);
+            mbar_init(smem_u32(&sh.empty[s]), 1);
+        }
+        for (int g = 0; g < 2; ++g) {
+            mbar_init(smem_u32(&sh.acc_full[g]), 1);
+            mbar_init(smem_u32(&sh.acc_empty[g]), EW);
+        }
+        mbar_init(smem_u32(&sh.drain), 1);
+        sh.abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == ISSUER) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh.tmem_base)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sh.tmem_base;
+    volatile int* abort_flag = &sh.abort_flag;
+    auto give_up = [&]() {
+        atomicOr(status, SGR_TC_TIMEOUT);
+        sh.abort_flag = 1;
+    };
+
+    if (warp == PRODUCER) {
+        if (lane == 0) {
+            const uint64_t keep = policy_evict_last();  // the reference operand is read by every band
+            uint32_t it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+                int mb, nb;
+                tile_coords(t, tiles_m, tiles_n, gm, mb, nb);
+                const int m0 = mb * BM, n0 = nb * WBN;
+                for (int kb = 0; kb < kblocks; ++kb, ++it) {
+                    const int s = it % WSTAGES;
+                    const uint32_t ph = (it / WSTAGES) & 1;
+                    if (!mbar_wait(smem_u32(&sh.empty[s]), ph ^ 1, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t a_dst = smem_u32(smem + s * WSTAGE_BYTES);
+                    const uint32_t b_dst = a_dst + A_BYTES;
+                    const int grp = kb / segb, plane = grp == 0 ? 0 : (grp == 1 ? 2 : 1);  // P0, S, L
+                    const int kx = (plane * segb + kb % segb) * BK;
+                    const uint32_t fb = smem_u32(&sh.full[s]);
+                    mbar_expect_tx(fb, WSTAGE_BYTES);
+                    tma_load_2d(a_dst, &tmA, kx, m0, fb);
+                    tma_load_2d_hint(b_dst, &tmB, kx, n0, fb, keep);
+                }
+            }
+            if (!ok) give_up();
+            for (uint32_t j = (it > (uint32_t)WSTAGES ? it - WSTAGES : 0); j < it; ++j) {
+                const uint32_t s = j % WSTAGES, ph = (j / WSTAGES) & 1;
+                const long long t0 = clock64();
+                while (!mbar_try(smem_u32(&sh.full[s]), ph) && clock64() - t0 < WAIT_CYCLES) {
+                }
+            }
+        }
+    } else if (warp == ISSUER) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_i8(BM, WBN);
+            uint32_t it = 0, tile_iter = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++tile_iter) {
+                for (int kb = 0; kb < kblocks; ++kb, ++it) {
+                    const int region = kb < 2 * segb ? 0 : 1;  // A1 (P0 and S planes), A2 (L plane)
+                    const bool first = kb == 0 || kb == 2 * segb;
+                    if (first) {
+                        if (!mbar_wait(smem_u32(&sh.acc_empty[region]), (tile_iter & 1) ^ 1, abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                    }
+                    const int s = it % WSTAGES;
+                    const uint32_t ph = (it / WSTAGES) & 1;
+                    if (!mbar_wait(smem_u32(&sh.full[s]), ph, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_addr = smem_u32(smem + s * WSTAGE_BYTES);
+                    const uint64_t da = smem_desc(a_addr), db = smem_desc(a_addr + A_BYTES);
+                    const uint32_t tc = tmem + region * WBN;
+#pragma unroll
+                    for (int k = 0; k < BK / 32; ++k)
+                        umma_i8(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc,
+                                (first && k == 0) ? 0u : 1u);
+                    umma_commit(smem_u32(&sh.empty[s]));
+                    if (kb == 2 * segb - 1) umma_commit(smem_u32(&sh.acc_full[0]));
+                    if (kb == kblocks - 1) umma_commit(smem_u32(&sh.acc_full[1]));
+                }
+            }
+            if (!ok) give_up();
+            umma_commit(smem_u32(&sh.drain));  // every MMA has finished before TMEM is freed
+        }
+        if (lane == 0) {
+            const long long t0 = clock64();
+            while (!mbar_try(smem_u32(&sh.drain), 0) && clock64() - t0 < WAIT_CYCLES) {
+            }
+        }
+    } else {
+        // ---- epilogue: warps 0-15 --------------------------------------------------------------
+        const int quarter = warp & 3, part = warp >> 2;
+        float4* chunk = reinterpret_cast<float4*>(smem + WSTAGES * WSTAGE_BYTES + warp * CHUNK_BYTES);
+        const bool vec_store = (ld % 4) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+        const int row = 32 * quarter + lane;
+        const int64_t c1 = cbase, c2 = cbase - 1;
+        auto release = [&](int g) {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh.acc_empty[g]));
+        };
+        const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
+        const uint32_t b1 = lane_base + part * WCOLS, b2 = lane_base + WBN + part * WCOLS;
+        uint32_t tile_iter = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++tile_iter) {
+            int mb, nb;
+            tile_coords(t, tiles_m, tiles_n, gm, mb, nb);
+            const int m0 = mb * BM, n0 = nb * WBN;
+            const int q = m0 + row;
+            const uint32_t par = tile_iter & 1;
+            // A1: all 64 columns into registers, then release it for the next tile's first planes
+            if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&sh.acc_full[0]), par, abort_flag))) {
+                if (lane == 0) give_up();
+                break;
+            }
+            tc_fence_after();
+            uint32_t a1[WCH][16];
+#pragma unroll
+            for (int c = 0; c < WCH; ++c) tmem_ld16(b1 + 16 * c, a1[c]);
+            tmem_wait_ld();
+            release(0);
+            const double rqv = q < nq ? rq[q] : 0.0;  // NaN when the query row is constant
+            int lab = 0, lab_end = 0;
+            float mnf = __int_as_float(0x7f800000), mxf = -__int_as_float(0x7f800000);
+            bool seen = false;
+            if (ext.kmin) {
+                const int cb = n0 + part * WCOLS;
+                int lo = 0, hi = ext.L - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (__ldg(ext.lstart + mid) <= cb) lo = mid;
+                    else hi = mid - 1;
+                }
+                lab = lo;
+                lab_end = __ldg(ext.lstart + lab + 1);
+            }
+            if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&sh.acc_full[1]), par, abort_flag))) {
+                if (lane == 0) give_up();
+                break;
+            }
+            tc_fence_after();
+#pragma unroll
+            for (int c = 0; c < WCH; ++c) {
+                const int col0 = part * WCOLS + c * 16;
+                const int rcol = n0 + col0 + lane;
+                const double rrl = (lane < 16 && rcol < R) ? rr[rcol] : 0.0;  // NaN for a constant reference row
+                uint32_t x2[16];
+                tmem_ld16(b2 + 16 * c, x2);
+                tmem_wait_ld();
+                if (c + 1 == WCH) release(1);  // every TMEM read of this warp has completed
+                float v[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const double N = (double)(c1 * (int)a1[c][j] - c2 * (int)x2[j]);
+                    const double rrj = __shfl_sync(0xffffffffu, rrl, j);
+                    v[j] = (float)((N * rqv) * rrj);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    chunk[lane * 4 + (u ^ ((lane >> 1) & 3))] =
+                        make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+                if (ext.kmin && n0 + col0 + 16 <= min(lab_end, R)) {  // the chunk lies in one label
+                    float a0 = fminf(fminf(v[0], v[1]), fminf(v[2], v[3]));
+                    float b0 = fmaxf(fmaxf(v[0], v[1]), fmaxf(v[2], v[3]));
+#pragma unroll
+                    for (int j = 4; j < 16; j += 4) {
+                        a0 = fminf(a0, fminf(fminf(v[j], v[j + 1]), fminf(v[j + 2], v[j + 3])));
+                        b0 = fmaxf(b0, fmaxf(fmaxf(v[j], v[j + 1]), fmaxf(v[j + 2], v[j + 3])));
+                    }
+                    mnf = fminf(mnf, a0);
+                    mxf = fmaxf(mxf, b0);
+                    seen = true;
+                } else if (ext.kmin) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int col = n0 + col0 + j;
+                        if (col >= R) break;
+                        if (col >= lab_end) {  // label boundary
+                            if (seen && q < nq) {
+                                atomicMin(ext.kmin + (size_t)q * ext.L + lab, ord_key(mnf));
+                                atomicMax(ext.kmax + (size_t)q * ext.L + lab, ord_key(mxf));
+                            }
+                            mnf = __int_as_float(0x7f800000);
+                            mxf = -__int_as_float(0x7f800000);
+                            do {
+                                ++lab;
+                                lab_end = __ldg(ext.lstart + lab + 1);
+                            } while (col >= lab_end);
+                        }
+                        mnf = fminf(mnf, v[j]);
+                        mxf = fmaxf(mxf, v[j]);
+                        seen = true;
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = 8 * i + (lane >> 2), u = lane & 3;
+                    const int qq = m0 + 32 * quarter + r, col = n0 + col0 + 4 * u;
+                    const float4 val = chunk[r * 4 + (u ^ ((r >> 1) & 3))];
+                    if (qq >= nq || col >= R) continue;
+                    float* dst = out + (size_t)qq * ld + col;
+                    if (vec_store && col + 3 < R) {
+                        *reinterpret_cast<float4*>(dst) = val;
+                    } else {
+                        dst[0] = val.x;
+                        if (col + 1 < R) dst[1] = val.y;
+                        if (col + 2 < R) dst[2] = val.z;
+                        if (col + 3 < R) dst[3] = val.w;
+                    }
+                }
+                __syncwarp();  // the next chunk may overwrite the staging buffer
+            }
+            if (ext.kmin && seen && q < nq) {
+                atomicMin(ext.kmin + (size_t)q * ext.L + lab, ord_key(mnf));
+                atomicMax(ext.kmax + (size_t)q * ext.L + lab, ord_key(mxf));
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == ISSUER) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -1018,12 +1284,30 @@ void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, con
     gm = std::max(gm, 1);
     // recombination of the planes' products for the split the limbs were written with
     const int k1 = limb_w ? 1 : 127, cbase = limb_w ? limb_w * limb_w + 1 : 128;
-    if (!f16 && !pair && limb_w > 0 && (wide_warps == 8 || wide_warps == 16)) {
+    if (!f16 && !pair && limb_w > 0 && (wide_warps == 8 || wide_warps == 16 || wide_warps == 18)) {
         const CUtensorMap ta = limb_map(A, nq, 3 * Kp, BM), tb = limb_map(B, R, 3 * Kp, WBN);
-        const size_t smem = corr_wide_smem(wide_warps);
         const long tiles = (long)((nq + BM - 1) / BM) * ((R + WBN - 1) / WBN);
         const int grid = (int)std::min<long>(tiles, device_sm_count());
+        int resident = 0;
+        if (wide_warps == 18) {
+            SGR_CUDA(cudaFuncSetAttribute(corr_wide_hold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)corr_wide_smem(16)));
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, corr_wide_hold_kernel, HOLD_THREADS,
+                                                              corr_wide_smem(16)) != cudaSuccess)
+                resident = 0;
+            cudaGetLastError();
+            if (resident < 1) wide_warps = 16;  // its registers and shared memory do not fit one SM here
+        }
+        if (wide_warps == 18) {  // the overlapped form (18 warps per CTA)
+            const size_t hsmem = corr_wide_smem(16);
+            corr_wide_hold_kernel<<<grid, HOLD_THREADS, hsmem, s>>>(ta, tb, nq, R, Kp, ra, rb, scores, ld, status, ext,
+                                                                    gm, cbase);
+            SGR_LAUNCH_CHECK();
+            count_launch();
+            return;
+        }
         auto kern = wide_warps == 16 ? corr_wide_kernel<16> : corr_wide_kernel<8>;
+        const size_t smem = corr_wide_smem(wide_warps);
         SGR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<grid, 32 * (4 + wide_warps), smem, s>>>(ta, tb, nq, R, Kp, ra, rb, scores, ld, status, ext, gm,
                                                         cbase);

@@ -191,7 +191,8 @@ struct LabelExtremes {
 // so the CTAs at work share them through L2); 1 visits band after band.
 // limb_w: the split of the exact limbs (split_limbs; 0 = base 128).  wide_warps 8 or 16 (with
 // limb_w > 0, not f16 or pair) runs the 128 x 256-tile two-accumulator form with that many epilogue
-// warps; 0 the 128 x 160 three-accumulator form.
+// warps, 18 its overlapped form (18 warps per CTA: A1 held in registers while the next tile's MMAs
+// run); 0 the 128 x 160 three-accumulator form.
 void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
                     const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s,
                     bool f16 = false, LabelExtremes ext = LabelExtremes{}, bool pair = false, int gm = 1,

@@ -152,10 +152,11 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
  * same with 32 registers per thread (twice the warps per SM);
  * what 8: 1 trains the markers on the host instead of the device; what 9 (exact mode): 1 fine-tunes
  * each score block on a second stream while the next block is scored; what 10: the exact
- * correlation's tile: 8 or 16 (default) for 128 x 256 tiles with two accumulators (when the trained
- * marker count allows the two-accumulator split, G <= 1921) and that many epilogue warps, 0 for
- * 128 x 160 tiles with three accumulators; what 11: 1 makes the next training write the base-128
- * limb split, which only the 128 x 160 form multiplies.
+ * correlation's tile: 8 or 16 for 128 x 256 tiles with two accumulators (when the trained marker
+ * count allows the two-accumulator split, G <= 1921) and that many epilogue warps, 18 (default)
+ * for the same tiles with the epilogue overlapping the next tile's products, 0 for 128 x 160 tiles
+ * with three accumulators; what 11: 1 makes the next training write the base-128 limb split, which
+ * only the 128 x 160 forms multiply.
  * No choice above changes any result.  what 4 (exact mode only; no counterpart in the reference):
  * 1 runs the score-step correlation on FP16 operands with FP32 accumulation (one tensor-core
  * product instead of three INT8 products; scores are not exact, their error against the exact
@@ -187,7 +188,7 @@ typedef struct sgr_tuning {
     int32_t score_trials;   /* phase-1 trials */
     double score_best_ms;   /* wall time of the chosen score step on the sample */
     int32_t pipeline;       /* 1: each score block's fine-tune overlaps the next block's score step */
-    int32_t corr_wide;      /* 8 / 16: 128 x 256-tile correlation with that many epilogue warps, 0: 128 x 160 */
+    int32_t corr_wide;      /* 8 / 16 / 18: 128 x 256-tile correlation (18: overlapped), 0: 128 x 160 */
 } sgr_tuning;
 sgr_status sgr_autotune(sgr_ctx* ctx, const sgr_csr* sample, float quantile, float finetune_thre,
                         int32_t finetune_times, int32_t learned, float min_confidence, float check_fraction,

@@ -150,13 +150,14 @@ def test_fp16_variant_close_to_exact(kind):
 
 
 @pytest.mark.parametrize("kind", ["tiny", "small"])
-@pytest.mark.parametrize("base128,pair,wide,gm", [(0, 0, 16, 1), (0, 0, 16, 8), (0, 0, 8, 1), (0, 0, 0, 1),
-                                                  (0, 1, 0, 8), (1, 0, 0, 8), (1, 1, 0, 1), (1, 0, 16, 1)])
+@pytest.mark.parametrize("base128,pair,wide,gm", [(0, 0, 18, 1), (0, 0, 18, 8), (0, 0, 16, 1), (0, 0, 16, 8),
+                                                  (0, 0, 8, 1), (0, 0, 0, 1), (0, 1, 0, 8), (1, 0, 0, 8),
+                                                  (1, 1, 0, 1), (1, 0, 18, 1)])
 def test_correlation_forms_bit_exact(kind, base128, pair, wide, gm):
     """Every tensor-core form of the exact correlation gives the oracle's exact scores bit for bit, and
     the oracle's labels (query and reference counts that are not multiples of the tile sizes
-    included): 128 x 256 tiles with two accumulators (8 or 16 epilogue warps), 128 x 160 tiles with
-    three, and their SM-pair form (tcgen05 cta_group::2), on either split of the limbs (the base-128
+    included): 128 x 256 tiles with two accumulators (8 or 16 epilogue warps, or 16 overlapping the
+    next tile's products), 128 x 160 tiles with three, and their SM-pair form (tcgen05 cta_group::2), on either split of the limbs (the base-128
     split has no two-accumulator form and takes the 128 x 160 tiles), in band-by-band or grouped tile
     order."""
     a, prob = annotator(kind, abi.MODE_EXACT, base128)
