@@ -640,13 +640,15 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const float4 val = chunk[r * 4 + (u ^ ((r >> 1) & 3))];
                     if (qq >= nq || col >= R) continue;
                     float* dst = out + (size_t)qq * ld + col;
+                    // streaming stores (evict first): the scores are read once, later, and must not
+                    // push the reference operand out of L2
                     if (vec_store && col + 3 < R) {
-                        *reinterpret_cast<float4*>(dst) = val;
+                        __stcs(reinterpret_cast<float4*>(dst), val);
                     } else {
-                        dst[0] = val.x;
-                        if (col + 1 < R) dst[1] = val.y;
-                        if (col + 2 < R) dst[2] = val.z;
-                        if (col + 3 < R) dst[3] = val.w;
+                        __stcs(dst, val.x);
+                        if (col + 1 < R) __stcs(dst + 1, val.y);
+                        if (col + 2 < R) __stcs(dst + 2, val.z);
+                        if (col + 3 < R) __stcs(dst + 3, val.w);
                     }
                 }
                 __syncwarp();  // the next chunk may overwrite the staging buffer
@@ -930,13 +932,15 @@ __global__ void __launch_bounds__(32 * (4 + EW), 1)
                     const float4 val = chunk[r * 4 + (u ^ ((r >> 1) & 3))];
                     if (qq >= nq || col >= R) continue;
                     float* dst = out + (size_t)qq * ld + col;
+                    // streaming stores (evict first): the scores are read once, later, and must not
+                    // push the reference operand out of L2
                     if (vec_store && col + 3 < R) {
-                        *reinterpret_cast<float4*>(dst) = val;
+                        __stcs(reinterpret_cast<float4*>(dst), val);
                     } else {
-                        dst[0] = val.x;
-                        if (col + 1 < R) dst[1] = val.y;
-                        if (col + 2 < R) dst[2] = val.z;
-                        if (col + 3 < R) dst[3] = val.w;
+                        __stcs(dst, val.x);
+                        if (col + 1 < R) __stcs(dst + 1, val.y);
+                        if (col + 2 < R) __stcs(dst + 2, val.z);
+                        if (col + 3 < R) __stcs(dst + 3, val.w);
                     }
                 }
                 __syncwarp();  // the next chunk may overwrite the staging buffer
@@ -1136,11 +1140,18 @@ __global__ void __launch_bounds__(HOLD_THREADS, 1)
                 break;
             }
             tc_fence_after();
+            // reference norms of this warp's columns, lanes 0-15 of chunk c; the next chunk's loaded
+            // while this one is scored (NaN for a constant reference row)
+            auto norm_of = [&](int c) {
+                const int rcol = n0 + part * WCOLS + c * 16 + lane;
+                return (lane < 16 && rcol < R) ? rr[rcol] : 0.0;
+            };
+            double rr_next = norm_of(0);
 #pragma unroll
             for (int c = 0; c < WCH; ++c) {
                 const int col0 = part * WCOLS + c * 16;
-                const int rcol = n0 + col0 + lane;
-                const double rrl = (lane < 16 && rcol < R) ? rr[rcol] : 0.0;  // NaN for a constant reference row
+                const double rrl = rr_next;
+                if (c + 1 < WCH) rr_next = norm_of(c + 1);
                 uint32_t x2[16];
                 tmem_ld16(b2 + 16 * c, x2);
                 tmem_wait_ld();
@@ -1197,13 +1208,15 @@ __global__ void __launch_bounds__(HOLD_THREADS, 1)
                     const float4 val = chunk[r * 4 + (u ^ ((r >> 1) & 3))];
                     if (qq >= nq || col >= R) continue;
                     float* dst = out + (size_t)qq * ld + col;
+                    // streaming stores (evict first): the scores are read once, later, and must not
+                    // push the reference operand out of L2
                     if (vec_store && col + 3 < R) {
-                        *reinterpret_cast<float4*>(dst) = val;
+                        __stcs(reinterpret_cast<float4*>(dst), val);
                     } else {
-                        dst[0] = val.x;
-                        if (col + 1 < R) dst[1] = val.y;
-                        if (col + 2 < R) dst[2] = val.z;
-                        if (col + 3 < R) dst[3] = val.w;
+                        __stcs(dst, val.x);
+                        if (col + 1 < R) __stcs(dst + 1, val.y);
+                        if (col + 2 < R) __stcs(dst + 2, val.z);
+                        if (col + 3 < R) __stcs(dst + 3, val.w);
                     }
                 }
                 __syncwarp();  // the next chunk may overwrite the staging buffer
