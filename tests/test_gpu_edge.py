@@ -255,7 +255,10 @@ def test_autotune_keeps_results():
     a = abi.Annotator(gpuid=0)
     a.train(prob.ref, prob.celltypes, prob.label_names, prob.ref_genes, prob.qry_genes)
     t = a.autotune(prob.qry)
-    assert t["trials"] == 20 and t["score_trials"] == 24 and t["pipeline"] in (0, 1)
+    # score step: 5 correlation forms (this marker count allows the two-accumulator split) x 2 tile
+    # orders x 2 block sizes x 3 selection forms
+    assert t["trials"] == 20 and t["score_trials"] == 60 and t["pipeline"] in (0, 1)
+    assert t["corr_wide"] in (0, 8, 16, 18)
     assert t["ft_warps"] in (8, 32) and t["ft_heavy"] in (4, 6, 9, 16, 1 << 30)
     assert t["score_chunk_mb"] in (256, 1024) and 0 < t["best_ms"] <= t["worst_ms"]
     assert t["corr_pair"] in (0, 1) and t["corr_gm"] in (1, 16) and t["select_warps"] in (0, 1, 16)
