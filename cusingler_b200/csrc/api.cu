@@ -1269,7 +1269,7 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
         ctx->sp_nq.ensure(Hm);
         ctx->sp_rq.ensure(Hm);
         ctx->sp_scores.ensure(Hm * ctx->R32);
-        ctx->sp_nan.ensure(Hm * 8 * max_label);
+        ctx->sp_nan.ensure(Hm * 16 * max_label);
         ctx->sp_rows.ensure(1);
         ss = side_stream(ctx);
         SGR_CUDA(cudaEventRecord(ctx->ev_fork, s));
@@ -1294,7 +1294,7 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
         ctx->sp_nq.ensure(H);
         ctx->sp_rq.ensure(H);
         ctx->sp_scores.ensure((size_t)H * ctx->R32);
-        ctx->sp_nan.ensure((size_t)H * 8 * max_label);
+        ctx->sp_nan.ensure((size_t)H * 16 * max_label);
         SGR_CUDA(cudaMemsetAsync(ctx->sp_state.p, 0, H * sizeof(int), s));
         ctx->sp_rows.ensure(1);
         SGR_CUDA(cudaMemsetAsync(ctx->sp_rows.p, 0, sizeof(unsigned long long), s));

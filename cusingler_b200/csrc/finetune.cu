@@ -580,7 +580,8 @@ __global__ void __launch_bounds__(NW * 32) ft_persistent_kernel(FtPersistentArgs
 // spread over a grid of 16 CTAs per SM, rows scanned with four loads in flight, and the scores of a
 // round are staged in shared memory for the quantiles.
 
-constexpr int SPLIT_STAGE = 12288;  // rows of a round whose scores are staged for the quantiles
+constexpr int SPLIT_STAGE = 21504;  // rows of a round whose scores are staged for the quantiles
+constexpr int SPLIT_NW = 16;        // warps of the setup and decision CTAs
 constexpr int SPLIT_SCAN_PF = 4;    // entry vectors in flight per row in the spread scan
 constexpr int SPLIT_SCAN_CTAS = 16; // scan CTAs per SM
 
@@ -596,7 +597,7 @@ __device__ void split_finish(const FtPersistentArgs& a, const FtSplit& sp, int i
 // ranks (e-values into sp.eqv), label offsets, and the round's chunks appended to chunk list q.
 // smem: split_prepare_smem bytes.
 __device__ void split_setup_round(const FtPersistentArgs& a, const FtSplit& sp, int i, int q, unsigned char* smem) {
-    constexpr int NW = 8;
+    constexpr int NW = SPLIT_NW;
     const int tid = threadIdx.x;
     const int Wt = a.Wt;
     const int nwords = (Wt + 31) / 32;
@@ -651,7 +652,7 @@ __device__ void split_setup_round(const FtPersistentArgs& a, const FtSplit& sp, 
 
 // First round of every heavy cell: candidates from the flags, then the round's setup (chunk list 0).
 // grid = H.
-__global__ void __launch_bounds__(256) split_first_kernel(FtPersistentArgs a, FtSplit sp) {
+__global__ void __launch_bounds__(SPLIT_NW * 32) split_first_kernel(FtPersistentArgs a, FtSplit sp) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int i = blockIdx.x, lane = threadIdx.x & 31;
     if (threadIdx.x < 32) {
@@ -714,9 +715,9 @@ __global__ void __launch_bounds__(256) split_scan_kernel(FtPersistentArgs a, FtS
 
 // Per cell scanned this round: quantiles (from shared memory when the round's scores fit), the keep /
 // drop rule, then the setup of its next round (chunks appended to list q).  grid = H.
-__global__ void __launch_bounds__(256) split_decide_kernel(FtPersistentArgs a, FtSplit sp, int q) {
+__global__ void __launch_bounds__(SPLIT_NW * 32) split_decide_kernel(FtPersistentArgs a, FtSplit sp, int q) {
     extern __shared__ __align__(16) unsigned char smem[];
-    constexpr int NW = 8;
+    constexpr int NW = SPLIT_NW;
     __shared__ int hist[NW * 256];
     __shared__ float lsc[256];
     __shared__ int off[257];
@@ -725,13 +726,13 @@ __global__ void __launch_bounds__(256) split_decide_kernel(FtPersistentArgs a, F
     const int total = sp.total[i];
     if (total == 0) return;  // finished
     const int ntop = sp.ntop[i];
-    for (int t = threadIdx.x; t <= ntop; t += 256) off[t] = sp.off[(size_t)i * 257 + t];
-    for (int t = threadIdx.x; t < ntop; t += 256) top[t] = sp.top[(size_t)i * 256 + t];
+    for (int t = threadIdx.x; t <= ntop; t += NW * 32) off[t] = sp.off[(size_t)i * 257 + t];
+    for (int t = threadIdx.x; t < ntop; t += NW * 32) top[t] = sp.top[(size_t)i * 256 + t];
     const float* scores = sp.scores + (size_t)i * sp.max_rcand;
     if (total <= SPLIT_STAGE) {  // total is a multiple of 32 (label ranges are padded to 32 rows)
         float4* st = reinterpret_cast<float4*>(smem);
         const float4* src = reinterpret_cast<const float4*>(scores);
-        for (int t = threadIdx.x; t < total / 4; t += 256) st[t] = src[t];
+        for (int t = threadIdx.x; t < total / 4; t += NW * 32) st[t] = src[t];
         scores = reinterpret_cast<const float*>(smem);
     }
     __syncthreads();
@@ -770,7 +771,7 @@ void split_round_setup(const FtPersistentArgs& a) {
 }
 
 void launch_split_first(const FtPersistentArgs& a, const FtSplit& sp, int H, cudaStream_t s) {
-    split_first_kernel<<<H, 256, split_prepare_smem(a.Wt, a.capq), s>>>(a, sp);
+    split_first_kernel<<<H, SPLIT_NW * 32, split_prepare_smem(a.Wt, a.capq), s>>>(a, sp);
     SGR_LAUNCH_CHECK();
     count_launch(1);
 }
@@ -778,7 +779,7 @@ void launch_split_first(const FtPersistentArgs& a, const FtSplit& sp, int H, cud
 void launch_split_round(const FtPersistentArgs& a, const FtSplit& sp, int H, int q, cudaStream_t s) {
     split_scan_kernel<<<SPLIT_SCAN_CTAS * device_sm_count(), 256, split_scan_smem(a.Wt), s>>>(a, sp, q);
     SGR_LAUNCH_CHECK();
-    split_decide_kernel<<<H, 256, split_decide_smem(a.Wt, a.capq), s>>>(a, sp, q ^ 1);
+    split_decide_kernel<<<H, SPLIT_NW * 32, split_decide_smem(a.Wt, a.capq), s>>>(a, sp, q ^ 1);
     SGR_LAUNCH_CHECK();
     count_launch(2);
 }

@@ -251,7 +251,7 @@ struct FtSplit {
     int* off;               // H x 257 label offsets
     int* eqv;               // H x Wt query e-values
     float* scores;          // H x max_rcand
-    float* nan_scratch;     // H x 8 x max_label
+    float* nan_scratch;     // H x 16 x max_label
     int max_rcand;
     unsigned long long* rows_scored;  // device counter: reference rows scored, summed over rounds
     int* items;             // 2 x max_items chunk lists (i * max_chunks + c)
