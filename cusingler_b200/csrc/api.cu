@@ -426,9 +426,11 @@ cudaStream_t copy_stream(sgr_ctx* ctx) {
 }
 
 // Copies the values and indices of a host query's rows into the device CSR buffers on the copy
-// stream, one row chunk at a time; ctx->up_ev[c] is recorded after chunk c.
-void copy_row_chunks(sgr_ctx* ctx, const sgr_csr* h, const DevCsr& q, uint32_t chunk, uint32_t n_chunks) {
+// stream, one row chunk at a time (chunk c: rows [starts[c], starts[c + 1])); ctx->up_ev[c] is
+// recorded after chunk c.
+void copy_row_chunks(sgr_ctx* ctx, const sgr_csr* h, const std::vector<uint32_t>& starts) {
     cudaStream_t cs = copy_stream(ctx);
+    const uint32_t n_chunks = (uint32_t)starts.size() - 1;
     while (ctx->up_ev.size() < n_chunks) {
         cudaEvent_t e;
         SGR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -439,7 +441,7 @@ void copy_row_chunks(sgr_ctx* ctx, const sgr_csr* h, const DevCsr& q, uint32_t c
     SGR_CUDA(cudaStreamWaitEvent(cs, ctx->up_ev[0], 0));
     const int sp = ctx->prof.begin(ST_H2D, cs);
     for (uint32_t c = 0; c < n_chunks; ++c) {
-        const uint32_t r0 = c * chunk, r1 = std::min(q.n_rows, r0 + chunk);
+        const uint32_t r0 = starts[c], r1 = starts[c + 1];
         const size_t b = (size_t)h->indptr[r0], e = (size_t)h->indptr[r1];
         if (e > b) {
             SGR_CUDA(cudaMemcpyAsync(ctx->q_data.p + b, h->data + b, (e - b) * sizeof(float),
@@ -695,7 +697,8 @@ struct ScorePlan {
     DevCsr q;
     const sgr_csr* host = nullptr;
     float p = 0.8f, thre = 0.05f;
-    uint32_t chunk = 1, n_chunks = 0;
+    uint32_t chunk = 1, n_chunks = 0;  // chunk: the largest block's rows
+    std::vector<uint32_t> starts;      // block c: rows [starts[c], starts[c + 1])
     bool fp32 = false, f16 = false, tc_ext = false;
     int rank_out = RANK_LIMBS, rank_norm = NORM_NONE;
     float* scratch = nullptr;
@@ -722,14 +725,31 @@ ScorePlan score_begin(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const 
     pl.f16 = ctx->corr_f16 && !pl.fp32;
     if (pl.f16) ensure_ref_f16(ctx);
     pl.chunk = (uint32_t)std::max<size_t>(1, std::min<size_t>(Q, ctx->score_chunk_bytes / (4 * (size_t)R)));
-    pl.n_chunks = (Q + pl.chunk - 1) / pl.chunk;
+    // Blocks of `chunk` rows.  When the rows come from the host, the score step waits on the copy,
+    // and only the last block is left to score once the copy ends: that block is cut into halves,
+    // quarters, ... down to about 2,048 rows, so that little is left after the last rows arrive.
+    std::vector<uint32_t> sizes;
+    for (uint32_t r = 0; r < Q; r += pl.chunk) sizes.push_back(std::min(pl.chunk, Q - r));
+    if (host && !sizes.empty()) {
+        uint32_t last = sizes.back();
+        sizes.pop_back();
+        while (last > 2048) {
+            const uint32_t half = last / 2;
+            sizes.push_back(half);
+            last -= half;
+        }
+        sizes.push_back(last);
+    }
+    pl.starts.assign(1, 0);
+    for (uint32_t n : sizes) pl.starts.push_back(pl.starts.back() + n);
+    pl.n_chunks = (uint32_t)sizes.size();
     // Rows already on the device are ranked in one launch.  Host rows are ranked block by block as
     // they arrive: one rank group per block, each writing its own rows' limbs and norms.
     const size_t row_bytes = (size_t)(pl.f16 ? 2 : 3) * ctx->Kp;
     const uint32_t n_groups = host ? pl.n_chunks : 1;
     std::vector<RankGroup> groups(n_groups);
     for (uint32_t c = 0; c < n_groups; ++c) {
-        const size_t r0 = (size_t)c * pl.chunk;
+        const size_t r0 = pl.starts[c];
         groups[c] = RankGroup{ctx->qry_map_common.p, ctx->G,          ctx->Kp,
                               ctx->q_limbs.p + r0 * row_bytes, ctx->q_n2.p + r0, ctx->q_rinv.p + r0,
                               ctx->q_f32.p + r0, ctx->limb_w};
@@ -738,7 +758,7 @@ ScorePlan score_begin(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const 
     pl.rank_out = pl.f16 ? RANK_F16 : RANK_LIMBS;
     pl.rank_norm = pl.fp32 ? NORM_SEQ : NORM_NONE;
     if (host) {
-        copy_row_chunks(ctx, host, q, pl.chunk, pl.n_chunks);
+        copy_row_chunks(ctx, host, pl.starts);
     } else {
         const uint64_t l0 = launch_count();
         const int sp = ctx->prof.begin(ST_RANK, s);
@@ -778,12 +798,12 @@ ScorePlan score_begin(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const 
     return pl;
 }
 
-// Block c of the score step on the context's stream: rows [c * chunk, min(Q, (c + 1) * chunk)).
+// Block c of the score step on the context's stream: rows [starts[c], starts[c + 1]).
 void score_block(sgr_ctx* ctx, const ScorePlan& pl, uint32_t c) {
     cudaStream_t s = ctx->stream;
     const uint32_t Q = pl.q.n_rows, R = ctx->R, L = ctx->mk.n_labels;
-    const uint32_t q0 = c * pl.chunk;
-    const int nq = (int)std::min(pl.chunk, Q - q0);
+    const uint32_t q0 = pl.starts[c];
+    const int nq = (int)(pl.starts[c + 1] - q0);
     int sp = -1;
     if (pl.host) {
         SGR_CUDA(cudaStreamWaitEvent(s, ctx->up_ev[c], 0));
@@ -1455,7 +1475,7 @@ void annotate_pipelined(sgr_ctx* ctx, const DevCsr& q, const sgr_csr* host, floa
     }
     const uint32_t per10k = (uint32_t)std::lround(std::min(std::max(check_fraction, 0.f), 1.f) * 10000.f);
     auto finetune_block = [&](uint32_t c) {
-        const uint32_t r0 = c * pl.chunk, n = std::min(pl.chunk, Q - r0);
+        const uint32_t r0 = pl.starts[c], n = pl.starts[c + 1] - r0;
         SGR_CUDA(cudaStreamWaitEvent(f, block_event(ctx, c), 0));
         DevCsr qc{q.data, q.indices, q.indptr + r0, n, q.n_cols, -1};
         ctx->stream = f;
@@ -1472,7 +1492,7 @@ void annotate_pipelined(sgr_ctx* ctx, const DevCsr& q, const sgr_csr* host, floa
     for (uint32_t c = 0; c < pl.n_chunks; ++c) {
         score_block(ctx, pl, c);
         if (learned) {
-            const uint32_t r0 = c * pl.chunk, n = std::min(pl.chunk, Q - r0);
+            const uint32_t r0 = pl.starts[c], n = pl.starts[c + 1] - r0;
             const int sp = ctx->prof.begin(ST_MLP, s);
             ctx->mlp.features(ctx->label_scores.p + (size_t)r0 * L, (int)n, ctx->mlp_x.p + (size_t)r0 * L,
                               ctx->mlp_bad.p + r0, s);
