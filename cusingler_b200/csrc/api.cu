@@ -127,6 +127,7 @@ struct sgr_ctx {
     std::vector<int64_t> h_ref_n2;
     DevBuf<float> reff_data;
     DevBuf<int32_t> reff_indices, reff_indptr;
+    DevBuf<int> filter_max;        // filter_csr: longest compacted row
     DevBuf<int> sp_items;          // split path: two chunk lists
     DevBuf<int> sp_nitems;         // split path: their lengths
     DevBuf<int32_t> d_blk_base;    // fine-tune lists: first 32-row block of each label
@@ -454,20 +455,26 @@ void copy_row_chunks(sgr_ctx* ctx, const sgr_csr* h, const std::vector<uint32_t>
     }
 }
 
-// Compacts a device CSR to the columns with map >= 0 into (data, indices, indptr) buffers.
-void filter_csr(sgr_ctx* ctx, const DevCsr& m, const int32_t* map, DevBuf<float>& od, DevBuf<int32_t>& oi,
-                DevBuf<int32_t>& op, const uint8_t* row_mask = nullptr) {
+// Compacts a device CSR to the columns with map >= 0 into (data, indices, indptr) buffers.  Returns
+// the longest compacted row (read back with the total, in the same synchronisation).
+int32_t filter_csr(sgr_ctx* ctx, const DevCsr& m, const int32_t* map, DevBuf<float>& od, DevBuf<int32_t>& oi,
+                   DevBuf<int32_t>& op, const uint8_t* row_mask = nullptr) {
     ctx->counts.ensure(m.n_rows + 1);
     op.ensure((size_t)m.n_rows + 1);
-    launch_filter_count(m.indptr, m.indices, m.n_rows, m.n_cols, map, ctx->counts.p, ctx->stream, row_mask);
+    ctx->filter_max.ensure(1);
+    SGR_CUDA(cudaMemsetAsync(ctx->filter_max.p, 0, sizeof(int), ctx->stream));
+    launch_filter_count(m.indptr, m.indices, m.n_rows, m.n_cols, map, ctx->counts.p, ctx->stream, row_mask,
+                        ctx->filter_max.p);
     int32_t* scan_scratch = ctx->scan_part.ensure(2 * (((size_t)m.n_rows + 4095) / 4096) + 1);
     launch_exclusive_scan(ctx->counts.p, op.p, m.n_rows, scan_scratch, ctx->stream);
-    int32_t total = 0;
+    int32_t total = 0, longest = 0;
     SGR_CUDA(cudaMemcpyAsync(&total, op.p + m.n_rows, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    SGR_CUDA(cudaMemcpyAsync(&longest, ctx->filter_max.p, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     SGR_CUDA(cudaStreamSynchronize(ctx->stream));
     od.ensure(std::max<int32_t>(total, 1));
     oi.ensure(std::max<int32_t>(total, 1));
     launch_filter_fill(m.data, m.indptr, m.indices, m.n_rows, m.n_cols, map, op.p, od.p, oi.p, ctx->stream, row_mask);
+    return longest;
 }
 
 std::vector<int32_t> position_map(const std::vector<int32_t>& colmap, const std::vector<uint32_t>& genes,
@@ -1166,7 +1173,8 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
         launch_mark_rows(cell_list, n, mask, s);
         row_mask = mask;
     }
-    filter_csr(ctx, q, ctx->qry_map_thre.p, ctx->qf_data, ctx->qf_indices, ctx->qf_indptr, row_mask);
+    const int32_t longest = filter_csr(ctx, q, ctx->qry_map_thre.p, ctx->qf_data, ctx->qf_indices, ctx->qf_indptr,
+                                       row_mask);
     uint32_t max_label = 1;
     std::vector<LabelQ> lq(L);
     for (uint32_t l = 0; l < L; ++l) {
@@ -1176,11 +1184,7 @@ void finetune_persistent(sgr_ctx* ctx, const DevCsr& q, const uint8_t* flags_dev
     ctx->d_lq_label.upload(lq, s);
     // query sort buffer: the longest thre-pool row of this batch (rows beyond 8192 entries take the
     // kernel's counting path)
-    std::vector<int32_t> qptr(Q + 1);
-    SGR_CUDA(cudaMemcpyAsync(qptr.data(), ctx->qf_indptr.p, (Q + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    SGR_CUDA(cudaStreamSynchronize(s));
-    int qmax = 32;
-    for (uint32_t i = 0; i < Q; ++i) qmax = std::max(qmax, qptr[i + 1] - qptr[i]);
+    const int qmax = std::max(32, longest);
     const int capq = std::min(pow2_at_least(qmax), 8192);
     const int nw = ctx->ft_warps;
     const size_t smem = ft_persistent_smem((int)std::max<uint32_t>(Wt, 1), capq, nw);

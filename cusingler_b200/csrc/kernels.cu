@@ -318,8 +318,9 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
 
 // row_mask (optional): rows with mask 0 are left empty.
 __global__ void filter_count_kernel(const int32_t* indptr, const int32_t* indices, uint32_t n_rows, uint32_t n_cols,
-                                    const int32_t* map, int32_t* counts, const uint8_t* row_mask) {
+                                    const int32_t* map, int32_t* counts, const uint8_t* row_mask, int* row_max) {
     const int lane = threadIdx.x & 31;
+    int mx = 0;
     for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n_rows;
          row += (gridDim.x * blockDim.x) >> 5) {
         if (row_mask && !row_mask[row]) {
@@ -333,7 +334,9 @@ __global__ void filter_count_kernel(const int32_t* indptr, const int32_t* indice
         }
         cnt = __reduce_add_sync(FULL, cnt);
         if (lane == 0) counts[row] = cnt;
+        mx = max(mx, cnt);
     }
+    if (row_max && lane == 0 && mx > 0) atomicMax(row_max, mx);
 }
 
 __global__ void filter_fill_kernel(const float* data, const int32_t* indptr, const int32_t* indices, uint32_t n_rows,
@@ -788,10 +791,11 @@ void launch_rank(const RankLaunch& a, cudaStream_t s) {
 }
 
 void launch_filter_count(const int32_t* indptr, const int32_t* indices, uint32_t n_rows, uint32_t n_cols,
-                         const int32_t* map, int32_t* counts, cudaStream_t s, const uint8_t* row_mask) {
+                         const int32_t* map, int32_t* counts, cudaStream_t s, const uint8_t* row_mask,
+                         int* row_max) {
     if (!n_rows) return;
     const unsigned blocks = std::min<unsigned>((n_rows + 7) / 8, sm_count() * 16);
-    filter_count_kernel<<<blocks, 256, 0, s>>>(indptr, indices, n_rows, n_cols, map, counts, row_mask);
+    filter_count_kernel<<<blocks, 256, 0, s>>>(indptr, indices, n_rows, n_cols, map, counts, row_mask, row_max);
     SGR_LAUNCH_CHECK();
     count_launch();
 }

@@ -84,10 +84,11 @@ void column_bits(const int32_t* colmap, uint32_t n_cols, uint32_t* bits, uint16_
 
 void launch_rank(const RankLaunch& a, cudaStream_t s);
 
-// Compact a CSR to the columns with map[c] >= 0 (new column = map[c]); two passes.
+// Compact a CSR to the columns with map[c] >= 0 (new column = map[c]); two passes.  row_max (may be
+// null, not cleared here): atomic maximum of the kept entries per row.
 void launch_filter_count(const int32_t* indptr, const int32_t* indices, uint32_t n_rows, uint32_t n_cols,
                          const int32_t* map, int32_t* counts, cudaStream_t s,
-                         const uint8_t* row_mask = nullptr);
+                         const uint8_t* row_mask = nullptr, int* row_max = nullptr);
 // *out += sum of vals[list[i]] for i < *n (n read on the device; *out is not cleared; each value is
 // below 2^32 and a warp's partial sum too).
 void launch_sum_listed(const int32_t* list, const int* n, const int32_t* vals, unsigned long long* out,
