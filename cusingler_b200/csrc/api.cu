@@ -686,7 +686,7 @@ void correlate(sgr_ctx* ctx, bool fp32, const int8_t* A, int nq, uint32_t q0, fl
     if (ctx->corr_f16 && !fp32) {
         launch_corr_tc(A, reinterpret_cast<const int8_t*>(ctx->ref_f16.p), nq, (int)ctx->R, ctx->Kp,
                        ctx->q_rinv.p + q0, ctx->ref_rinv.p, ctx->q_n2.p + q0, ctx->ref_n2.p, out, ld, ctx->status.p,
-                       ctx->stream, true, ext, false, ctx->corr_gm);
+                       ctx->stream, true, ext, false, ctx->corr_gm, 0, ctx->corr_wide);
         return;
     }
     if (fp32 || exact_simt())

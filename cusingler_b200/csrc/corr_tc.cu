@@ -1234,6 +1234,256 @@ __global__ void __launch_bounds__(HOLD_THREADS, 1)
     }
 }
 
+// FP16-operand variant on 128 x 256 tiles (not exact: see corr_tc_kernel<true>).  One plane of d
+// as IEEE half, kind::f16 MMAs with FP32 accumulation into one 256-column accumulator, so two
+// accumulators fit TMEM and the epilogue of tile t reads one while the MMAs of tile t + 1 fill the
+// other.  Warp roles and the epilogue's staging as in corr_wide_hold_kernel.
+__global__ void __launch_bounds__(HOLD_THREADS, 1)
+    corr_wide_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nq,
+                         int R, int Kp, const double* __restrict__ rq, const double* __restrict__ rr,
+                         float* __restrict__ out, int64_t ld, int* status, LabelExtremes ext, int gm) {
+    constexpr int EW = 16, WCOLS = 64, WCH = 4;
+    constexpr int PRODUCER = 16, ISSUER = 17;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ TcShared sh;
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tiles_n = (R + WBN - 1) / WBN, tiles_m = (nq + BM - 1) / BM;
+    const int n_tiles = tiles_m * tiles_n;
+    const int kblocks = 2 * Kp / BK;  // one plane of 2 * Kp bytes
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < WSTAGES; ++s) {
+            mbar_init(smem_u32(&sh.full[s]), 1);
+            mbar_init(smem_u32(&sh.empty[s]), 1);
+        }
+        for (int g = 0; g < 2; ++g) {
+            mbar_init(smem_u32(&sh.acc_full[g]), 1);
+            mbar_init(smem_u32(&sh.acc_empty[g]), EW);
+        }
+        mbar_init(smem_u32(&sh.drain), 1);
+        sh.abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == ISSUER) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh.tmem_base)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sh.tmem_base;
+    volatile int* abort_flag = &sh.abort_flag;
+    auto give_up = [&]() {
+        atomicOr(status, SGR_TC_TIMEOUT);
+        sh.abort_flag = 1;
+    };
+
+    if (warp == PRODUCER) {
+        if (lane == 0) {
+            const uint64_t keep = policy_evict_last();
+            uint32_t it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+                int mb, nb;
+                tile_coords(t, tiles_m, tiles_n, gm, mb, nb);
+                const int m0 = mb * BM, n0 = nb * WBN;
+                for (int kb = 0; kb < kblocks; ++kb, ++it) {
+                    const int s = it % WSTAGES;
+                    const uint32_t ph = (it / WSTAGES) & 1;
+                    if (!mbar_wait(smem_u32(&sh.empty[s]), ph ^ 1, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t a_dst = smem_u32(smem + s * WSTAGE_BYTES);
+                    const uint32_t fb = smem_u32(&sh.full[s]);
+                    mbar_expect_tx(fb, WSTAGE_BYTES);
+                    tma_load_2d(a_dst, &tmA, kb * BK, m0, fb);
+                    tma_load_2d_hint(a_dst + A_BYTES, &tmB, kb * BK, n0, fb, keep);
+                }
+            }
+            if (!ok) give_up();
+            for (uint32_t j = (it > (uint32_t)WSTAGES ? it - WSTAGES : 0); j < it; ++j) {
+                const uint32_t s = j % WSTAGES, ph = (j / WSTAGES) & 1;
+                const long long t0 = clock64();
+                while (!mbar_try(smem_u32(&sh.full[s]), ph) && clock64() - t0 < WAIT_CYCLES) {
+                }
+            }
+        }
+    } else if (warp == ISSUER) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_f16(BM, WBN);
+            uint32_t it = 0, tile_iter = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++tile_iter) {
+                const int region = tile_iter & 1;  // the two accumulators alternate between tiles
+                const uint32_t use = tile_iter >> 1;
+                if (!mbar_wait(smem_u32(&sh.acc_empty[region]), (use & 1) ^ 1, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                for (int kb = 0; kb < kblocks; ++kb, ++it) {
+                    const int s = it % WSTAGES;
+                    const uint32_t ph = (it / WSTAGES) & 1;
+                    if (!mbar_wait(smem_u32(&sh.full[s]), ph, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_addr = smem_u32(smem + s * WSTAGE_BYTES);
+                    const uint64_t da = smem_desc(a_addr), db = smem_desc(a_addr + A_BYTES);
+                    const uint32_t tc = tmem + region * WBN;
+#pragma unroll
+                    for (int k = 0; k < BK / 32; ++k)  // 32 bytes of K (16 halves) per MMA
+                        umma_f16(tc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc,
+                                 (kb == 0 && k == 0) ? 0u : 1u);
+                    umma_commit(smem_u32(&sh.empty[s]));
+                    if (kb == kblocks - 1) umma_commit(smem_u32(&sh.acc_full[region]));
+                }
+            }
+            if (!ok) give_up();
+            umma_commit(smem_u32(&sh.drain));
+        }
+        if (lane == 0) {
+            const long long t0 = clock64();
+            while (!mbar_try(smem_u32(&sh.drain), 0) && clock64() - t0 < WAIT_CYCLES) {
+            }
+        }
+    } else {
+        // ---- epilogue: warps 0-15 --------------------------------------------------------------
+        const int quarter = warp & 3, part = warp >> 2;
+        float4* chunk = reinterpret_cast<float4*>(smem + WSTAGES * WSTAGE_BYTES + warp * CHUNK_BYTES);
+        const bool vec_store = (ld % 4) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+        const int row = 32 * quarter + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
+        uint32_t tile_iter = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++tile_iter) {
+            int mb, nb;
+            tile_coords(t, tiles_m, tiles_n, gm, mb, nb);
+            const int m0 = mb * BM, n0 = nb * WBN;
+            const int q = m0 + row;
+            const int region = tile_iter & 1;
+            const double rqv = q < nq ? rq[q] : 0.0;  // NaN when the query row is constant
+            auto norm_of = [&](int c) {
+                const int rcol = n0 + part * WCOLS + c * 16 + lane;
+                return (lane < 16 && rcol < R) ? rr[rcol] : 0.0;
+            };
+            double rr_next = norm_of(0);
+            int lab = 0, lab_end = 0;
+            float mnf = __int_as_float(0x7f800000), mxf = -__int_as_float(0x7f800000);
+            bool seen = false;
+            if (ext.kmin) {
+                const int cb = n0 + part * WCOLS;
+                int lo = 0, hi = ext.L - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (__ldg(ext.lstart + mid) <= cb) lo = mid;
+                    else hi = mid - 1;
+                }
+                lab = lo;
+                lab_end = __ldg(ext.lstart + lab + 1);
+            }
+            if (!__all_sync(0xffffffffu,
+                            mbar_wait(smem_u32(&sh.acc_full[region]), (tile_iter >> 1) & 1, abort_flag))) {
+                if (lane == 0) give_up();
+                break;
+            }
+            tc_fence_after();
+            const uint32_t base = lane_base + region * WBN + part * WCOLS;
+            uint32_t acc[2][16];
+            tmem_ld16(base, acc[0]);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < WCH; ++c) {
+                const int col0 = part * WCOLS + c * 16;
+                const double rrl = rr_next;
+                if (c + 1 < WCH) {
+                    rr_next = norm_of(c + 1);
+                    tmem_ld16(base + 16 * (c + 1), acc[(c + 1) & 1]);
+                } else {
+                    tc_fence_before();  // every TMEM read of this warp has completed
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(smem_u32(&sh.acc_empty[region]));
+                }
+                float v[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const double rrj = __shfl_sync(0xffffffffu, rrl, j);
+                    v[j] = (float)(((double)__uint_as_float(acc[c & 1][j]) * rqv) * rrj);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    chunk[lane * 4 + (u ^ ((lane >> 1) & 3))] =
+                        make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+                if (ext.kmin && n0 + col0 + 16 <= min(lab_end, R)) {  // the chunk lies in one label
+                    float a0 = fminf(fminf(v[0], v[1]), fminf(v[2], v[3]));
+                    float b0 = fmaxf(fmaxf(v[0], v[1]), fmaxf(v[2], v[3]));
+#pragma unroll
+                    for (int j = 4; j < 16; j += 4) {
+                        a0 = fminf(a0, fminf(fminf(v[j], v[j + 1]), fminf(v[j + 2], v[j + 3])));
+                        b0 = fmaxf(b0, fmaxf(fmaxf(v[j], v[j + 1]), fmaxf(v[j + 2], v[j + 3])));
+                    }
+                    mnf = fminf(mnf, a0);
+                    mxf = fmaxf(mxf, b0);
+                    seen = true;
+                } else if (ext.kmin) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int col = n0 + col0 + j;
+                        if (col >= R) break;
+                        if (col >= lab_end) {  // label boundary
+                            if (seen && q < nq) {
+                                atomicMin(ext.kmin + (size_t)q * ext.L + lab, ord_key(mnf));
+                                atomicMax(ext.kmax + (size_t)q * ext.L + lab, ord_key(mxf));
+                            }
+                            mnf = __int_as_float(0x7f800000);
+                            mxf = -__int_as_float(0x7f800000);
+                            do {
+                                ++lab;
+                                lab_end = __ldg(ext.lstart + lab + 1);
+                            } while (col >= lab_end);
+                        }
+                        mnf = fminf(mnf, v[j]);
+                        mxf = fmaxf(mxf, v[j]);
+                        seen = true;
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = 8 * i + (lane >> 2), u = lane & 3;
+                    const int qq = m0 + 32 * quarter + r, col = n0 + col0 + 4 * u;
+                    const float4 val = chunk[r * 4 + (u ^ ((r >> 1) & 3))];
+                    if (qq >= nq || col >= R) continue;
+                    float* dst = out + (size_t)qq * ld + col;
+                    if (vec_store && col + 3 < R) {
+                        __stcs(reinterpret_cast<float4*>(dst), val);
+                    } else {
+                        __stcs(dst, val.x);
+                        if (col + 1 < R) __stcs(dst + 1, val.y);
+                        if (col + 2 < R) __stcs(dst + 2, val.z);
+                        if (col + 3 < R) __stcs(dst + 3, val.w);
+                    }
+                }
+                __syncwarp();  // the next chunk may overwrite the staging buffer
+                if (c + 1 < WCH) tmem_wait_ld();
+            }
+            if (ext.kmin && seen && q < nq) {
+                atomicMin(ext.kmin + (size_t)q * ext.L + lab, ord_key(mnf));
+                atomicMax(ext.kmax + (size_t)q * ext.L + lab, ord_key(mxf));
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == ISSUER) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -1297,6 +1547,17 @@ void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, con
     gm = std::max(gm, 1);
     // recombination of the planes' products for the split the limbs were written with
     const int k1 = limb_w ? 1 : 127, cbase = limb_w ? limb_w * limb_w + 1 : 128;
+    if (f16 && wide_warps != 0) {  // FP16 operands on 128 x 256 tiles
+        const CUtensorMap ta = limb_map(A, nq, 2 * Kp, BM), tb = limb_map(B, R, 2 * Kp, WBN);
+        const size_t fsmem = corr_wide_smem(16);
+        const long tiles = (long)((nq + BM - 1) / BM) * ((R + WBN - 1) / WBN);
+        const int grid = (int)std::min<long>(tiles, device_sm_count());
+        SGR_CUDA(cudaFuncSetAttribute(corr_wide_f16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem));
+        corr_wide_f16_kernel<<<grid, HOLD_THREADS, fsmem, s>>>(ta, tb, nq, R, Kp, ra, rb, scores, ld, status, ext, gm);
+        SGR_LAUNCH_CHECK();
+        count_launch();
+        return;
+    }
     if (!f16 && !pair && limb_w > 0 && (wide_warps == 8 || wide_warps == 16 || wide_warps == 18)) {
         const CUtensorMap ta = limb_map(A, nq, 3 * Kp, BM), tb = limb_map(B, R, 3 * Kp, WBN);
         const long tiles = (long)((nq + BM - 1) / BM) * ((R + WBN - 1) / WBN);

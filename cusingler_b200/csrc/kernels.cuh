@@ -193,7 +193,8 @@ struct LabelExtremes {
 // limb_w: the split of the exact limbs (split_limbs; 0 = base 128).  wide_warps 8 or 16 (with
 // limb_w > 0, not f16 or pair) runs the 128 x 256-tile two-accumulator form with that many epilogue
 // warps, 18 its overlapped form (18 warps per CTA: A1 held in registers while the next tile's MMAs
-// run); 0 the 128 x 160 three-accumulator form.
+// run); 0 the 128 x 160 three-accumulator form.  With f16, any wide_warps but 0 runs the FP16
+// operands on 128 x 256 tiles with two alternating accumulators.
 void launch_corr_tc(const int8_t* A, const int8_t* B, int nq, int R, int Kp, const double* ra, const double* rb,
                     const int64_t* na, const int64_t* nb, float* scores, int64_t ld, int* status, cudaStream_t s,
                     bool f16 = false, LabelExtremes ext = LabelExtremes{}, bool pair = false, int gm = 1,

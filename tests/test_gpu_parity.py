@@ -130,13 +130,16 @@ def test_final_labels_spread_and_queue_paths(kind, heavy, times):
 
 
 @pytest.mark.parametrize("kind", ["tiny", "small"])
-def test_fp16_variant_close_to_exact(kind):
-    """The FP16-operand correlation variant (FP32 accumulation, not exact): every score within 1e-4
-    of the exact score (a bound of K x 2^-24 relative to the Cauchy-Schwarz bound of the sum), NaN
-    where the exact score is NaN, and first labels that differ only at near-ties."""
+@pytest.mark.parametrize("wide", [18, 0])
+def test_fp16_variant_close_to_exact(kind, wide):
+    """The FP16-operand correlation variant (FP32 accumulation, not exact), on 128 x 256 tiles with
+    two alternating accumulators or on 128 x 160 tiles: every score within 1e-4 of the exact score
+    (a bound of K x 2^-24 relative to the Cauchy-Schwarz bound of the sum), NaN where the exact score
+    is NaN, and first labels that differ only at near-ties."""
     a, prob = annotator(kind, abi.MODE_EXACT)
     raw_exact = a.debug_scores(prob.qry)
     f_exact, s_exact, _ = a.score_first(prob.qry)
+    a.set_tuning(10, wide)
     a.set_tuning(4, 1)
     raw_f16 = a.debug_scores(prob.qry)
     f16, s16, _ = a.score_first(prob.qry)
@@ -157,9 +160,9 @@ def test_correlation_forms_bit_exact(kind, base128, pair, wide, gm):
     """Every tensor-core form of the exact correlation gives the oracle's exact scores bit for bit, and
     the oracle's labels (query and reference counts that are not multiples of the tile sizes
     included): 128 x 256 tiles with two accumulators (8 or 16 epilogue warps, or 16 overlapping the
-    next tile's products), 128 x 160 tiles with three, and their SM-pair form (tcgen05 cta_group::2), on either split of the limbs (the base-128
-    split has no two-accumulator form and takes the 128 x 160 tiles), in band-by-band or grouped tile
-    order."""
+    next tile's products), 128 x 160 tiles with three, and their SM-pair form (tcgen05 cta_group::2),
+    on either split of the limbs (the base-128 split has no two-accumulator form and takes the
+    128 x 160 tiles), in band-by-band or grouped tile order."""
     a, prob = annotator(kind, abi.MODE_EXACT, base128)
     a.set_tuning(5, pair)
     a.set_tuning(10, wide)
