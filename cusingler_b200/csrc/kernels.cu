@@ -59,6 +59,8 @@ __device__ __forceinline__ int rank_bucket(uint64_t key, float fmin, float scale
     return t >= 0.f ? min(255, (int)t) : 0;
 }
 
+constexpr int GATHER_CHUNKS = 8;  // 32-entry chunks of a row whose loads are in flight together
+
 __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
@@ -94,22 +96,22 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
         const int beg = a.indptr[it.row], end = a.indptr[it.row + 1];
 
         // 1) compact the row's entries in the gene subset into (value key, position) sort keys;
-        //    four chunks of 32 entries per step, their loads issued before any is used
+        //    several chunks of 32 entries per step, their loads issued before any is used
         int k = 0, bad = 0;
         if (a.map_bits) {
             // compact map in shared memory: index and value loads are independent, one memory
-            // latency per step
-            for (int base = beg; base < end; base += 128) {
-                int c[4];
-                float v[4];
+            // latency per step of GATHER_CHUNKS chunks
+            for (int base = beg; base < end; base += 32 * GATHER_CHUNKS) {
+                int c[GATHER_CHUNKS];
+                float v[GATHER_CHUNKS];
 #pragma unroll
-                for (int t = 0; t < 4; ++t) {
+                for (int t = 0; t < GATHER_CHUNKS; ++t) {
                     const int i = base + 32 * t + lane;
                     c[t] = i < end ? __ldcs(a.indices + i) : -1;
                     v[t] = i < end ? __ldcs(a.data + i) : 0.f;
                 }
 #pragma unroll
-                for (int t = 0; t < 4; ++t) {
+                for (int t = 0; t < GATHER_CHUNKS; ++t) {
                     const int i = base + 32 * t + lane;
                     bad |= (i < end && (unsigned)c[t] >= a.n_cols) ? 1 : 0;
                     int pos = -1;
