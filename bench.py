@@ -472,7 +472,7 @@ def main():
             ann.set_tuning(1, args.ft_heavy)
             tuning["learned" if learned else "plain"] = {"pinned": True, "ft_warps": args.ft_warps,
                                                           "ft_heavy": args.ft_heavy, "score_chunk_mb": 1024,
-                                                          "corr_pair": 0, "corr_gm": 16, "select_warps": 16,
+                                                          "corr_pair": 0, "corr_gm": 16, "select_warps": 0,
                                                           "pipeline": 0, "corr_wide": 18}
             return
         tuning["learned" if learned else "plain"] = ann.autotune(
