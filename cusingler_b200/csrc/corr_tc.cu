@@ -3,26 +3,29 @@
 // The reference computes every (query, reference) Spearman correlation with one FP32 fused
 // multiply-add chain per pair on CUDA cores (spearman, src/cusingler.cu:918-945 of
 // STOmics/cusingler).  Doubled centred ranks d = 2*rank - (G+1) are integers with |d| < G, so the
-// numerator N = sum_g d_q d_r is computed exactly here: d = 128 h + l (l in [-64, 63]) and the
-// Karatsuba limb s = h + l are int8, and
-//     P1 = H_q . H_r,  P2 = L_q . L_r,  P3 = S_q . S_r   (int32 accumulation in TMEM)
-//     N  = 128 (127 P1 + P3) - 127 P2                     (exact in FP64, |N| < 2^53)
+// numerator N = sum_g d_q d_r is computed exactly here from int8 limbs (split_limbs): planes
+// P0 | L | S with d = m * p0 + s, written by the rank kernel (3 * Kp bytes per row, Kp a multiple
+// of 128, one TMA tensor map per operand over all three planes).  Then
 //     score = float((N * (1/sqrt(n_q))) * (1/sqrt(n_r)))   (FP64); a zero norm has a NaN
 //             reciprocal, so the score of a constant row is NaN as in the reference.
+// Three forms of the exact product (all bit-identical):
+//   corr_wide_hold_kernel (default) and corr_wide_kernel<8|16>: 128 x 256 tiles, two-accumulator
+//       split d = C h + l, C = w^2 + 1: A1 = P0.P0' + S.S', A2 = L.L', N = C A1 - (C - 1) A2;
+//   corr_tc_kernel: 128 x 160 tiles, three accumulators P1 = P0.P0', P3 = S.S', P2 = L.L',
+//       N = C (k1 P1 + P3) - (C - 1) P2 with (k1, C) = (127, 128) for the base-128 split
+//       d = 128 h + l and (1, w^2 + 1) for the two-accumulator one;
+//   its SM-pair form (PAIR), and an FP16-operand variant of the 128 x 160 and 128 x 256 tiles.
 //
-// Operands are the rank kernel's int8 rows [H | L | S] (3 * Kp bytes, Kp a multiple of 128), so one
-// TMA tensor map per operand covers all three limb planes.  Per tile the K loop runs plane by plane
-// in the order H, S, L into three TMEM accumulators of BN = 160 columns (P1, P3, P2; 480 of 512
-// columns).  A 128 x 160 tile (rather than 128 x 128) reads fewer operand bytes from shared memory
-// per MMA cycle, which bounds the M = 128 int8 MMA.
-//
+// corr_tc_kernel: per tile the K loop runs plane by plane in the order P0, S, L into three TMEM
+// accumulators of BN = 160 columns (P1, P3, P2; 480 of 512 columns).
+
 // Structure: persistent kernel, one CTA per SM, 384 threads:
 //   warp 0      TMA producer (128 x 128-byte A boxes, 160 x 128-byte B boxes, 128B swizzle,
 //               STAGES-deep ring)
 //   warp 1      TMEM allocator and single-thread tcgen05.mma issuer (M = 128, N = 160, K = 32)
 //   warps 4..11 epilogue, two warps per TMEM lane quadrant (warp % 4), one column half each:
-//               tcgen05.ld 32x32b of P1 and P3 into T = 127 P1 + P3 (registers), release of those
-//               two accumulators (the next tile's H and S planes may start), then P2, the exact
+//               tcgen05.ld 32x32b of P1 and P3 into T = k1 P1 + P3 (registers), release of those
+//               two accumulators (the next tile's P0 and S planes may start), then P2, the exact
 //               recombination, scores into a 128 x 160 staging tile in shared memory, release of
 //               P2, and row-contiguous 16-byte stores from the staging tile; with LabelExtremes it
 //               also keeps each (query, label) list's min / max for the selection
