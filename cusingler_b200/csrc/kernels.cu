@@ -29,13 +29,16 @@
 namespace sgr {
 namespace {
 
-__device__ __forceinline__ int stage_d(const unsigned char* stage, int mode, int Kp, int p, int w) {
+// d at position p of a rank row already written to global memory by the warp's lanes (read through
+// L2: other lanes wrote it).
+__device__ __forceinline__ int stage_d(const unsigned char* row, int mode, int Kp, int p, int w) {
     if (mode == RANK_LIMBS) {
-        const int8_t* s = reinterpret_cast<const int8_t*>(stage);
-        return limb_mult(w) * (int)s[p] + (int)s[2 * Kp + p];
+        const signed char* s = reinterpret_cast<const signed char*>(row);
+        return limb_mult(w) * (int)__ldcg(s + p) + (int)__ldcg(s + 2 * Kp + p);
     }
-    if (mode == RANK_F16) return __half2int_rn(reinterpret_cast<const __half*>(stage)[p]);
-    return reinterpret_cast<const int16_t*>(stage)[p];
+    if (mode == RANK_F16)
+        return __half2int_rn(__ushort_as_half(__ldcg(reinterpret_cast<const unsigned short*>(row) + p)));
+    return __ldcg(reinterpret_cast<const short*>(row) + p);
 }
 
 __device__ __forceinline__ void stage_put(unsigned char* stage, int mode, int Kp, int p, int d, int w) {
@@ -76,11 +79,11 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
         }
         __syncthreads();
     }
-    // per warp: keys (cap x 8 B) | values by bucket (cap x 4 B) | 256 bucket counts / ends | stage
+    // per warp: keys (cap x 8 B) | values by bucket (cap x 4 B) | 256 bucket counts / ends; the
+    // output row is written in place in global memory (zeros first, then the stored entries)
     uint64_t* keys = reinterpret_cast<uint64_t*>(smem + map_bytes + (size_t)warp * warp_bytes);
     uint32_t* vals = reinterpret_cast<uint32_t*>(keys + a.cap);
     int* hist = reinterpret_cast<int*>(vals + a.cap);
-    unsigned char* stage = reinterpret_cast<unsigned char*>(hist + 256);
     const uint32_t n_items = a.n_items_dev ? (uint32_t)*a.n_items_dev : a.n_items;
     for (uint32_t item = blockIdx.x * wpb + warp; item < n_items; item += gridDim.x * wpb) {
         RankItem it;
@@ -205,7 +208,10 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
         }
 
         // 2) every position of the subset starts as an implicit zero: rank (G-k+1)/2, d = -k;
-        //    the padding [G, Kp) is 0 so that it adds nothing to a dot product
+        //    the padding [G, Kp) is 0 so that it adds nothing to a dot product.  Written straight
+        //    into the output row (coalesced words); the stored entries are written over it below.
+        const int row_bytes = a.out_mode == RANK_LIMBS ? 3 * Kp : 2 * Kp;
+        unsigned char* stage = reinterpret_cast<unsigned char*>(g.out) + (size_t)it.slot * row_bytes;
         const int d0 = -k;
         if (a.out_mode == RANK_LIMBS) {
             int h0, l0, s0;
@@ -230,6 +236,7 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
         }
         __syncwarp();
 
+        // the zeros are in place before any lane writes a stored entry over them (__syncwarp above)
         // 3) stored entries: d = 2 * (G - k + #less + (#equal + 1)/2) - (G + 1)
         int64_t sq = 0;
         if (fits) {
@@ -307,11 +314,6 @@ __global__ void __launch_bounds__(256) rank_kernel(RankLaunch a, int warp_bytes)
             if (lane == 0) g.f32norm[it.slot] = v;
         }
 
-        // 5) coalesced write of the staged row
-        const int row_bytes = a.out_mode == RANK_LIMBS ? 3 * Kp : 2 * Kp;
-        uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(g.out) + (size_t)it.slot * row_bytes);
-        const uint4* src = reinterpret_cast<const uint4*>(stage);
-        for (int w = lane; w < row_bytes / 16; w += 32) dst[w] = src[w];
         __syncwarp();
     }
 }
@@ -729,8 +731,7 @@ int sm_count() { return device_sm_count(); }
 
 namespace {
 void launch_rank_tier(const RankLaunch& a, long max_blocks, cudaStream_t s) {
-    const int stage_bytes = a.out_mode == RANK_LIMBS ? 3 * a.max_Kp : 2 * a.max_Kp;
-    const int warp_bytes = ((a.cap * 12 + 256 * 4 + stage_bytes) + 15) & ~15;
+    const int warp_bytes = ((a.cap * 12 + 256 * 4) + 15) & ~15;
     const int map_bytes = a.map_bits ? (int)(((a.n_cols + 31) / 32 * 6 + 15) & ~15u) : 0;
     // warps per CTA: the most resident warps per SM, then the widest CTA
     int wpb = 0, best = 0;
