@@ -580,8 +580,8 @@ __global__ void __launch_bounds__(NW * 32) select_first_kernel(const float* scor
 // (global memory; a label's second pass hits L1 / L2), so no block barrier waits for a row's longest
 // label, and a CTA needs only a histogram per warp (up to 64 warps per SM).  Every row has the same
 // labels, so the warps' work is balanced by construction.  Each warp prefetches its next row into L2.
-// MINB: CTAs per SM the register allocation is sized for (2: 64 registers, 4: 32 registers and 64
-// warps per SM).
+// MINB: CTAs per SM the register allocation is sized for (2: 64 registers and 32 warps per SM,
+// 3: 40 registers and 48 warps per SM).
 template <int NW, int MINB>
 __global__ void __launch_bounds__(NW * 32, MINB) select_rows_kernel(const float* scores, int64_t ld, int nq, int L,
                                                            const LabelQ* lq, float p, float thre,
@@ -963,7 +963,7 @@ void launch_select_first(const float* scores, int64_t ld, int nq, int L, const L
     if (nq <= 0) return;
     const size_t stage_bytes = (((size_t)std::max(row_len, 1) * 4 + 15) & ~size_t(15));
     if (lorder && (warps == 0 || warps == 1)) {  // one warp per row, 16 warps per CTA
-        auto kern = warps == 1 ? select_rows_kernel<16, 4> : select_rows_kernel<16, 2>;
+        auto kern = warps == 1 ? select_rows_kernel<16, 3> : select_rows_kernel<16, 2>;
         int per_sm = 0;
         SGR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 512, 0));
         per_sm = std::max(1, std::min(per_sm, 4));  // scratch is sized for 64 warps per SM

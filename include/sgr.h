@@ -149,7 +149,7 @@ sgr_status sgr_set_profiling(sgr_ctx* ctx, int on);
  * (1 to 4096; the bands of a group sweep the reference together so that the CTAs at work share
  * operand tiles in L2); what 7: the score-step selection's form: 8 or 16 warps per CTA that stages
  * a query row in shared memory, 0 for one warp per query row reading the scores directly, 1 the
- * same with 32 registers per thread (twice the warps per SM);
+ * same with 40 registers per thread (half again the warps per SM);
  * what 8: 1 trains the markers on the host instead of the device; what 9 (exact mode): 1 fine-tunes
  * each score block on a second stream while the next block is scored; what 10: the exact
  * correlation's tile: 8 or 16 for 128 x 256 tiles with two accumulators (when the trained marker
