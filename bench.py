@@ -472,8 +472,9 @@ def main():
             ann.set_tuning(1, args.ft_heavy)
             tuning["learned" if learned else "plain"] = {"pinned": True, "ft_warps": args.ft_warps,
                                                           "ft_heavy": args.ft_heavy, "score_chunk_mb": 1024,
-                                                          "corr_pair": 0, "corr_gm": 16, "select_warps": 0,
+                                                          "corr_pair": 0, "corr_gm": 16, "select_warps": 1,
                                                           "pipeline": 0, "corr_wide": 18}
+            apply_tuning("learned" if learned else "plain")  # the recorded shapes are the ones timed
             return
         tuning["learned" if learned else "plain"] = ann.autotune(
             tune_sample, learned=learned, min_confidence=args.min_confidence, check_fraction=args.check_fraction)

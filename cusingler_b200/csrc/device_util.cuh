@@ -3,6 +3,7 @@
 // STOmics/cusingler) by radix selection, with libstdc++'s sort order for NaN-bearing lists.
 #pragma once
 
+#include <climits>
 #include <cstdint>
 
 #include "kernels.cuh"
@@ -171,9 +172,15 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
     const float span = fmax - fmin;
     if (!(span > 1e-30f) || !(span < 1e30f)) return false;
     const float scale = 256.0f / span;
-    // clamped both ways, so that a value outside [min, max] (extremes supplied by the caller that do
-    // not match the list) still lands in a bin rather than outside the histogram
-    auto bin_of = [&](float x) { return max(0, min(255, (int)((x - fmin) * scale))); };
+    // The bin of x is round-to-nearest((x - min) * scale), read from the bits of one FMA whose result
+    // lies in [2^23, 2^24), where floats are the integers: bits(y) = 0x4B000000 + y - 2^23.  The map
+    // from x to those bits is monotone non-decreasing, which is all the selection needs (both passes
+    // use the same map).  Clamped both ways on the bits, so that a value outside [min, max] (extremes
+    // that do not match the list) still lands in a bin rather than outside the histogram.
+    constexpr int B0 = 0x4B000000;
+    const float shift = fmaf(-fmin, scale, 8388608.0f);
+    auto bin_bits = [&](float x) { return __float_as_int(fmaf(x, scale, shift)); };
+    auto bin_of = [&](float x) { return min(max(bin_bits(x), B0), B0 + 255) - B0; };
     for (int b = lane; b < 256; b += 32) hist[b] = 0;
     __syncwarp();
     int i = lane;
@@ -230,19 +237,35 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
         else nb = -1;
     }
     __syncwarp();
+    // Collect the values of bins bin..last (the bins between bin and nb are empty), compared on the
+    // map's bits: bin(x) >= bin holds for every x when bin is 0, else exactly when bits >= B0 + bin;
+    // bin(x) <= last likewise.  Raw float bits are stored and turned into order keys afterwards.
+    const int last = nb >= 0 ? nb : bin;
+    const int lo = bin == 0 ? INT_MIN : B0 + bin, hi = last == 255 ? INT_MAX : B0 + last;
     uint32_t* buf = reinterpret_cast<uint32_t*>(hist);
     int w = 0;
     const unsigned lt = (1u << lane) - 1u;
-    for (int base = 0; base < n; base += 64) {  // two 32-value chunks per step
-        const int i0 = base + lane, i1 = base + 32 + lane;
-        const float x0 = i0 < n ? v[i0] : 0.f, x1 = i1 < n ? v[i1] : 0.f;
-        const int b0 = bin_of(x0), b1 = bin_of(x1);
-        const bool in0 = i0 < n && (b0 == bin || b0 == nb), in1 = i1 < n && (b1 == bin || b1 == nb);
+    int base = 0;
+    for (; base + 64 <= n; base += 64) {  // two 32-value chunks per step
+        const float x0 = v[base + lane], x1 = v[base + 32 + lane];
+        const int y0 = bin_bits(x0), y1 = bin_bits(x1);
+        const bool in0 = y0 >= lo && y0 <= hi, in1 = y1 >= lo && y1 <= hi;
         const unsigned m0 = __ballot_sync(FULL, in0), m1 = __ballot_sync(FULL, in1);
-        if (in0) buf[w + __popc(m0 & lt)] = ord_key(x0);
-        if (in1) buf[w + __popc(m0) + __popc(m1 & lt)] = ord_key(x1);
+        if (in0) buf[w + __popc(m0 & lt)] = __float_as_uint(x0);
+        if (in1) buf[w + __popc(m0) + __popc(m1 & lt)] = __float_as_uint(x1);
         w += __popc(m0) + __popc(m1);
     }
+    for (; base < n; base += 32) {
+        const int i0 = base + lane;
+        const float x0 = i0 < n ? v[i0] : 0.f;
+        const int y0 = bin_bits(x0);
+        const bool in0 = i0 < n && y0 >= lo && y0 <= hi;
+        const unsigned m0 = __ballot_sync(FULL, in0);
+        if (in0) buf[w + __popc(m0 & lt)] = __float_as_uint(x0);
+        w += __popc(m0);
+    }
+    __syncwarp();
+    for (int i = lane; i < total; i += 32) buf[i] = ord_key(__uint_as_float(buf[i]));
     int np = 1;
     while (np < total) np <<= 1;
     for (int i = total + lane; i < np; i += 32) buf[i] = 0xffffffffu;
