@@ -171,7 +171,7 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
     const float fmin = key_float(kmin), fmax = key_float(kmax);
     const float span = fmax - fmin;
     if (!(span > 1e-30f) || !(span < 1e30f)) return false;
-    const float scale = 256.0f / span;
+    const float scale = __fdividef(256.0f, span);  // any positive scale keeps the map monotone
     // The bin of x is round-to-nearest((x - min) * scale), read from the bits of one FMA whose result
     // lies in [2^23, 2^24), where floats are the integers: bits(y) = 0x4B000000 + y - 2^23.  The map
     // from x to those bits is monotone non-decreasing, which is all the selection needs (both passes
@@ -265,28 +265,41 @@ __device__ bool bucket_select(const float* v, int n, int j, int* hist, int lane,
         w += __popc(m0);
     }
     __syncwarp();
-    for (int i = lane; i < total; i += 32) buf[i] = ord_key(__uint_as_float(buf[i]));
-    int np = 1;
-    while (np < total) np <<= 1;
-    for (int i = total + lane; i < np; i += 32) buf[i] = 0xffffffffu;
-    __syncwarp();
-    for (int size = 2; size <= np; size <<= 1)
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int t = lane; t < (np >> 1); t += 32) {
-                const int a = 2 * t - (t & (stride - 1)), b = a + stride;
-                const uint32_t x = buf[a], y = buf[b];
-                if ((x > y) == ((a & size) == 0)) {
-                    buf[a] = y;
-                    buf[b] = x;
-                }
-            }
-            __syncwarp();
+    const int r = j - before;  // statistic j is the r-th smallest collected key (r < cnt <= total)
+    bool have_b = r + 1 < total;
+    if (total <= 32) {
+        // one key per lane; its rank among the collected keys (ties by position) picks r and r + 1
+        const uint32_t key = lane < total ? ord_key(__uint_as_float(buf[lane])) : 0xffffffffu;
+        int rank = 0;
+        for (int t = 0; t < total; ++t) {
+            const uint32_t kt = __shfl_sync(FULL, key, t);
+            rank += (kt < key) | ((kt == key) & (t < lane));
         }
-    const int r = j - before;
-    *ka = buf[r];
-    if (r + 1 < total) {
-        *kb = buf[r + 1];
+        *ka = __shfl_sync(FULL, key, __ffs(__ballot_sync(FULL, lane < total && rank == r)) - 1);
+        const unsigned mb = __ballot_sync(FULL, lane < total && rank == r + 1);
+        if (have_b) *kb = __shfl_sync(FULL, key, __ffs(mb) - 1);
     } else {
+        for (int i = lane; i < total; i += 32) buf[i] = ord_key(__uint_as_float(buf[i]));
+        int np = 1;
+        while (np < total) np <<= 1;
+        for (int i = total + lane; i < np; i += 32) buf[i] = 0xffffffffu;
+        __syncwarp();
+        for (int size = 2; size <= np; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int t = lane; t < (np >> 1); t += 32) {
+                    const int a = 2 * t - (t & (stride - 1)), b = a + stride;
+                    const uint32_t x = buf[a], y = buf[b];
+                    if ((x > y) == ((a & size) == 0)) {
+                        buf[a] = y;
+                        buf[b] = x;
+                    }
+                }
+                __syncwarp();
+            }
+        *ka = buf[r];
+        if (have_b) *kb = buf[r + 1];
+    }
+    if (!have_b) {  // statistic j + 1 lies beyond the collected bins: the smallest key above ka
         uint32_t nxt = 0xffffffffu;
         for (int i = lane; i < n; i += 32) {
             const uint32_t u = ord_key(v[i]);
