@@ -808,7 +808,7 @@ ScorePlan score_begin(sgr_ctx* ctx, const DevCsr& q, float p, float thre, const 
 // Block c of the score step on the context's stream: rows [starts[c], starts[c + 1]).
 void score_block(sgr_ctx* ctx, const ScorePlan& pl, uint32_t c) {
     cudaStream_t s = ctx->stream;
-    const uint32_t Q = pl.q.n_rows, R = ctx->R, L = ctx->mk.n_labels;
+    const uint32_t R = ctx->R, L = ctx->mk.n_labels;
     const uint32_t q0 = pl.starts[c];
     const int nq = (int)(pl.starts[c + 1] - q0);
     int sp = -1;

@@ -161,13 +161,15 @@ __device__ int cta_gene_set(const FtPersistentArgs& a, const uint8_t* top, int n
             }
         }
     }
-    // many pairs: a warp takes 32 ordered pairs at a time: each lane fetches one pair's list, then the
-    // warp walks the 32 lists together so that the gene loads of several pairs are in flight at once
-    for (int base = warp * 32; np > 4 * NW && base < np; base += NW * 32) {
+    // many pairs: a warp takes ppw ordered pairs at a time (at most 32, and few enough that every warp
+    // gets some): each lane fetches one pair's list, then the warp walks the lists together so that the
+    // gene loads of several pairs are in flight at once
+    const int ppw = min(32, (np + NW - 1) / NW);
+    for (int base = warp * ppw; np > 4 * NW && base < np; base += NW * ppw) {
         const int pr = base + lane;
         uint32_t pos = 0;
         int len = 0;
-        if (pr < ntop * ntop) {
+        if (lane < ppw && pr < np) {
             const int i = pr / ntop, j = pr % ntop;
             if (i != j) {
                 const size_t pi = (size_t)top[i] * a.L + top[j];
@@ -178,7 +180,7 @@ __device__ int cta_gene_set(const FtPersistentArgs& a, const uint8_t* top, int n
         const int maxn = __reduce_max_sync(FULL, len);
         for (int e0 = 0; e0 < maxn; e0 += 32) {
 #pragma unroll 8
-            for (int t = 0; t < 32; ++t) {
+            for (int t = 0; t < ppw; ++t) {
                 const uint32_t p = __shfl_sync(FULL, pos, t);
                 const int n = __shfl_sync(FULL, len, t);
                 const int e = e0 + lane;

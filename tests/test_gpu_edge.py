@@ -156,6 +156,44 @@ def test_long_labels_ties_and_nan_lists(select_form):
     _run_both(prob, abi.MODE_EXACT, tuning=[(7, select_form)])
 
 
+@pytest.mark.parametrize("mode,select_form", [(abi.MODE_EXACT, 1), (abi.MODE_EXACT, 16), (abi.MODE_FP32REF, 1)])
+def test_tied_order_statistics_in_small_bins(mode, select_form):
+    """Score lists whose order statistic k-1 lies in a run of tied values that fits the bucket
+    selection's 256-key buffer.  One label holds 150 copies of one reference cell among 180 (the
+    statistic's bin holds 150 to 180 keys: the bitonic sort ranks them), another 20 copies among 25
+    (20 to 25 keys: the warp-shuffle rank, with ties).  Scores, first labels, flags and final labels
+    equal the oracle's."""
+    w, ref, qry = synth.custom_dataset(900, 96, 2000, 3, 0.08, seed=41)
+
+    def rows_of(m):
+        return [list(zip(m.indices[m.indptr[i]:m.indptr[i + 1]], m.data[m.indptr[i]:m.indptr[i + 1]]))
+                for i in range(m.n_rows)]
+
+    rows_r = rows_of(ref)
+    by_label = [np.flatnonzero(ref.labels == l) for l in range(3)]
+    keep0, keep1 = by_label[0][:180], by_label[1][:25]
+    for i in keep0[1:150]:
+        rows_r[i] = list(rows_r[keep0[0]])
+    for i in keep1[1:20]:
+        rows_r[i] = list(rows_r[keep1[0]])
+    order = np.concatenate([keep0, keep1, by_label[2]])
+    labels = ref.labels[order]
+    r = _csr_from_rows([rows_r[i] for i in order], ref.n_cols)
+    prob = O.Problem(r, qry, synth.names("CT", 3), labels, synth.names("G", ref.n_cols),
+                     synth.names("G", qry.n_cols))
+    # the construction: in every scored row, statistic k-1 of label 0 is tied 150+ times, of label 1
+    # 20+ times (p = 0.8: k - 1 = 143 of 180 and 19 of 25 lie inside the copies' run of ranks)
+    orc = O.Oracle(prob)
+    orc.train()
+    raw = orc.score(mode=1, raw=True)[3]
+    for q in range(raw.shape[0]):
+        for lab, k1, ties in ((0, 143, 150), (1, 19, 20)):
+            v = np.sort(raw[q, labels == lab])
+            if not np.isnan(v).any():
+                assert (v == v[k1]).sum() >= ties, (q, lab)
+    _run_both(prob, mode, tuning=[(7, select_form)])
+
+
 def test_many_query_rows_tiled_scan():
     """9,000 query rows: the thre-pool compaction's exclusive scan over the rows' counts runs as
     4,096-row tiles in parallel (three tiles); scores, labels, flags and fine-tune rounds equal
