@@ -91,6 +91,12 @@ class ClockSampler:
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
+            # nvidia-smi's start-up (NVML initialisation) takes driver time: let it finish before the
+            # timed steps, whose host round trips it would otherwise stall; its first sample is the
+            # clock at the start of the region
+            t0 = time.monotonic()
+            while not self.rows and self.proc.poll() is None and time.monotonic() - t0 < 10.0:
+                time.sleep(0.005)
         except Exception:
             self.proc = None
         return self
