@@ -595,17 +595,28 @@ __global__ void __launch_bounds__(NW * 32, MINB) select_rows_kernel(const float*
     const int gw = blockIdx.x * NW + warp, n_warps = gridDim.x * NW;
     float* my_scratch = scratch ? scratch + (size_t)gw * spw : nullptr;
     float* ls = ls_all[warp];
+    // rows start on 16 bytes when ld is a multiple of 4, so a label's list widened to 16-byte bounds
+    // stays inside its row
     const bool pf = (ld % 4) == 0 && (reinterpret_cast<uintptr_t>(scores) & 15) == 0;
     for (int q = gw; q < nq; q += n_warps) {
         const float* row = scores + (size_t)q * ld;
         const bool qnan = qn2[q] == 0;
-        if (pf && lane == 0 && q + n_warps < nq && qn2[q + n_warps] != 0) {
-            const uint32_t bytes = (uint32_t)(row_len * 4 + 15) & ~15u;
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(scores + (size_t)(q + n_warps) * ld),
-                         "r"(bytes)
-                         : "memory");
-        }
+        // L2 prefetch of the list of the label two ahead (a whole row fetched a row ahead is evicted
+        // before use: every warp of the GPU streams its own rows meanwhile)
+        auto prefetch_label = [&](int idx) {
+            if (pf && !qnan && lane == 0 && idx < L) {
+                const LabelQ dn = lq[lorder[idx]];
+                const uintptr_t a0 = reinterpret_cast<uintptr_t>(row + dn.start) & ~uintptr_t(15);
+                const uintptr_t a1 = (reinterpret_cast<uintptr_t>(row + dn.start + dn.len) + 15) & ~uintptr_t(15);
+                if (a1 > a0)
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"((uint32_t)(a1 - a0))
+                                 : "memory");
+            }
+        };
+        prefetch_label(0);
+        prefetch_label(1);
         for (int i = 0; i < L; ++i) {
+            prefetch_label(i + 2);
             const int l = lorder[i];
             const LabelQ d = lq[l];
             float r;
