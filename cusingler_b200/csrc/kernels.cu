@@ -579,7 +579,8 @@ __global__ void __launch_bounds__(NW * 32) select_first_kernel(const float* scor
 // Warp-per-row form: each warp selects every label of its query rows straight from the score rows
 // (global memory; a label's second pass hits L1 / L2), so no block barrier waits for a row's longest
 // label, and a CTA needs only a histogram per warp (up to 64 warps per SM).  Every row has the same
-// labels, so the warps' work is balanced by construction.  Each warp prefetches its next row into L2.
+// labels, so the warps' work is balanced by construction.  Each warp prefetches into L2 the list of the
+// label two ahead in its row.
 // MINB: CTAs per SM the register allocation is sized for (2: 64 registers and 32 warps per SM,
 // 3: 40 registers and 48 warps per SM).
 template <int NW, int MINB>
