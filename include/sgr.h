@@ -28,7 +28,7 @@ typedef enum sgr_status {
     SGR_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed                              */
     SGR_ERR_NO_INTERSECTION = 4,  /* reference and query share no gene name                */
     SGR_ERR_EMPTY_LABEL = 5,      /* a label name has no reference cell                    */
-    SGR_ERR_UNSUPPORTED = 6,      /* a size beyond what this build supports                */
+    SGR_ERR_UNSUPPORTED = 6,      /* a size beyond what the library supports               */
     SGR_ERR_STATE = 7,            /* call order violated (e.g. score before train)         */
     SGR_ERR_TIMEOUT = 8           /* a bounded device wait ran out                          */
 } sgr_status;
